@@ -1,0 +1,490 @@
+"""Benchmark: direct softened gravity at N = 2^20 on B200 (mixed precision vs FP64).
+
+A "step" is one kick-drift-kick step of the whole system (one force evaluation of
+N(N-1) ordered interactions).  Default workload: two exponential disks of 524,288 bodies
+(mass ratio 3:1), softening 0.01, dt 0.001; one initial force evaluation, W untimed warm-up
+steps and K timed steps (K = 10: "1 eval + 10 KDK steps").  The 80 MiB FP64 state fits in
+L2, so L2 is flushed (a 256 MiB device write) before every timed step, outside the timed
+interval.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line from rank 0.  `value` is device-resident throughput (CUDA events on the
+stream the session launches on, max over ranks); `e2e` is the same metric through the C ABI
+with host buffers (gx_leapfrog_step: H2D of the state, the step, D2H of the result, every
+step).  Multi-GPU (torchrun): target ranges per rank, one NCCL all-gather of positions per
+step, strong scaling at fixed N.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "galaxy-collision-simulation_b200"
+METRIC = "Ginteractions/s at N=1M: mixed-prec vs FP64 GPU @ rel-err≤1e-6; adjoint/fwd"
+UNIT = "Ginteractions/s"
+FMA_PIPE_OPS_PER_INTERACTION = 12  # 3 FADD, 3 FFMA (r^2), 2 FMUL (inv^3), 1 FMUL (m), 3 FFMA (acc)
+FP32_LANES_PER_SM = 128
+
+
+def load_gx():
+    if "gx" in sys.modules:
+        return sys.modules["gx"]
+    spec = importlib.util.spec_from_file_location("gx", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gx"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="gx_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            f = [c.strip() for c in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(f[1]), max=float(f[2]), power=float(f[3]) if f[3] not in ("[N/A]", "") else 0.0,
+                                 hw=f[5], hwt=f[6], swt=f[7], swp=f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [r for r in rows if r["power"] > 300.0] or rows
+        reasons = set()
+        for r in loaded:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                              ("swp", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median([r["sm"] for r in loaded])), "sm_max_mhz": max(r["max"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(loaded),
+                "power_w_max": max(r["power"] for r in rows)}
+
+
+# ---------------------------------------------------------------------------------------
+# CPU baseline: the reference's own per-target direct sum on the host cores
+# ---------------------------------------------------------------------------------------
+def cpu_threads() -> int:
+    return len(os.sched_getaffinity(0))
+
+
+def cpu_reference_rate(p, eps, seconds: float = 10.0, threads: int | None = None) -> dict:
+    """G interactions/s of compute_direct_accelerations_for_targets split over all host
+    threads by ownership ranges (oracle/_ref), or of the C restatement when the reference
+    library is absent, on a contiguous target sample sized to about `seconds` of wall time."""
+    sys.path.insert(0, str(ROOT))
+    import oracle
+
+    threads = threads or cpu_threads()
+    n = len(p)
+    kind = "reference" if oracle.ref_available() else "port"
+
+    def run(count):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            oracle.ref_direct_targets(p.x, p.y, p.z, p.m, 1.0, eps, 0, count, threads=threads)
+        else:
+            oracle.direct_indexed(p.x, p.y, p.z, p.m, 1.0, eps, np.arange(count), threads=threads)
+        return time.perf_counter() - t0
+
+    cal = min(n, threads * 2)
+    t = run(cal)
+    count = int(min(n, max(threads, cal * seconds / max(t, 1e-3))))
+    t = run(count)
+    rate = count * (n - 1) / t / 1e9
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"targets 0..{count} of N={n} against all N sources "
+                      f"({'compute_direct_accelerations_for_targets' if kind == 'reference' else 'oracle restatement'}"
+                      f", {threads} threads by ownership ranges), {t:.1f} s wall",
+            "seconds": t, "targets": count}
+
+
+# ---------------------------------------------------------------------------------------
+# profiles: DRAM traffic of the dominant kernel from the committed ncu summary
+# ---------------------------------------------------------------------------------------
+def ncu_traffic(n: int):
+    f = ROOT / "profiles" / "force_mixed_n1048576.md"
+    if not f.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch_at_n1048576\s*=\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m and n == 1 << 20 else None
+
+
+# ---------------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1 << 20, help="bodies (default 2^20; two disks, mass ratio 3:1)")
+    ap.add_argument("--precision", choices=["mixed", "f64"], default="mixed")
+    ap.add_argument("--quick", action="store_true", help="kernel timing only (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 1)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    eps, dt = 0.01, 0.001
+    n = args.n
+
+    if args.impl == "reference":
+        return reference_arm(args, rank, n, eps, dt)
+
+    import torch
+    import torch.distributed as dist
+
+    gx = load_gx()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps, mass1=1.0, mass2=1.0 / 3.0)
+    prec = gx.PRECISION_MIXED if args.precision == "mixed" else gx.PRECISION_F64
+    if world > 1:
+        res = run_sharded(gx, torch, dist, p, args, rank, world, eps, dt, prec)
+    else:
+        res = run_single(gx, torch, p, args, eps, dt, prec)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def l2_flusher(torch):
+    buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    return lambda: buf.fill_(1)
+
+
+def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
+    n = len(p)
+    params = gx.PhysicsParams(1.0, eps)
+    pairs = n * (n - 1)
+    stream = torch.cuda.current_stream()
+    flush = l2_flusher(torch)
+    peaks = measured_peaks()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    sm_max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    out = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "data": "synthetic",
+           "dtype": "f32-pair/f64-state" if prec == gx.PRECISION_MIXED else "f64"}
+
+    sess = gx.Session(n, params)
+    sess.set_stream(stream)
+    sess.set_particles(p)
+    tune_ms = None
+    if not args.no_autotune and not args.quick:
+        tune_ms = sess.autotune(prec)
+    variant, jsplit = sess.get_config(prec)
+    sess.compute_accelerations(prec)  # the initial force evaluation
+    torch.cuda.synchronize()
+    e0 = None if args.quick else sess.diagnostics().total_energy
+    for _ in range(args.warmup):
+        sess.step(1, dt, prec)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    sess.enable_timing(True)
+    evs = []
+    for _ in range(args.steps):
+        flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sess.step(1, dt, prec)
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    force_ms, force_launches = sess.force_timing()
+    sess.enable_timing(False)
+    clk = clocks.stop()
+    total_s = sum(step_ms) / 1e3
+    value = args.steps * pairs / total_s / 1e9
+    force_avg_s = force_ms / 1e3 / max(force_launches, 1)
+    launches_per_step = 2 + (1 if jsplit > 1 else 0)
+    out.update({"value": value, "ms_per_step": sum(step_ms) / args.steps, "steps_per_s": args.steps / total_s,
+                "gpu_launches": args.steps * launches_per_step})
+    fp32_peak = sms * FP32_LANES_PER_SM * sm_max_mhz * 1e6 / 1e12
+    achieved = pairs * FMA_PIPE_OPS_PER_INTERACTION / force_avg_s / 1e12
+    roof = {"bound": "fp32_fma_pipe", "achieved": achieved,
+            "peak": fp32_peak, "unit": "T FP32-pipe lane-ops/s",
+            "frac": achieved / fp32_peak,
+            "peak_basis": f"{sms} SMs x {FP32_LANES_PER_SM} FP32 lanes x {sm_max_mhz:.0f} MHz (sm_max_mhz of "
+                          "MEASURED_PEAKS.json); the FP32 FMA pipe bounds this kernel, not HBM or tensor cores",
+            "ops_per_interaction": FMA_PIPE_OPS_PER_INTERACTION,
+            "kernel_ms_per_launch": force_avg_s * 1e3,
+            "traffic": ncu_traffic(n)}
+    if clk.get("sm_mhz"):
+        roof["frac_at_observed_clock"] = achieved / (sms * FP32_LANES_PER_SM * clk["sm_mhz"] * 1e6 / 1e12)
+    if prec == gx.PRECISION_F64:
+        roof["note"] = "FP64 form: 17 FP64 pipe ops per interaction; frac is against the FP32 pipe"
+    out["roofline"] = roof
+    out["clocks"] = clk
+    out["config"] = {"workload": f"direct-mixed-n{n}" if prec == gx.PRECISION_MIXED else f"direct-f64-n{n}",
+                     "n": n, "disks": "2 exponential disks, mass ratio 3:1", "softening": eps, "dt": dt,
+                     "initial_eval": 1, "kernel": gx.describe_variant(prec, variant), "jsplit": jsplit,
+                     "autotune_ms_per_eval": tune_ms,
+                     "l2": "flushed (256 MiB device write) before every timed step, outside the timed interval"}
+    if args.quick:
+        sess.close()
+        return out
+
+    state = sess.get_state()
+    e1 = sess.diagnostics().total_energy
+    out["energy_drift"] = {"relative": abs(e1 - e0) / abs(e0), "steps": args.warmup + args.steps,
+                           "precision": "fp64 diagnostics"}
+
+    # -- accuracy of the production accelerations on 4096 sampled targets (FP64 exact form
+    #    = compute_direct_accelerations_for_targets bit for bit) --------------------------
+    rng = np.random.default_rng(4096)
+    idx = np.sort(rng.choice(n, 4096, replace=False))
+    q = gx.ParticleSet(state["x"], state["y"], state["z"], state["vx"], state["vy"], state["vz"], p.m)
+    a_prod = np.stack([state["ax"], state["ay"], state["az"]], 1)[idx]
+    a_ref = gx.indexed_accelerations(q, params, idx, gx.PRECISION_F64_EXACT)
+    err = np.linalg.norm(a_prod - a_ref, axis=1) / np.maximum(np.linalg.norm(a_ref, axis=1), 1e-300)
+    out["rel_err"] = {"median": float(np.median(err)), "max": float(err.max()), "targets": 4096,
+                      "vs": "FP64 (exact per-target form) at the final positions"}
+
+    # -- FP64 direct path on the same system ---------------------------------------------
+    if prec == gx.PRECISION_MIXED:
+        out["fp64"] = fp64_rate(gx, torch, sess, p, dt, flush)
+        out["mixed_over_fp64"] = value / out["fp64"]["value"]
+    sess.close()
+
+    # -- end to end through the C ABI with host buffers ------------------------------------
+    out["e2e"] = e2e_rate(gx, torch, p, params, dt, prec)
+
+    # -- adjoint vs forward at the differentiable-fit size --------------------------------
+    out["adjoint"] = adjoint_ratio(gx, torch)
+
+    # -- CPU baseline on the host cores -----------------------------------------------------
+    q0 = gx.ParticleSet(p.x, p.y, p.z, p.vx, p.vy, p.vz, p.m)
+    out["cpu_baseline"] = cpu_reference_rate(q0, eps, args.cpu_seconds)
+    return out
+
+
+def fp64_rate(gx, torch, sess, p, dt, flush, steps: int = 2) -> dict:
+    n = len(p)
+    stream = torch.cuda.current_stream()
+    sess.set_particles(p)
+    sess.compute_accelerations(gx.PRECISION_F64)
+    sess.step(1, dt, gx.PRECISION_F64)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sess.step(1, dt, gx.PRECISION_F64)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    v, js = sess.get_config(gx.PRECISION_F64)
+    return {"value": steps * n * (n - 1) / (sum(ms) / 1e3) / 1e9, "unit": UNIT, "ms_per_step": sum(ms) / steps,
+            "steps": steps, "kernel": gx.describe_variant(gx.PRECISION_F64, v), "jsplit": js}
+
+
+def e2e_rate(gx, torch, p, params, dt, prec, steps: int = 2) -> dict:
+    """gx_leapfrog_step on pinned host arrays: copies in, step, copies out, every step."""
+    n = len(p)
+    host = {}
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m"):
+        t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = getattr(p, k)
+        host[k] = t.numpy()
+    q = gx.ParticleSet(*(host[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m", "ax", "ay", "az")))
+    # the ParticleSet keeps the pinned buffers (already contiguous float64)
+    for k in host:
+        setattr(q, k, host[k])
+    gx.compute_cuda_direct_accelerations(q, params, prec)
+    gx.cuda_direct_leapfrog_step(q, dt, params, prec)  # warm-up
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        gx.cuda_direct_leapfrog_step(q, dt, params, prec)
+        times.append(time.perf_counter() - t0)
+    return {"value": steps * n * (n - 1) / sum(times) / 1e9, "unit": UNIT, "h2d_bytes_per_step": 10 * 8 * n,
+            "d2h_bytes_per_step": 9 * 8 * n, "steps": steps,
+            "api": "gx_leapfrog_step (cuda_direct_leapfrog_step) on pinned host arrays, wall clock"}
+
+
+def adjoint_ratio(gx, torch, n: int = 16384) -> dict:
+    """Adjoint step (VJP kernel + reverse kick-drift-kick vector work) vs forward KDK step."""
+    from gx import adjoint
+
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 16384, 0.05)
+    params = gx.PhysicsParams(1.0, 0.05)
+    X = torch.tensor(np.stack([p.x, p.y, p.z]), device="cuda")
+    V = torch.tensor(np.stack([p.vx, p.vy, p.vz]), device="cuda")
+    m = torch.tensor(p.m, device="cuda")
+    A = adjoint.accelerations(X, m, params, gx.PRECISION_MIXED)
+    xb = torch.randn_like(X)
+    vb = torch.randn_like(X)
+    dt = 0.005
+
+    def fwd():
+        adjoint._step(X, V, A, m, dt, params, gx.PRECISION_MIXED)
+
+    def adj():
+        nonlocal xb, vb
+        vb2 = vb + dt * xb
+        g, gm = adjoint.direct_vjp(X, m, dt * vb2, params, gx.PRECISION_MIXED)
+        xb = xb + g
+
+    res = {}
+    for name, fn in (("fwd_step_ms", fwd), ("adj_step_ms", adj)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(20):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        res[name] = a.elapsed_time(b) / 20
+    res["ratio"] = res["adj_step_ms"] / res["fwd_step_ms"]
+    res["n"] = n
+    res["precision"] = "mixed"
+    res["note"] = "checkpoint recompute costs one forward step per adjoint step, reported separately"
+    return res
+
+
+def run_sharded(gx, torch, dist, p, args, rank, world, eps, dt, prec) -> dict:
+    """Strong scaling: rank r owns the targets of ownership_range(n, r, world); every step
+    kicks and drifts the owned bodies, all-gathers positions (NCCL) and evaluates the owned
+    targets against all sources with the engine kernel."""
+    from gx.sharded import ShardedLeapfrog
+
+    n = len(p)
+    params = gx.PhysicsParams(1.0, eps)
+    pairs = n * (n - 1)
+    X = torch.tensor(np.stack([p.x, p.y, p.z]), device="cuda")
+    m = torch.tensor(p.m, device="cuda")
+    ffi = gx._ffi
+
+    def force(Xf, mm, b, e):
+        A = torch.empty(3, e - b, dtype=torch.float64, device="cuda")
+        ffi.call("gx_direct_accel_targets", n, Xf[0].data_ptr(), Xf[1].data_ptr(), Xf[2].data_ptr(), mm.data_ptr(),
+                 b, e, None, 0, params.ffi(), prec, A[0].data_ptr(), A[1].data_ptr(), A[2].data_ptr(),
+                 torch.cuda.current_stream().cuda_stream)
+        return A
+
+    sh = ShardedLeapfrog(n, force)
+    V = torch.tensor(np.stack([p.vx, p.vy, p.vz])[:, sh.begin:sh.end].copy(), device="cuda")
+    A = sh.initial_accelerations(X, m)
+    for _ in range(args.warmup):
+        sh.step(X, V, A, m, dt)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        sh.step(X, V, A, m, dt)
+    b.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = torch.tensor([a.elapsed_time(b)], device="cuda")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    clk = clocks.stop()
+    total_s = float(ms) / 1e3
+    return {"metric": METRIC, "value": args.steps * pairs / total_s / 1e9, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(ms) / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32-pair/f64-state",
+            "data": "synthetic", "gpu_launches": args.steps * 4, "clocks": clk,
+            "config": {"workload": f"direct-mixed-n{n}", "n": n, "parallelism": f"targets{world}",
+                       "exchange": "NCCL all-gather of FP64 positions (24 B/body/step)", "softening": eps, "dt": dt,
+                       "l2": "state 80 MiB < L2; not flushed in the multi-GPU run (one exchange per step)"}}
+
+
+def reference_arm(args, rank, n, eps, dt):
+    """The reference's own CPU direct sum (compute_direct_accelerations_for_targets, its
+    unmodified sources in oracle/_ref) on all host threads; each step a bounded sample of
+    targets of the same N=2^20 system."""
+    if rank != 0:
+        return
+    gx = load_gx()
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps, mass1=1.0, mass2=1.0 / 3.0)
+    per_step_s = max(2.0, min(12.0, 150.0 / max(1, args.steps + args.warmup)))
+    first = cpu_reference_rate(p, eps, per_step_s)
+    rates = []
+    for k in range(args.steps):
+        rates.append(cpu_reference_rate(p, eps, per_step_s)["value"])
+    value = float(np.median(rates))
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": n * (n - 1) / (value * 1e9) * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"direct-mixed-n{n}", "n": n, "softening": eps, "dt": dt,
+                   "note": "CPU timing extrapolated from a bounded target sample per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": first["cores"], "kind": first["kind"],
+                         "sample": first["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+if __name__ == "__main__":
+    main()

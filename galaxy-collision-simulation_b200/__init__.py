@@ -1,0 +1,30 @@
+"""B200 softened-gravity engine for ryan-charette/galaxy-collision-simulation.
+
+Drops in behind the reference's ``solver = "cuda-direct"`` path and the P2P near-field leaves
+of its FMM.  Compute runs in hand-written sm_100a CUDA kernels behind the C ABI of
+``include/gx.h`` (``_lib/libgx.so``); this package is the Python host side:
+
+* ``engine``   -- the reference solver interface (cuda_solver_available,
+                  compute_cuda_direct_accelerations, cuda_direct_leapfrog_step, ...)
+* ``session``  -- device-resident sessions and batched ensembles (CUDA graphs)
+* ``fmm_p2p``  -- reference-octree leaf lists and the GPU near field
+* ``adjoint``  -- autograd Function over the leapfrog with the adjoint kernel (needs torch)
+* ``ics``      -- seeded two-disk initial conditions
+"""
+from ._ffi import (GX_ERR_CUDA, GX_ERR_INVALID_ARGUMENT, GX_ERR_NO_DEVICE, GX_ERR_OUT_OF_MEMORY, GX_ERR_TIMEOUT,
+                   GX_ERR_UNSUPPORTED, GX_OK, LIB_PATH, PRECISION_F64, PRECISION_F64_EXACT, PRECISION_MIXED, GxError,
+                   device_available, load)
+from .engine import (Diagnostics, ParticleSet, PhysicsParams, compute_cuda_direct_accelerations,
+                     compute_diagnostics, compute_direct_accelerations_for_targets, cuda_direct_leapfrog_step,
+                     cuda_solver_available, indexed_accelerations)
+from .fmm_p2p import LeafLists, build_leaf_lists, p2p_leaves
+from .session import Batch, Session, batch_accelerations, describe_variant
+from . import ics
+
+__all__ = [
+    "GxError", "PhysicsParams", "ParticleSet", "Diagnostics", "Session", "Batch", "LeafLists",
+    "cuda_solver_available", "compute_cuda_direct_accelerations", "compute_direct_accelerations_for_targets",
+    "cuda_direct_leapfrog_step", "compute_diagnostics", "indexed_accelerations", "build_leaf_lists", "p2p_leaves",
+    "batch_accelerations", "describe_variant", "device_available", "load", "ics",
+    "PRECISION_F64", "PRECISION_MIXED", "PRECISION_F64_EXACT",
+]

@@ -1,0 +1,1858 @@
+// api.cu -- the C ABI of include/gx.h: argument checking, host/device pointer handling,
+// kernel-variant choice (with the j-split sized by a wave-quantisation model), the
+// resident session with CUDA-graph stepping, batched ensembles, the adjoint and the
+// autotuner.  No exception crosses the ABI; every entry point returns a gx_status and
+// records a message for gx_last_error() on the calling thread.
+#include "gx.h"
+
+#include "batch.cuh"
+#include "force.cuh"
+#include "integrate.cuh"
+#include "p2p.cuh"
+#include "vjp.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <initializer_list>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+using namespace gx;
+
+// ======================================================================================
+// errors
+// ======================================================================================
+namespace {
+thread_local std::string g_err;
+std::atomic<int> g_fail_allocs{0};
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int fail_cuda(cudaError_t e, const char* what) {
+    cudaGetLastError();  // clear a non-sticky error so the context stays usable
+    return fail(e == cudaErrorMemoryAllocation ? GX_ERR_OUT_OF_MEMORY : GX_ERR_CUDA, "%s: %s (%s)",
+                what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+#define GX_CUDA(call)                                        \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return fail_cuda(e_, #call);  \
+    } while (0)
+
+#define GX_TRY(call)                    \
+    do {                                \
+        int s_ = (call);                \
+        if (s_ != GX_OK) return s_;     \
+    } while (0)
+
+#define GX_GUARD_BEGIN try {
+#define GX_GUARD_END                                                                 \
+    }                                                                                \
+    catch (const std::bad_alloc&) {                                                  \
+        return fail(GX_ERR_OUT_OF_MEMORY, "host allocation failed");                 \
+    }                                                                                \
+    catch (...) {                                                                    \
+        return fail(GX_ERR_CUDA, "unexpected C++ exception inside the gx library");  \
+    }
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    int left = g_fail_allocs.load();
+    while (left > 0) {
+        if (g_fail_allocs.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes ? bytes : 16);
+}
+
+cudaError_t dev_alloc_async(void** p, size_t bytes, cudaStream_t st) {
+    int left = g_fail_allocs.load();
+    while (left > 0) {
+        if (g_fail_allocs.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
+    }
+    return cudaMallocAsync(p, bytes ? bytes : 16, st);
+}
+
+// ======================================================================================
+// devices, pointers
+// ======================================================================================
+int g_dev_status = -1;  // -1 unknown, else GX_OK / GX_ERR_NO_DEVICE
+std::string g_dev_msg;
+std::once_flag g_dev_once;
+
+int require_device() {
+    std::call_once(g_dev_once, [] {
+        int count = 0;
+        cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count <= 0) {
+            cudaGetLastError();
+            g_dev_status = GX_ERR_NO_DEVICE;
+            g_dev_msg = std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0");
+            return;
+        }
+        for (int d = 0; d < count; ++d) {
+            cudaDeviceProp p;
+            if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10 && p.minor == 0) {
+                g_dev_status = GX_OK;
+                return;
+            }
+        }
+        g_dev_status = GX_ERR_NO_DEVICE;
+        g_dev_msg = "no device of compute capability 10.0 (this build targets sm_100a only)";
+    });
+    if (g_dev_status != GX_OK) return fail(GX_ERR_NO_DEVICE, "%s", g_dev_msg.c_str());
+    return GX_OK;
+}
+
+int sm_count(int dev) {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int v = 148;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        v = 148;
+    }
+    cache[dev] = v;
+    return v;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (dev >= 0 && cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// All non-null pointers must be of one kind: *device = true for device/managed memory.
+int classify(std::initializer_list<const void*> ptrs, bool* device, int* dev_id, const char* fn) {
+    int kind = 0;  // 0 unknown, 1 host, 2 device
+    *dev_id = -1;
+    for (const void* p : ptrs) {
+        if (!p) continue;
+        cudaPointerAttributes at;
+        int k = 1;
+        if (cudaPointerGetAttributes(&at, p) == cudaSuccess) {
+            if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+                k = 2;
+                *dev_id = at.device;
+            }
+        } else {
+            cudaGetLastError();
+        }
+        if (kind == 0) kind = k;
+        else if (kind != k)
+            return fail(GX_ERR_INVALID_ARGUMENT, "%s: arrays mix host and device memory", fn);
+    }
+    *device = kind == 2;
+    if (!*device) cudaGetDevice(dev_id);
+    return GX_OK;
+}
+
+bool valid_precision(int p) { return p == kF64 || p == kMixed || p == kF64Exact; }
+
+int check_phys(const gx_physics& ph, const char* fn) {
+    if (!std::isfinite(ph.G) || !std::isfinite(ph.softening) || ph.softening < 0.0)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: G must be finite and softening finite and >= 0", fn);
+    return GX_OK;
+}
+
+bool eps0_of(int precision, const gx_physics& ph) {
+    const double e2 = ph.softening * ph.softening;
+    if (precision == kMixed) return (float)e2 < 1e-24f;
+    return e2 < 1e-200;
+}
+
+// Device scratch obtained from the stream-ordered pool and returned at scope exit.
+struct AsyncBuf {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    ~AsyncBuf() {
+        if (p) cudaFreeAsync(p, st);
+    }
+    int alloc(size_t bytes, cudaStream_t s) {
+        st = s;
+        cudaError_t e = dev_alloc_async(&p, bytes, s);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail_cuda(e, "cudaMallocAsync (scratch)");
+        }
+        return GX_OK;
+    }
+    double* d() const { return (double*)p; }
+};
+
+// ======================================================================================
+// variant choice
+// ======================================================================================
+struct Choice {
+    int variant = -1;
+    int nsplit = 1;
+};
+
+// Source chunking: j_chunk a multiple of jt, nsplit = number of chunks actually used.
+void split_layout(int64_t n_src, int jt, int want, int64_t* chunk, int* nsplit) {
+    if (want < 1) want = 1;
+    int64_t c = (n_src + want - 1) / want;
+    c = ((c + jt - 1) / jt) * jt;
+    if (c < jt) c = jt;
+    *chunk = c;
+    *nsplit = (int)std::max<int64_t>(1, (n_src + c - 1) / c);
+}
+
+// Predicted time of (variant, nsplit) in units of "one SM running one source against one
+// target at full rate".  The CTAs are spread evenly over the SMs (L per SM); an SM runs
+// them in rounds of `occupancy` concurrent CTAs, and a round with fewer CTAs than needed to
+// cover latency (about 12 warps) runs at a proportionally lower rate.
+double split_cost(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int ns, int sms) {
+    const int64_t tile = (int64_t)v.block * v.ipt;
+    const int64_t T = (n_tgt + tile - 1) / tile;
+    const int occ = force_occupancy(v);
+    int64_t chunk;
+    int nse;
+    split_layout(n_src, v.jt, ns, &chunk, &nse);
+    const int64_t L = (T * nse + sms - 1) / sms;
+    const double W = (double)tile * (double)(chunk + v.jt);
+    const double warps = v.block / 32.0;
+    auto eff = [&](int64_t c) { return std::min(1.0, (double)c * warps / 12.0); };
+    const int64_t full = L / occ, rem = L % occ;
+    double t = (double)full * (double)occ * W / eff(occ);
+    if (rem) t += (double)rem * W / eff(rem);
+    // the ordered reduction pass reads nse partials per target
+    if (nse > 1) t += 0.05 * (double)nse * (double)n_tgt * 64.0 / sms;
+    return t;
+}
+
+int best_split(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int sms) {
+    if (v.precision == kF64Exact) return 1;
+    int best = 1;
+    double bc = split_cost(v, n_tgt, n_src, 1, sms);
+    for (int ns = 2; ns <= 64; ++ns) {
+        int64_t chunk;
+        int nse;
+        split_layout(n_src, v.jt, ns, &chunk, &nse);
+        if (nse != ns) continue;
+        const double c = split_cost(v, n_tgt, n_src, ns, sms);
+        if (c < bc * 0.995) {
+            bc = c;
+            best = ns;
+        }
+    }
+    return best;
+}
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int64_t>, Choice> g_tuned;  // (device, precision, eps0, n)
+
+// Untuned choice: the wave model over all variants of the precision, with a small penalty
+// for every variant but the first (the one measured fastest per interaction on B200).
+Choice heuristic_choice(int dev, int precision, bool eps0, int64_t n_tgt, int64_t n_src) {
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find(std::make_tuple(dev, precision, (int)eps0, n_src));
+        if (it != g_tuned.end() && n_tgt == n_src) return it->second;
+    }
+    int ids[32];
+    const int c = std::min(32, force_variant_ids(precision, eps0 ? 1 : 0, ids, 32));
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    const int sms = sm_count(dev);
+    Choice best;
+    double bc = 1e300;
+    for (int k = 0; k < c; ++k) {
+        const ForceVariant& v = all[ids[k]];
+        if (precision == kMixed && !v.packed) continue;  // the scalar form is kept for measurement only
+        const int ns = best_split(v, n_tgt, n_src, sms);
+        const double cost = split_cost(v, n_tgt, n_src, ns, sms) * (k == 0 ? 1.0 : 1.08);
+        if (cost < bc) {
+            bc = cost;
+            best.variant = ids[k];
+            best.nsplit = ns;
+        }
+    }
+    return best;
+}
+
+// ======================================================================================
+// force evaluation on device pointers
+// ======================================================================================
+struct ForceJob {
+    const double *x, *y, *z, *m;
+    int64_t n_src;
+    const int64_t* tgt_idx;
+    int64_t t_begin, n_tgt;
+    double *ax, *ay, *az;
+    double *vx, *vy, *vz;
+    double kick_dt;
+};
+
+ForceArgs make_args(const ForceJob& j, const gx_physics& ph, const ForceVariant& v, int nsplit,
+                    double* part) {
+    ForceArgs a;
+    a.x = j.x;
+    a.y = j.y;
+    a.z = j.z;
+    a.m = j.m;
+    a.n_src = j.n_src;
+    a.tgt_idx = j.tgt_idx;
+    a.t_begin = j.t_begin;
+    a.n_tgt = j.n_tgt;
+    int ns = nsplit;
+    split_layout(j.n_src, v.jt, nsplit, &a.j_chunk, &ns);
+    a.nsplit = ns;
+    a.ax = j.ax;
+    a.ay = j.ay;
+    a.az = j.az;
+    a.part = part;
+    a.vx = j.vx;
+    a.vy = j.vy;
+    a.vz = j.vz;
+    a.kick_dt = j.kick_dt;
+    a.G = ph.G;
+    a.eps2 = ph.softening * ph.softening;
+    a.eps2f = (float)a.eps2;
+    return a;
+}
+
+size_t part_bytes(const ForceVariant& v, int64_t n_src, int64_t n_tgt, int nsplit) {
+    int64_t chunk;
+    int ns;
+    split_layout(n_src, v.jt, nsplit, &chunk, &ns);
+    return ns > 1 ? (size_t)ns * 3 * (size_t)n_tgt * sizeof(double) : 0;
+}
+
+// Runs one force evaluation with scratch from `part` (or a stream-ordered allocation).
+int run_force(const ForceJob& j, const gx_physics& ph, int precision, Choice ch, int dev,
+              cudaStream_t st, double* part, size_t part_cap) {
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    const bool eps0 = eps0_of(precision, ph);
+    if (ch.variant < 0) ch = heuristic_choice(dev, precision, eps0, j.n_tgt, j.n_src);
+    const ForceVariant& v = all[ch.variant];
+    const size_t need = part_bytes(v, j.n_src, j.n_tgt, ch.nsplit);
+    AsyncBuf tmp;
+    if (need > part_cap) {
+        GX_TRY(tmp.alloc(need, st));
+        part = tmp.d();
+    }
+    const ForceArgs a = make_args(j, ph, v, ch.nsplit, part);
+    GX_CUDA(force_launch(v, a, st));
+    return GX_OK;
+}
+
+// ======================================================================================
+// host staging helpers
+// ======================================================================================
+struct HostStage {
+    cudaStream_t st;
+    std::vector<AsyncBuf> bufs;
+    explicit HostStage(cudaStream_t s) : st(s) {}
+    // Device copy of a host array (nullptr stays nullptr).
+    int in(const double* h, int64_t n, double** d) {
+        if (!h) {
+            *d = nullptr;
+            return GX_OK;
+        }
+        bufs.emplace_back();
+        GX_TRY(bufs.back().alloc((size_t)std::max<int64_t>(n, 1) * sizeof(double), st));
+        *d = bufs.back().d();
+        if (n > 0) GX_CUDA(cudaMemcpyAsync(*d, h, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+        return GX_OK;
+    }
+    int out(double** d, int64_t n) {
+        bufs.emplace_back();
+        GX_TRY(bufs.back().alloc((size_t)std::max<int64_t>(n, 1) * sizeof(double), st));
+        *d = bufs.back().d();
+        return GX_OK;
+    }
+    template <typename T>
+    int in_any(const T* h, int64_t n, T** d) {
+        if (!h) {
+            *d = nullptr;
+            return GX_OK;
+        }
+        bufs.emplace_back();
+        GX_TRY(bufs.back().alloc((size_t)std::max<int64_t>(n, 1) * sizeof(T), st));
+        *d = (T*)bufs.back().p;
+        if (n > 0) GX_CUDA(cudaMemcpyAsync(*d, h, (size_t)n * sizeof(T), cudaMemcpyHostToDevice, st));
+        return GX_OK;
+    }
+};
+
+int copy_back(double* h, const double* d, int64_t n, cudaStream_t st) {
+    if (h && n > 0) GX_CUDA(cudaMemcpyAsync(h, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    return GX_OK;
+}
+
+}  // namespace
+
+// ======================================================================================
+// library
+// ======================================================================================
+extern "C" int gxi_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
+extern "C" const char* gx_last_error(void) { return g_err.c_str(); }
+
+extern "C" int gx_abi_version(void) { return GX_ABI_VERSION; }
+
+extern "C" int gx_device_available(int* available) {
+    if (!available) return fail(GX_ERR_INVALID_ARGUMENT, "gx_device_available: null pointer");
+    *available = require_device() == GX_OK ? 1 : 0;
+    return GX_OK;
+}
+
+extern "C" int gx_debug_fail_allocations(int count) {
+    g_fail_allocs.store(count < 0 ? 0 : count);
+    return GX_OK;
+}
+
+extern "C" int gx_variant_count(int precision, int* count) {
+    if (!count || !valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_variant_count: bad arguments");
+    int ids[64];
+    *count = force_variant_ids(precision, 0, ids, 64);
+    if (precision != kF64Exact) *count += force_variant_ids(precision, 1, ids, 64);
+    return GX_OK;
+}
+
+extern "C" int gx_variant_describe(int precision, int variant, char* buf, int buflen) {
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    if (!buf || buflen <= 0 || variant < 0 || variant >= cnt || all[variant].precision != precision)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_variant_describe: bad arguments");
+    const ForceVariant& v = all[variant];
+    const char* p = v.precision == kMixed ? "mixed" : v.precision == kF64 ? "f64" : "f64-exact";
+    snprintf(buf, (size_t)buflen, "%s block=%d ipt=%d jt=%d%s%s", p, v.block, v.ipt, v.jt,
+             v.packed ? " f32x2" : "", v.eps0 && v.precision != kF64Exact ? " eps0" : "");
+    return GX_OK;
+}
+
+// ======================================================================================
+// stateless direct sum
+// ======================================================================================
+static int direct_common(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                         int64_t begin, int64_t end, const int64_t* targets, int64_t n_targets,
+                         gx_physics phys, int precision, double* ax, double* ay, double* az, void* stream,
+                         const char* fn) {
+    if (n < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n < 0", fn);
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision %d", fn, precision);
+    GX_TRY(check_phys(phys, fn));
+    const int64_t nt = targets ? n_targets : end - begin;
+    if (!targets && (begin < 0 || end < begin || end > n))
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: need 0 <= begin <= end <= n", fn);
+    if (targets && n_targets < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n_targets < 0", fn);
+    if (nt > 0 && (!x || !y || !z || !m || !ax || !ay || !az))
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    if (nt == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, ax, ay, az, targets}, &device, &dev, fn));
+    DeviceGuard guard(dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (device) {
+        ForceJob j{x, y, z, m, n, targets, targets ? 0 : begin, nt, ax, ay, az, nullptr, nullptr, nullptr, 0.0};
+        return run_force(j, phys, precision, Choice(), dev, st, nullptr, 0);
+    }
+    if (targets) {
+        for (int64_t k = 0; k < n_targets; ++k)
+            if (targets[k] < 0 || targets[k] >= n) return fail(GX_ERR_INVALID_ARGUMENT, "%s: target index out of range", fn);
+    }
+    HostStage hs(st);
+    double *dx, *dy, *dz, *dm, *dax, *day, *daz;
+    int64_t* dt = nullptr;
+    GX_TRY(hs.in(x, n, &dx));
+    GX_TRY(hs.in(y, n, &dy));
+    GX_TRY(hs.in(z, n, &dz));
+    GX_TRY(hs.in(m, n, &dm));
+    GX_TRY(hs.in_any(targets, n_targets, &dt));
+    GX_TRY(hs.out(&dax, nt));
+    GX_TRY(hs.out(&day, nt));
+    GX_TRY(hs.out(&daz, nt));
+    ForceJob j{dx, dy, dz, dm, n, dt, targets ? 0 : begin, nt, dax, day, daz, nullptr, nullptr, nullptr, 0.0};
+    GX_TRY(run_force(j, phys, precision, Choice(), dev, st, nullptr, 0));
+    GX_TRY(copy_back(ax, dax, nt, st));
+    GX_TRY(copy_back(ay, day, nt, st));
+    GX_TRY(copy_back(az, daz, nt, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    return GX_OK;
+}
+
+extern "C" int gx_direct_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                               gx_physics phys, int precision, double* ax, double* ay, double* az,
+                               void* stream) {
+    GX_GUARD_BEGIN
+    return direct_common(n, x, y, z, m, 0, n, nullptr, 0, phys, precision, ax, ay, az, stream, "gx_direct_accel");
+    GX_GUARD_END
+}
+
+extern "C" int gx_direct_accel_targets(int64_t n, const double* x, const double* y, const double* z,
+                                       const double* m, int64_t begin, int64_t end, const int64_t* targets,
+                                       int64_t n_targets, gx_physics phys, int precision, double* ax,
+                                       double* ay, double* az, void* stream) {
+    GX_GUARD_BEGIN
+    return direct_common(n, x, y, z, m, begin, end, targets, n_targets, phys, precision, ax, ay, az, stream,
+                         "gx_direct_accel_targets");
+    GX_GUARD_END
+}
+
+// ======================================================================================
+// integration
+// ======================================================================================
+extern "C" int gx_kick(int64_t n, double* vx, double* vy, double* vz, const double* ax, const double* ay,
+                       const double* az, double dt, void* stream) {
+    GX_GUARD_BEGIN
+    if (n < 0 || (n > 0 && (!vx || !vy || !vz || !ax || !ay || !az)))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_kick: bad arguments");
+    GX_TRY(require_device());
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({vx, vy, vz, ax, ay, az}, &device, &dev, "gx_kick"));
+    if (!device) return fail(GX_ERR_INVALID_ARGUMENT, "gx_kick: device arrays only");
+    DeviceGuard g(dev);
+    GX_CUDA(launch_kick(n, vx, vy, vz, ax, ay, az, dt, (cudaStream_t)stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_drift(int64_t n, double* x, double* y, double* z, const double* vx, const double* vy,
+                        const double* vz, double dt, void* stream) {
+    GX_GUARD_BEGIN
+    if (n < 0 || (n > 0 && (!x || !y || !z || !vx || !vy || !vz)))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_drift: bad arguments");
+    GX_TRY(require_device());
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz}, &device, &dev, "gx_drift"));
+    if (!device) return fail(GX_ERR_INVALID_ARGUMENT, "gx_drift: device arrays only");
+    DeviceGuard g(dev);
+    GX_CUDA(launch_drift(n, x, y, z, vx, vy, vz, dt, (cudaStream_t)stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_kick_drift(int64_t n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             const double* ax, const double* ay, const double* az, double kick_dt,
+                             double drift_dt, void* stream) {
+    GX_GUARD_BEGIN
+    if (n < 0 || (n > 0 && (!x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az)))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_kick_drift: bad arguments");
+    GX_TRY(require_device());
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, ax, ay, az}, &device, &dev, "gx_kick_drift"));
+    if (!device) return fail(GX_ERR_INVALID_ARGUMENT, "gx_kick_drift: device arrays only");
+    DeviceGuard g(dev);
+    GX_CUDA(launch_kick_drift(n, x, y, z, vx, vy, vz, ax, ay, az, kick_dt, drift_dt, (cudaStream_t)stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+// One KDK step on device arrays: kick(dt/2) + drift(dt), force with the closing kick fused.
+static int kdk_device(int64_t n, double* x, double* y, double* z, double* vx, double* vy, double* vz, double* ax,
+                      double* ay, double* az, const double* m, double dt, const gx_physics& phys, int precision,
+                      Choice ch, int dev, cudaStream_t st, double* part, size_t part_cap) {
+    const double half = 0.5 * dt;
+    GX_CUDA(launch_kick_drift(n, x, y, z, vx, vy, vz, ax, ay, az, half, dt, st));
+    ForceJob j{x, y, z, m, n, nullptr, 0, n, ax, ay, az, vx, vy, vz, half};
+    return run_force(j, phys, precision, ch, dev, st, part, part_cap);
+}
+
+extern "C" int gx_leapfrog_step(int64_t n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                                double* ax, double* ay, double* az, const double* m, double dt, gx_physics phys,
+                                int precision, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_leapfrog_step";
+    if (n < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n < 0", fn);
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
+    if (!std::isfinite(dt)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: dt must be finite", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (n > 0 && (!x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az || !m))
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, ax, ay, az, m}, &device, &dev, fn));
+    DeviceGuard g(dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (device) return kdk_device(n, x, y, z, vx, vy, vz, ax, ay, az, m, dt, phys, precision, Choice(), dev, st, nullptr, 0);
+    HostStage hs(st);
+    double* d[10];
+    const double* h[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
+    for (int k = 0; k < 10; ++k) GX_TRY(hs.in(h[k], n, &d[k]));
+    GX_TRY(kdk_device(n, d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8], d[9], dt, phys, precision, Choice(),
+                      dev, st, nullptr, 0));
+    double* o[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    for (int k = 0; k < 9; ++k) GX_TRY(copy_back(o[k], d[k], n, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+static void fill_diag(const double* v, gx_diagnostics* out) {
+    out->total_mass = v[0];
+    out->kinetic_energy = v[1];
+    out->potential_energy = v[2];
+    out->total_energy = v[3];
+    for (int c = 0; c < 3; ++c) {
+        out->momentum[c] = v[4 + c];
+        out->center_of_mass[c] = v[7 + c];
+        out->angular_momentum[c] = v[10 + c];
+    }
+}
+
+extern "C" int gx_diagnostics_compute(int64_t n, const double* x, const double* y, const double* z,
+                                      const double* vx, const double* vy, const double* vz, const double* m,
+                                      gx_physics phys, gx_diagnostics* out, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_diagnostics_compute";
+    if (n < 0 || !out) return fail(GX_ERR_INVALID_ARGUMENT, "%s: bad arguments", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (n > 0 && (!x || !y || !z || !vx || !vy || !vz || !m)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    std::memset(out, 0, sizeof(*out));
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, m}, &device, &dev, fn));
+    DeviceGuard g(dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    HostStage hs(st);
+    const double* d[7] = {x, y, z, vx, vy, vz, m};
+    if (!device) {
+        for (int k = 0; k < 7; ++k) {
+            double* p;
+            GX_TRY(hs.in(d[k], n, &p));
+            d[k] = p;
+        }
+    }
+    AsyncBuf scratch;
+    GX_TRY(scratch.alloc(diagnostics_scratch_bytes(n) + 16 * sizeof(double), st));
+    double* res = scratch.d();
+    double* work = res + 16;
+    GX_CUDA(launch_diagnostics(n, d[0], d[1], d[2], d[3], d[4], d[5], d[6], phys.G,
+                               phys.softening * phys.softening, work, res, st));
+    double h[13];
+    GX_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    fill_diag(h, out);
+    return GX_OK;
+    GX_GUARD_END
+}
+
+// ======================================================================================
+// resident session
+// ======================================================================================
+struct gx_session {
+    int device = 0;
+    int64_t n = 0;
+    gx_physics phys{1.0, 0.02};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double* buf = nullptr;  // 10 * n doubles
+    double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az, *m;
+    double* part = nullptr;
+    size_t part_cap = 0;
+    double* diag = nullptr;  // device: 16 result slots + diagnostics scratch
+    size_t diag_cap = 0;
+    double* host_diag = nullptr;  // pinned, 16 doubles
+    Choice cfg[3];
+    std::map<std::tuple<int64_t, uint64_t, int, int, int>, cudaGraphExec_t> graphs;
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    double timed_ms = 0.0;
+    int64_t timed_launches = 0;
+
+    void clear_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+};
+
+namespace {
+
+int session_choice(gx_session* s, int precision, Choice* out) {
+    if (s->cfg[precision].variant < 0) {
+        s->cfg[precision] = heuristic_choice(s->device, precision, eps0_of(precision, s->phys), s->n, s->n);
+    }
+    *out = s->cfg[precision];
+    return GX_OK;
+}
+
+int session_ensure_part(gx_session* s, const Choice& ch) {
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    const size_t need = part_bytes(all[ch.variant], s->n, s->n, ch.nsplit);
+    if (need <= s->part_cap) return GX_OK;
+    if (s->part) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->part);
+        s->part = nullptr;
+        s->part_cap = 0;
+    }
+    void* p;
+    cudaError_t e = dev_alloc(&p, need);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc (session j-split scratch)");
+    s->part = (double*)p;
+    s->part_cap = need;
+    return GX_OK;
+}
+
+int flush_events(gx_session* s) {
+    if (s->events.empty()) return GX_OK;
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto& ev : s->events) {
+        float ms = 0.f;
+        GX_CUDA(cudaEventElapsedTime(&ms, ev.first, ev.second));
+        s->timed_ms += ms;
+        s->timed_launches += 1;
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    s->events.clear();
+    return GX_OK;
+}
+
+// Force evaluation of the session (closing kick when kick_dt != 0), timed on request.
+int session_force(gx_session* s, int precision, double kick_dt) {
+    Choice ch;
+    GX_TRY(session_choice(s, precision, &ch));
+    GX_TRY(session_ensure_part(s, ch));
+    ForceJob j{s->x, s->y, s->z, s->m, s->n, nullptr, 0, s->n, s->ax, s->ay, s->az,
+               kick_dt != 0.0 ? s->vx : nullptr, kick_dt != 0.0 ? s->vy : nullptr,
+               kick_dt != 0.0 ? s->vz : nullptr, kick_dt};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s->timing) {
+        GX_CUDA(cudaEventCreate(&e0));
+        GX_CUDA(cudaEventCreate(&e1));
+        GX_CUDA(cudaEventRecord(e0, s->stream));
+    }
+    const int r = run_force(j, s->phys, precision, ch, s->device, s->stream, s->part, s->part_cap);
+    if (s->timing) {
+        GX_CUDA(cudaEventRecord(e1, s->stream));
+        s->events.emplace_back(e0, e1);
+    }
+    return r;
+}
+
+int session_enqueue_steps(gx_session* s, int64_t k, double dt, int precision) {
+    const double half = 0.5 * dt;
+    for (int64_t i = 0; i < k; ++i) {
+        GX_CUDA(launch_kick_drift(s->n, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, half, dt,
+                                  s->stream));
+        GX_TRY(session_force(s, precision, half));
+    }
+    return GX_OK;
+}
+
+int session_graph(gx_session* s, int64_t k, double dt, int precision, cudaGraphExec_t* out) {
+    Choice ch;
+    GX_TRY(session_choice(s, precision, &ch));
+    GX_TRY(session_ensure_part(s, ch));
+    uint64_t dtb;
+    std::memcpy(&dtb, &dt, sizeof(dtb));
+    const auto key = std::make_tuple(k, dtb, precision, ch.variant, ch.nsplit);
+    auto it = s->graphs.find(key);
+    if (it != s->graphs.end()) {
+        *out = it->second;
+        return GX_OK;
+    }
+    GX_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int r = session_enqueue_steps(s, k, dt, precision);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (r != GX_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return r;
+    }
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture (session steps)");
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGraphInstantiate (session steps)");
+    if (s->graphs.size() > 32) s->clear_graphs();
+    s->graphs[key] = exec;
+    *out = exec;
+    return GX_OK;
+}
+
+int check_session(gx_session* s, const char* fn) {
+    if (!s) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null session", fn);
+    return GX_OK;
+}
+
+}  // namespace
+
+extern "C" int gx_session_create(int64_t n, gx_physics phys, int device, gx_session** out) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_session_create";
+    if (!out) return fail(GX_ERR_INVALID_ARGUMENT, "%s: out is null", fn);
+    *out = nullptr;
+    if (n < 1) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n must be >= 1", fn);
+    GX_TRY(check_phys(phys, fn));
+    GX_TRY(require_device());
+    int count = 0;
+    GX_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(GX_ERR_INVALID_ARGUMENT, "%s: device %d out of range", fn, device);
+    DeviceGuard g(device);
+    gx_session* s = new gx_session();
+    s->device = device;
+    s->n = n;
+    s->phys = phys;
+    void* p = nullptr;
+    cudaError_t e = dev_alloc(&p, (size_t)n * 10 * sizeof(double));
+    if (e != cudaSuccess) {
+        delete s;
+        return fail_cuda(e, "cudaMalloc (session state)");
+    }
+    s->buf = (double*)p;
+    double** arr[10] = {&s->x, &s->y, &s->z, &s->vx, &s->vy, &s->vz, &s->ax, &s->ay, &s->az, &s->m};
+    for (int k = 0; k < 10; ++k) *arr[k] = s->buf + (size_t)k * (size_t)n;
+    s->diag_cap = diagnostics_scratch_bytes(n) + 16 * sizeof(double);
+    e = dev_alloc(&p, s->diag_cap);
+    if (e == cudaSuccess) s->diag = (double*)p;
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->host_diag, 16 * sizeof(double));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->buf, 0, (size_t)n * 10 * sizeof(double), s->stream);
+    if (e != cudaSuccess) {
+        const int r = fail_cuda(e, "gx_session_create");
+        if (s->diag) cudaFree(s->diag);
+        if (s->host_diag) cudaFreeHost(s->host_diag);
+        cudaFree(s->buf);
+        delete s;
+        return r;
+    }
+    s->own_stream = true;
+    *out = s;
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_destroy(gx_session* s) {
+    GX_GUARD_BEGIN
+    if (!s) return GX_OK;
+    DeviceGuard g(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto& ev : s->events) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    s->clear_graphs();
+    if (s->part) cudaFree(s->part);
+    if (s->diag) cudaFree(s->diag);
+    if (s->host_diag) cudaFreeHost(s->host_diag);
+    if (s->buf) cudaFree(s->buf);
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_set_stream(gx_session* s, void* stream) {
+    GX_TRY(check_session(s, "gx_session_set_stream"));
+    DeviceGuard g(s->device);
+    cudaStreamSynchronize(s->stream);
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    s->own_stream = false;
+    s->stream = (cudaStream_t)stream;
+    return GX_OK;
+}
+
+extern "C" int gx_session_get_stream(gx_session* s, void** stream) {
+    GX_TRY(check_session(s, "gx_session_get_stream"));
+    if (!stream) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_get_stream: null");
+    *stream = (void*)s->stream;
+    return GX_OK;
+}
+
+extern "C" int gx_session_set_state(gx_session* s, const double* x, const double* y, const double* z,
+                                    const double* vx, const double* vy, const double* vz, const double* m,
+                                    const double* ax, const double* ay, const double* az) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_session_set_state";
+    GX_TRY(check_session(s, fn));
+    if (!x || !y || !z || !vx || !vy || !vz || !m) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    if ((ax || ay || az) && !(ax && ay && az)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: give all of ax, ay, az or none", fn);
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, m, ax, ay, az}, &device, &dev, fn));
+    DeviceGuard g(s->device);
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const double* src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
+    double* dst[10] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m};
+    const size_t bytes = (size_t)s->n * sizeof(double);
+    for (int k = 0; k < 10; ++k) {
+        if (src[k]) GX_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, kind, s->stream));
+        else GX_CUDA(cudaMemsetAsync(dst[k], 0, bytes, s->stream));
+    }
+    if (!device) GX_CUDA(cudaStreamSynchronize(s->stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_get_state(gx_session* s, double* x, double* y, double* z, double* vx, double* vy,
+                                    double* vz, double* ax, double* ay, double* az) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_session_get_state";
+    GX_TRY(check_session(s, fn));
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, ax, ay, az}, &device, &dev, fn));
+    DeviceGuard g(s->device);
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    double* dst[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    const double* src[9] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
+    const size_t bytes = (size_t)s->n * sizeof(double);
+    for (int k = 0; k < 9; ++k)
+        if (dst[k]) GX_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, kind, s->stream));
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_device_arrays(gx_session* s, double** p) {
+    GX_TRY(check_session(s, "gx_session_device_arrays"));
+    if (!p) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_device_arrays: null");
+    double* a[10] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m};
+    for (int k = 0; k < 10; ++k) p[k] = a[k];
+    return GX_OK;
+}
+
+extern "C" int gx_session_compute_accelerations(gx_session* s, int precision) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_session(s, "gx_session_compute_accelerations"));
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_compute_accelerations: precision");
+    DeviceGuard g(s->device);
+    return session_force(s, precision, 0.0);
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_step(gx_session* s, int64_t n_steps, double dt, int precision) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_session_step";
+    GX_TRY(check_session(s, fn));
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
+    if (n_steps < 0 || !std::isfinite(dt)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: need n_steps >= 0, finite dt", fn);
+    if (n_steps == 0) return GX_OK;
+    DeviceGuard g(s->device);
+    if (s->timing || s->stream == nullptr) return session_enqueue_steps(s, n_steps, dt, precision);
+    const int64_t chunk = std::min<int64_t>(n_steps, 32);
+    cudaGraphExec_t ge;
+    GX_TRY(session_graph(s, chunk, dt, precision, &ge));
+    const int64_t full = n_steps / chunk, rem = n_steps % chunk;
+    for (int64_t i = 0; i < full; ++i) GX_CUDA(cudaGraphLaunch(ge, s->stream));
+    if (rem) {
+        GX_TRY(session_graph(s, rem, dt, precision, &ge));
+        GX_CUDA(cudaGraphLaunch(ge, s->stream));
+    }
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_diagnostics(gx_session* s, gx_diagnostics* out) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_session(s, "gx_session_diagnostics"));
+    if (!out) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_diagnostics: null");
+    DeviceGuard g(s->device);
+    GX_CUDA(launch_diagnostics(s->n, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->m, s->phys.G,
+                               s->phys.softening * s->phys.softening, s->diag + 16, s->diag, s->stream));
+    GX_CUDA(cudaMemcpyAsync(s->host_diag, s->diag, 13 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    fill_diag(s->host_diag, out);
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_synchronize(gx_session* s) {
+    GX_TRY(check_session(s, "gx_session_synchronize"));
+    DeviceGuard g(s->device);
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    return GX_OK;
+}
+
+extern "C" int gx_session_synchronize_timeout(gx_session* s, double timeout_ms) {
+    GX_TRY(check_session(s, "gx_session_synchronize_timeout"));
+    DeviceGuard g(s->device);
+    cudaEvent_t ev;
+    GX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, s->stream);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(ev);
+        return fail_cuda(e, "cudaEventRecord");
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        e = cudaEventQuery(ev);
+        if (e != cudaErrorNotReady) break;
+        const double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (el > timeout_ms) {
+            cudaEventDestroy(ev);
+            return fail(GX_ERR_TIMEOUT, "gx_session_synchronize_timeout: stream still busy after %.1f ms", timeout_ms);
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaEventQuery");
+    return GX_OK;
+}
+
+extern "C" int gx_session_enable_timing(gx_session* s, int enable) {
+    GX_TRY(check_session(s, "gx_session_enable_timing"));
+    DeviceGuard g(s->device);
+    GX_TRY(flush_events(s));
+    s->timing = enable != 0;
+    s->timed_ms = 0.0;
+    s->timed_launches = 0;
+    return GX_OK;
+}
+
+extern "C" int gx_session_force_timing(gx_session* s, double* total_ms, int64_t* launches) {
+    GX_TRY(check_session(s, "gx_session_force_timing"));
+    DeviceGuard g(s->device);
+    GX_TRY(flush_events(s));
+    if (total_ms) *total_ms = s->timed_ms;
+    if (launches) *launches = s->timed_launches;
+    return GX_OK;
+}
+
+extern "C" int gx_session_get_config(gx_session* s, int precision, int* variant, int* jsplit) {
+    GX_TRY(check_session(s, "gx_session_get_config"));
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_get_config: precision");
+    DeviceGuard g(s->device);
+    Choice ch;
+    GX_TRY(session_choice(s, precision, &ch));
+    if (variant) *variant = ch.variant;
+    if (jsplit) {
+        int cnt;
+        const ForceVariant* all = force_variants(&cnt);
+        int64_t chunk;
+        int ns;
+        split_layout(s->n, all[ch.variant].jt, ch.nsplit, &chunk, &ns);
+        *jsplit = ns;
+    }
+    return GX_OK;
+}
+
+extern "C" int gx_session_set_config(gx_session* s, int precision, int variant, int jsplit) {
+    GX_TRY(check_session(s, "gx_session_set_config"));
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_set_config: precision");
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    const bool eps0 = eps0_of(precision, s->phys);
+    if (variant < 0 || variant >= cnt || all[variant].precision != precision ||
+        (precision != kF64Exact && (bool)all[variant].eps0 != eps0))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_set_config: variant %d does not fit precision %d, softening %g",
+                    variant, precision, s->phys.softening);
+    if (jsplit < 1 || jsplit > 4096 || (precision == kF64Exact && jsplit != 1))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_set_config: jsplit out of range");
+    s->cfg[precision].variant = variant;
+    s->cfg[precision].nsplit = jsplit;
+    return GX_OK;
+}
+
+// ---- autotuner ---------------------------------------------------------------------
+namespace {
+
+// Times `reps` force evaluations of targets [0, n_tgt) with a given choice on the
+// session's state (results go to the session's acceleration array).
+int time_choice(gx_session* s, int precision, Choice ch, int64_t n_tgt, int reps, double* ms_out) {
+    GX_TRY(session_ensure_part(s, ch));
+    ForceJob j{s->x, s->y, s->z, s->m, s->n, nullptr, 0, n_tgt, s->ax, s->ay, s->az, nullptr, nullptr, nullptr, 0.0};
+    GX_TRY(run_force(j, s->phys, precision, ch, s->device, s->stream, s->part, s->part_cap));  // warm-up
+    cudaEvent_t e0, e1;
+    GX_CUDA(cudaEventCreate(&e0));
+    GX_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    for (int r = 0; r < reps; ++r) {
+        GX_CUDA(cudaEventRecord(e0, s->stream));
+        GX_TRY(run_force(j, s->phys, precision, ch, s->device, s->stream, s->part, s->part_cap));
+        GX_CUDA(cudaEventRecord(e1, s->stream));
+        GX_CUDA(cudaEventSynchronize(e1));
+        float ms;
+        GX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, (double)ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_out = best;
+    return GX_OK;
+}
+
+}  // namespace
+
+extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_session_autotune";
+    GX_TRY(check_session(s, fn));
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: precision", fn);
+    DeviceGuard g(s->device);
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    const bool eps0 = eps0_of(precision, s->phys);
+    int ids[32];
+    const int c = std::min(32, force_variant_ids(precision, eps0 ? 1 : 0, ids, 32));
+    const int sms = sm_count(s->device);
+    // Save the accelerations: timing runs overwrite them.
+    void* save = nullptr;
+    GX_CUDA(dev_alloc(&save, (size_t)s->n * 3 * sizeof(double)));
+    GX_CUDA(cudaMemcpyAsync(save, s->ax, (size_t)s->n * 3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    Choice best;
+    double bms = 1e300;
+    int status = GX_OK;
+    for (int k = 0; k < c && status == GX_OK; ++k) {
+        const ForceVariant& v = all[ids[k]];
+        std::vector<int> splits = {best_split(v, s->n, s->n, sms)};
+        if (splits[0] != 1) splits.push_back(1);
+        for (int ns : {2, 4, 8}) {
+            if (std::find(splits.begin(), splits.end(), ns) == splits.end() && (int64_t)ns * v.jt <= s->n) splits.push_back(ns);
+        }
+        for (int ns : splits) {
+            Choice ch{ids[k], ns};
+            double ms;
+            // A large system is timed once per candidate at the model's split only.
+            const bool large = (double)s->n * (double)s->n > 4.0e10;
+            if (large && ns != splits[0]) continue;
+            status = time_choice(s, precision, ch, s->n, large ? 1 : 3, &ms);
+            if (status != GX_OK) break;
+            if (ms < bms) {
+                bms = ms;
+                best = ch;
+            }
+        }
+    }
+    cudaMemcpyAsync(s->ax, save, (size_t)s->n * 3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+    cudaStreamSynchronize(s->stream);
+    cudaFree(save);
+    if (status != GX_OK) return status;
+    if (best.variant < 0) return fail(GX_ERR_UNSUPPORTED, "%s: no candidate variant", fn);
+    s->cfg[precision] = best;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[std::make_tuple(s->device, precision, (int)eps0, s->n)] = best;
+    }
+    s->clear_graphs();
+    if (best_ms) *best_ms = bms;
+    return GX_OK;
+    GX_GUARD_END
+}
+
+// ======================================================================================
+// P2P
+// ======================================================================================
+extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                             int32_t n_leaves, const int32_t* leaf_offsets, const int32_t* leaf_particles,
+                             const int32_t* near_offsets, const int32_t* near_leaves, gx_physics phys,
+                             int precision, double* ax, double* ay, double* az, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_p2p_leaves";
+    if (n < 0 || n_leaves < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: negative size", fn);
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (n_leaves > 0 && (!x || !y || !z || !m || !leaf_offsets || !leaf_particles || !near_offsets || !ax || !ay || !az))
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    if (n_leaves == 0 || n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, leaf_offsets, leaf_particles, near_offsets, near_leaves, ax, ay, az}, &device, &dev, fn));
+    DeviceGuard g(dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    P2PArgs a;
+    a.n_leaves = n_leaves;
+    a.G = phys.G;
+    a.eps2 = phys.softening * phys.softening;
+    a.eps2f = (float)a.eps2;
+    if (device) {
+        a.x = x; a.y = y; a.z = z; a.m = m;
+        a.leaf_off = leaf_offsets; a.leaf_part = leaf_particles; a.near_off = near_offsets; a.near_leaf = near_leaves;
+        a.ax = ax; a.ay = ay; a.az = az;
+        GX_CUDA(launch_p2p(a, precision, st));
+        return GX_OK;
+    }
+    // Host arrays: validate the CSR (the kernel trusts it), then stage.
+    const int32_t n_lp = leaf_offsets[n_leaves];
+    const int32_t n_nl = near_offsets[n_leaves];
+    if (leaf_offsets[0] != 0 || near_offsets[0] != 0 || n_lp < 0 || n_nl < 0)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: CSR offsets must start at 0", fn);
+    for (int32_t l = 0; l < n_leaves; ++l)
+        if (leaf_offsets[l + 1] < leaf_offsets[l] || near_offsets[l + 1] < near_offsets[l])
+            return fail(GX_ERR_INVALID_ARGUMENT, "%s: CSR offsets must be non-decreasing", fn);
+    for (int32_t k = 0; k < n_lp; ++k)
+        if (leaf_particles[k] < 0 || leaf_particles[k] >= n) return fail(GX_ERR_INVALID_ARGUMENT, "%s: body index out of range", fn);
+    for (int32_t k = 0; k < n_nl; ++k)
+        if (near_leaves[k] < 0 || near_leaves[k] >= n_leaves) return fail(GX_ERR_INVALID_ARGUMENT, "%s: leaf id out of range", fn);
+    HostStage hs(st);
+    double *dx, *dy, *dz, *dm, *dax, *day, *daz;
+    int32_t *dlo, *dlp, *dno, *dnl;
+    GX_TRY(hs.in(x, n, &dx));
+    GX_TRY(hs.in(y, n, &dy));
+    GX_TRY(hs.in(z, n, &dz));
+    GX_TRY(hs.in(m, n, &dm));
+    GX_TRY(hs.in(ax, n, &dax));
+    GX_TRY(hs.in(ay, n, &day));
+    GX_TRY(hs.in(az, n, &daz));
+    GX_TRY(hs.in_any(leaf_offsets, (int64_t)n_leaves + 1, &dlo));
+    GX_TRY(hs.in_any(leaf_particles, (int64_t)n_lp, &dlp));
+    GX_TRY(hs.in_any(near_offsets, (int64_t)n_leaves + 1, &dno));
+    GX_TRY(hs.in_any(near_leaves ? near_leaves : leaf_offsets, (int64_t)std::max<int32_t>(n_nl, 1), &dnl));
+    a.x = dx; a.y = dy; a.z = dz; a.m = dm;
+    a.leaf_off = dlo; a.leaf_part = dlp; a.near_off = dno; a.near_leaf = dnl;
+    a.ax = dax; a.ay = day; a.az = daz;
+    GX_CUDA(launch_p2p(a, precision, st));
+    GX_TRY(copy_back(ax, dax, n, st));
+    GX_TRY(copy_back(ay, day, n, st));
+    GX_TRY(copy_back(az, daz, n, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+// ======================================================================================
+// adjoint
+// ======================================================================================
+extern "C" int gx_direct_vjp(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                             const double* lx, const double* ly, const double* lz, gx_physics phys, int precision,
+                             double* gxo, double* gyo, double* gzo, double* gmo, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_direct_vjp";
+    if (n < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n < 0", fn);
+    if (precision != kF64 && precision != kMixed)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: precision must be F64 or MIXED", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (n > 0 && (!x || !y || !z || !m || !lx || !ly || !lz || !gxo || !gyo || !gzo))
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, lx, ly, lz, gxo, gyo, gzo, gmo}, &device, &dev, fn));
+    DeviceGuard g(dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    HostStage hs(st);
+    const double* in[7] = {x, y, z, m, lx, ly, lz};
+    double* out[4] = {gxo, gyo, gzo, gmo};
+    if (!device) {
+        for (int k = 0; k < 7; ++k) {
+            double* p;
+            GX_TRY(hs.in(in[k], n, &p));
+            in[k] = p;
+        }
+        for (int k = 0; k < 4; ++k) {
+            if (!out[k]) continue;
+            double* p;
+            GX_TRY(hs.out(&p, n));
+            out[k] = p;
+        }
+    }
+    VjpArgs a;
+    a.x = in[0]; a.y = in[1]; a.z = in[2]; a.m = in[3]; a.lx = in[4]; a.ly = in[5]; a.lz = in[6];
+    a.n = n;
+    a.gx = out[0]; a.gy = out[1]; a.gz = out[2]; a.gm = out[3];
+    a.G = phys.G;
+    a.eps2 = phys.softening * phys.softening;
+    a.eps2f = (float)a.eps2;
+    // j-split so that at least ~2 waves of CTAs exist.
+    const int sms = sm_count(dev);
+    const int64_t tiles = (n + vjp_tile(precision) - 1) / vjp_tile(precision);
+    int want = (int)std::min<int64_t>(64, std::max<int64_t>(1, (4 * sms + tiles - 1) / tiles));
+    split_layout(n, vjp_jt(precision), want, &a.j_chunk, &a.nsplit);
+    AsyncBuf part;
+    a.part = nullptr;
+    if (a.nsplit > 1) {
+        GX_TRY(part.alloc((size_t)a.nsplit * 4 * (size_t)n * sizeof(double), st));
+        a.part = part.d();
+    }
+    GX_CUDA(launch_vjp(a, precision, st));
+    if (!device) {
+        for (int k = 0; k < 4; ++k)
+            if (out[k]) GX_TRY(copy_back(k == 0 ? gxo : k == 1 ? gyo : k == 2 ? gzo : gmo, out[k], n, st));
+        GX_CUDA(cudaStreamSynchronize(st));
+    }
+    return GX_OK;
+    GX_GUARD_END
+}
+
+// ======================================================================================
+// batched ensembles
+// ======================================================================================
+struct gx_batch {
+    int device = 0;
+    int32_t ni = 0;
+    std::vector<int64_t> off_h;
+    int64_t n = 0;
+    gx_physics phys{1.0, 0.05};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double* buf = nullptr;
+    double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az, *m;
+    int64_t* off_d = nullptr;
+    int2* items_d = nullptr;
+    int n_items = 0;
+    int items_tile = 0;
+    int* counter = nullptr;
+    int cfg[3] = {-1, -1, -1};
+    int2* pot_items_d = nullptr;
+    int n_pot_items = 0;
+    int* pot_first_d = nullptr;
+    int* pot_count_d = nullptr;
+    double* pot_part = nullptr;
+    double* diag_out = nullptr;
+    std::map<std::tuple<int64_t, uint64_t, int, int>, cudaGraphExec_t> graphs;
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    double timed_ms = 0.0;
+    int64_t timed_launches = 0;
+
+    void clear_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+};
+
+namespace {
+
+int batch_default_variant(gx_batch* b, int precision) {
+    if (b->cfg[precision] >= 0) return b->cfg[precision];
+    int ids[16];
+    const int c = batch_variant_ids(precision, eps0_of(precision, b->phys) ? 1 : 0, ids, 16);
+    if (c <= 0) return -1;
+    b->cfg[precision] = ids[0];
+    return ids[0];
+}
+
+// (instance, tile) items for tiles of `tile` targets, largest instances first.
+int batch_build_items(gx_batch* b, int tile) {
+    if (b->items_tile == tile && b->items_d) return GX_OK;
+    std::vector<int> order((size_t)b->ni);
+    for (int i = 0; i < b->ni; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
+        return b->off_h[p + 1] - b->off_h[p] > b->off_h[q + 1] - b->off_h[q];
+    });
+    std::vector<int2> items;
+    for (int inst : order) {
+        const int64_t nb = b->off_h[inst + 1] - b->off_h[inst];
+        const int64_t tiles = (nb + tile - 1) / tile;
+        for (int64_t t = 0; t < tiles; ++t) items.push_back(make_int2(inst, (int)t));
+    }
+    if (items.size() > (size_t)INT32_MAX) return fail(GX_ERR_INVALID_ARGUMENT, "batch: too many work items");
+    if (b->items_d) {
+        cudaStreamSynchronize(b->stream);
+        cudaFree(b->items_d);
+        b->items_d = nullptr;
+    }
+    void* p;
+    cudaError_t e = dev_alloc(&p, std::max<size_t>(1, items.size()) * sizeof(int2));
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc (batch items)");
+    b->items_d = (int2*)p;
+    if (!items.empty())
+        GX_CUDA(cudaMemcpyAsync(b->items_d, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    GX_CUDA(cudaStreamSynchronize(b->stream));
+    b->n_items = (int)items.size();
+    b->items_tile = tile;
+    b->clear_graphs();
+    return GX_OK;
+}
+
+BatchArgs batch_args(gx_batch* b, double kick_dt) {
+    BatchArgs a;
+    a.x = b->x; a.y = b->y; a.z = b->z; a.m = b->m;
+    a.offsets = b->off_d;
+    a.items = b->items_d;
+    a.n_items = b->n_items;
+    a.counter = b->counter;
+    a.ax = b->ax; a.ay = b->ay; a.az = b->az;
+    a.vx = kick_dt != 0.0 ? b->vx : nullptr;
+    a.vy = kick_dt != 0.0 ? b->vy : nullptr;
+    a.vz = kick_dt != 0.0 ? b->vz : nullptr;
+    a.kick_dt = kick_dt;
+    a.G = b->phys.G;
+    a.eps2 = b->phys.softening * b->phys.softening;
+    a.eps2f = (float)a.eps2;
+    return a;
+}
+
+int batch_force(gx_batch* b, int precision, double kick_dt) {
+    const int vid = batch_default_variant(b, precision);
+    if (vid < 0) return fail(GX_ERR_UNSUPPORTED, "batch: precision %d has no batched variant", precision);
+    int cnt;
+    const BatchVariant& v = batch_variants(&cnt)[vid];
+    GX_TRY(batch_build_items(b, v.block * v.ipt));
+    if (b->n_items == 0) return GX_OK;
+    const int grid = std::max(1, std::min(b->n_items, sm_count(b->device) * batch_occupancy(v)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (b->timing) {
+        GX_CUDA(cudaEventCreate(&e0));
+        GX_CUDA(cudaEventCreate(&e1));
+        GX_CUDA(cudaEventRecord(e0, b->stream));
+    }
+    GX_CUDA(batch_force_launch(v, batch_args(b, kick_dt), grid, b->stream));
+    if (b->timing) {
+        GX_CUDA(cudaEventRecord(e1, b->stream));
+        b->events.emplace_back(e0, e1);
+    }
+    return GX_OK;
+}
+
+int batch_enqueue_steps(gx_batch* b, int64_t k, double dt, int precision) {
+    const double half = 0.5 * dt;
+    for (int64_t i = 0; i < k; ++i) {
+        GX_CUDA(launch_kick_drift(b->n, b->x, b->y, b->z, b->vx, b->vy, b->vz, b->ax, b->ay, b->az, half, dt, b->stream));
+        GX_TRY(batch_force(b, precision, half));
+    }
+    return GX_OK;
+}
+
+int batch_flush_events(gx_batch* b) {
+    if (b->events.empty()) return GX_OK;
+    GX_CUDA(cudaStreamSynchronize(b->stream));
+    for (auto& ev : b->events) {
+        float ms = 0.f;
+        GX_CUDA(cudaEventElapsedTime(&ms, ev.first, ev.second));
+        b->timed_ms += ms;
+        b->timed_launches += 1;
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    b->events.clear();
+    return GX_OK;
+}
+
+int check_batch(gx_batch* b, const char* fn) {
+    if (!b) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null batch", fn);
+    return GX_OK;
+}
+
+void batch_release(gx_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& ev : b->events) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    b->clear_graphs();
+    void* ptrs[] = {b->buf, b->off_d, b->items_d, b->counter, b->pot_items_d, b->pot_first_d,
+                    b->pot_count_d, b->pot_part, b->diag_out};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" int gx_batch_create(int32_t n_instances, const int64_t* offsets, gx_physics phys, int device,
+                               gx_batch** out) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_batch_create";
+    if (!out) return fail(GX_ERR_INVALID_ARGUMENT, "%s: out is null", fn);
+    *out = nullptr;
+    if (n_instances < 1 || !offsets) return fail(GX_ERR_INVALID_ARGUMENT, "%s: need n_instances >= 1 and offsets", fn);
+    if (offsets[0] != 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: offsets[0] must be 0", fn);
+    for (int32_t i = 0; i < n_instances; ++i)
+        if (offsets[i + 1] < offsets[i]) return fail(GX_ERR_INVALID_ARGUMENT, "%s: offsets must be non-decreasing", fn);
+    if (offsets[n_instances] < 1) return fail(GX_ERR_INVALID_ARGUMENT, "%s: no bodies", fn);
+    GX_TRY(check_phys(phys, fn));
+    GX_TRY(require_device());
+    int count = 0;
+    GX_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(GX_ERR_INVALID_ARGUMENT, "%s: device %d out of range", fn, device);
+    DeviceGuard g(device);
+    gx_batch* b = new gx_batch();
+    b->device = device;
+    b->ni = n_instances;
+    b->off_h.assign(offsets, offsets + n_instances + 1);
+    b->n = offsets[n_instances];
+    b->phys = phys;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail_cuda(e, "cudaStreamCreate (batch)");
+    }
+    b->own_stream = true;
+    void* p = nullptr;
+    e = dev_alloc(&p, (size_t)b->n * 10 * sizeof(double));
+    if (e == cudaSuccess) {
+        b->buf = (double*)p;
+        double** arr[10] = {&b->x, &b->y, &b->z, &b->vx, &b->vy, &b->vz, &b->ax, &b->ay, &b->az, &b->m};
+        for (int k = 0; k < 10; ++k) *arr[k] = b->buf + (size_t)k * (size_t)b->n;
+        e = dev_alloc(&p, (size_t)(n_instances + 1) * sizeof(int64_t));
+    }
+    if (e == cudaSuccess) {
+        b->off_d = (int64_t*)p;
+        e = dev_alloc(&p, 16);
+    }
+    if (e == cudaSuccess) {
+        b->counter = (int*)p;
+        // diagnostics work lists: tiles of batch_potential_tile() targets, instance order
+        const int pt = batch_potential_tile();
+        std::vector<int2> pitems;
+        std::vector<int> first((size_t)n_instances), cnt((size_t)n_instances);
+        for (int32_t i = 0; i < n_instances; ++i) {
+            const int64_t nb = offsets[i + 1] - offsets[i];
+            first[(size_t)i] = (int)pitems.size();
+            const int64_t tiles = (nb + pt - 1) / pt;
+            for (int64_t t = 0; t < tiles; ++t) pitems.push_back(make_int2(i, (int)t));
+            cnt[(size_t)i] = (int)tiles;
+        }
+        b->n_pot_items = (int)pitems.size();
+        e = dev_alloc(&p, std::max<size_t>(1, pitems.size()) * sizeof(int2));
+        if (e == cudaSuccess) {
+            b->pot_items_d = (int2*)p;
+            e = dev_alloc(&p, (size_t)n_instances * sizeof(int));
+        }
+        if (e == cudaSuccess) {
+            b->pot_first_d = (int*)p;
+            e = dev_alloc(&p, (size_t)n_instances * sizeof(int));
+        }
+        if (e == cudaSuccess) {
+            b->pot_count_d = (int*)p;
+            e = dev_alloc(&p, std::max<size_t>(1, pitems.size()) * sizeof(double));
+        }
+        if (e == cudaSuccess) {
+            b->pot_part = (double*)p;
+            e = dev_alloc(&p, (size_t)n_instances * 13 * sizeof(double));
+        }
+        if (e == cudaSuccess) {
+            b->diag_out = (double*)p;
+            if (!pitems.empty())
+                e = cudaMemcpyAsync(b->pot_items_d, pitems.data(), pitems.size() * sizeof(int2), cudaMemcpyHostToDevice, b->stream);
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->pot_first_d, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->pot_count_d, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->off_d, offsets, (size_t)(n_instances + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->buf, 0, (size_t)b->n * 10 * sizeof(double), b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    }
+    if (e != cudaSuccess) {
+        const int r = fail_cuda(e, "gx_batch_create");
+        batch_release(b);
+        return r;
+    }
+    *out = b;
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_destroy(gx_batch* b) {
+    GX_GUARD_BEGIN
+    if (!b) return GX_OK;
+    DeviceGuard g(b->device);
+    batch_release(b);
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_set_stream(gx_batch* b, void* stream) {
+    GX_TRY(check_batch(b, "gx_batch_set_stream"));
+    DeviceGuard g(b->device);
+    cudaStreamSynchronize(b->stream);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    b->own_stream = false;
+    b->stream = (cudaStream_t)stream;
+    b->clear_graphs();
+    return GX_OK;
+}
+
+extern "C" int gx_batch_set_state(gx_batch* b, const double* x, const double* y, const double* z, const double* vx,
+                                  const double* vy, const double* vz, const double* m) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_batch_set_state";
+    GX_TRY(check_batch(b, fn));
+    if (!x || !y || !z || !vx || !vy || !vz || !m) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, m}, &device, &dev, fn));
+    DeviceGuard g(b->device);
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const double* src[7] = {x, y, z, vx, vy, vz, m};
+    double* dst[7] = {b->x, b->y, b->z, b->vx, b->vy, b->vz, b->m};
+    const size_t bytes = (size_t)b->n * sizeof(double);
+    for (int k = 0; k < 7; ++k) GX_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, kind, b->stream));
+    GX_CUDA(cudaMemsetAsync(b->ax, 0, 3 * bytes, b->stream));
+    GX_CUDA(cudaStreamSynchronize(b->stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_get_state(gx_batch* b, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                                  double* ax, double* ay, double* az) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_batch_get_state";
+    GX_TRY(check_batch(b, fn));
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, vx, vy, vz, ax, ay, az}, &device, &dev, fn));
+    DeviceGuard g(b->device);
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    double* dst[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    const double* src[9] = {b->x, b->y, b->z, b->vx, b->vy, b->vz, b->ax, b->ay, b->az};
+    const size_t bytes = (size_t)b->n * sizeof(double);
+    for (int k = 0; k < 9; ++k)
+        if (dst[k]) GX_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, kind, b->stream));
+    GX_CUDA(cudaStreamSynchronize(b->stream));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_device_arrays(gx_batch* b, double** p) {
+    GX_TRY(check_batch(b, "gx_batch_device_arrays"));
+    if (!p) return fail(GX_ERR_INVALID_ARGUMENT, "gx_batch_device_arrays: null");
+    double* a[10] = {b->x, b->y, b->z, b->vx, b->vy, b->vz, b->ax, b->ay, b->az, b->m};
+    for (int k = 0; k < 10; ++k) p[k] = a[k];
+    return GX_OK;
+}
+
+extern "C" int gx_batch_compute_accelerations(gx_batch* b, int precision) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_batch(b, "gx_batch_compute_accelerations"));
+    if (precision != kF64 && precision != kMixed)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_batch_compute_accelerations: precision must be F64 or MIXED");
+    DeviceGuard g(b->device);
+    return batch_force(b, precision, 0.0);
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_step(gx_batch* b, int64_t n_steps, double dt, int precision) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_batch_step";
+    GX_TRY(check_batch(b, fn));
+    if (precision != kF64 && precision != kMixed) return fail(GX_ERR_INVALID_ARGUMENT, "%s: precision must be F64 or MIXED", fn);
+    if (n_steps < 0 || !std::isfinite(dt)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: need n_steps >= 0, finite dt", fn);
+    if (n_steps == 0) return GX_OK;
+    DeviceGuard g(b->device);
+    if (b->timing || b->stream == nullptr) return batch_enqueue_steps(b, n_steps, dt, precision);
+    const int vid = batch_default_variant(b, precision);
+    if (vid < 0) return fail(GX_ERR_UNSUPPORTED, "%s: no batched variant", fn);
+    int cnt;
+    const BatchVariant& v = batch_variants(&cnt)[vid];
+    GX_TRY(batch_build_items(b, v.block * v.ipt));
+    uint64_t dtb;
+    std::memcpy(&dtb, &dt, sizeof(dtb));
+    // The whole multi-step run is one graph (capped at 1024 steps per graph).
+    const int64_t chunk = std::min<int64_t>(n_steps, 1024);
+    auto get = [&](int64_t k, cudaGraphExec_t* ge) -> int {
+        const auto key = std::make_tuple(k, dtb, precision, vid);
+        auto it = b->graphs.find(key);
+        if (it != b->graphs.end()) {
+            *ge = it->second;
+            return GX_OK;
+        }
+        GX_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const int r = batch_enqueue_steps(b, k, dt, precision);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        if (r != GX_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return r;
+        }
+        if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture (batch)");
+        cudaGraphExec_t exec;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaGraphInstantiate (batch)");
+        if (b->graphs.size() > 16) b->clear_graphs();
+        b->graphs[key] = exec;
+        *ge = exec;
+        return GX_OK;
+    };
+    cudaGraphExec_t ge;
+    GX_TRY(get(chunk, &ge));
+    for (int64_t i = 0; i < n_steps / chunk; ++i) GX_CUDA(cudaGraphLaunch(ge, b->stream));
+    if (n_steps % chunk) {
+        GX_TRY(get(n_steps % chunk, &ge));
+        GX_CUDA(cudaGraphLaunch(ge, b->stream));
+    }
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_diagnostics(gx_batch* b, gx_diagnostics* out) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_batch(b, "gx_batch_diagnostics"));
+    if (!out) return fail(GX_ERR_INVALID_ARGUMENT, "gx_batch_diagnostics: null");
+    DeviceGuard g(b->device);
+    BatchArgs a = batch_args(b, 0.0);
+    a.items = b->pot_items_d;
+    a.n_items = b->n_pot_items;
+    GX_CUDA(batch_diagnostics_launch(a, b->n_pot_items, b->ni, b->vx, b->vy, b->vz, b->pot_first_d, b->pot_count_d,
+                                     b->pot_part, b->diag_out, b->stream));
+    std::vector<double> h((size_t)b->ni * 13);
+    GX_CUDA(cudaMemcpyAsync(h.data(), b->diag_out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    GX_CUDA(cudaStreamSynchronize(b->stream));
+    for (int32_t i = 0; i < b->ni; ++i) fill_diag(h.data() + (size_t)i * 13, out + i);
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_synchronize(gx_batch* b) {
+    GX_TRY(check_batch(b, "gx_batch_synchronize"));
+    DeviceGuard g(b->device);
+    GX_CUDA(cudaStreamSynchronize(b->stream));
+    return GX_OK;
+}
+
+extern "C" int gx_batch_get_config(gx_batch* b, int precision, int* variant) {
+    GX_TRY(check_batch(b, "gx_batch_get_config"));
+    if ((precision != kF64 && precision != kMixed) || !variant)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_batch_get_config: bad arguments");
+    *variant = batch_default_variant(b, precision);
+    return GX_OK;
+}
+
+extern "C" int gx_batch_set_config(gx_batch* b, int precision, int variant) {
+    GX_TRY(check_batch(b, "gx_batch_set_config"));
+    int cnt;
+    const BatchVariant* all = batch_variants(&cnt);
+    if ((precision != kF64 && precision != kMixed) || variant < 0 || variant >= cnt ||
+        all[variant].precision != precision || (bool)all[variant].eps0 != eps0_of(precision, b->phys))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_batch_set_config: variant does not fit");
+    b->cfg[precision] = variant;
+    b->clear_graphs();
+    return GX_OK;
+}
+
+extern "C" int gx_batch_autotune(gx_batch* b, int precision, double* best_ms) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_batch_autotune";
+    GX_TRY(check_batch(b, fn));
+    if (precision != kF64 && precision != kMixed) return fail(GX_ERR_INVALID_ARGUMENT, "%s: precision", fn);
+    DeviceGuard g(b->device);
+    int ids[16];
+    const int c = std::min(16, batch_variant_ids(precision, eps0_of(precision, b->phys) ? 1 : 0, ids, 16));
+    const bool was_timing = b->timing;
+    b->timing = false;
+    cudaEvent_t e0, e1;
+    GX_CUDA(cudaEventCreate(&e0));
+    GX_CUDA(cudaEventCreate(&e1));
+    int best = -1;
+    double bms = 1e300;
+    int status = GX_OK;
+    for (int k = 0; k < c && status == GX_OK; ++k) {
+        b->cfg[precision] = ids[k];
+        status = batch_force(b, precision, 0.0);  // warm-up (and item rebuild)
+        double t = 1e300;
+        for (int r = 0; r < 2 && status == GX_OK; ++r) {
+            cudaEventRecord(e0, b->stream);
+            status = batch_force(b, precision, 0.0);
+            cudaEventRecord(e1, b->stream);
+            cudaEventSynchronize(e1);
+            float ms;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t = std::min(t, (double)ms);
+        }
+        if (status == GX_OK && t < bms) {
+            bms = t;
+            best = ids[k];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->timing = was_timing;
+    if (status != GX_OK) return status;
+    b->cfg[precision] = best;
+    b->clear_graphs();
+    // accelerations must describe the state again
+    GX_TRY(batch_force(b, precision, 0.0));
+    if (best_ms) *best_ms = bms;
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_batch_enable_timing(gx_batch* b, int enable) {
+    GX_TRY(check_batch(b, "gx_batch_enable_timing"));
+    DeviceGuard g(b->device);
+    GX_TRY(batch_flush_events(b));
+    b->timing = enable != 0;
+    b->timed_ms = 0.0;
+    b->timed_launches = 0;
+    return GX_OK;
+}
+
+extern "C" int gx_batch_force_timing(gx_batch* b, double* total_ms, int64_t* launches) {
+    GX_TRY(check_batch(b, "gx_batch_force_timing"));
+    DeviceGuard g(b->device);
+    GX_TRY(batch_flush_events(b));
+    if (total_ms) *total_ms = b->timed_ms;
+    if (launches) *launches = b->timed_launches;
+    return GX_OK;
+}
+
+extern "C" int gx_batch_accel(int32_t n_instances, const int64_t* offsets, const double* x, const double* y,
+                              const double* z, const double* m, gx_physics phys, int precision, double* ax,
+                              double* ay, double* az, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_batch_accel";
+    if (n_instances < 1 || !offsets || !x || !y || !z || !m || !ax || !ay || !az)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: bad arguments", fn);
+    if (precision != kF64 && precision != kMixed) return fail(GX_ERR_INVALID_ARGUMENT, "%s: precision must be F64 or MIXED", fn);
+    GX_TRY(require_device());
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, ax, ay, az}, &device, &dev, fn));
+    int cur = 0;
+    cudaGetDevice(&cur);
+    gx_batch* b = nullptr;
+    GX_TRY(gx_batch_create(n_instances, offsets, phys, device ? dev : cur, &b));
+    int r = GX_OK;
+    {
+        DeviceGuard g(b->device);
+        const int64_t n = b->n;
+        const cudaMemcpyKind kin = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        const cudaMemcpyKind kout = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        cudaStream_t st = (cudaStream_t)stream;
+        // Order the batch's own stream after the caller's stream.
+        cudaEvent_t ev;
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, ev, 0);
+        const double* src[4] = {x, y, z, m};
+        double* dst[4] = {b->x, b->y, b->z, b->m};
+        for (int k = 0; k < 4 && e == cudaSuccess; ++k)
+            e = cudaMemcpyAsync(dst[k], src[k], (size_t)n * sizeof(double), kin, b->stream);
+        if (e != cudaSuccess) r = fail_cuda(e, fn);
+        if (r == GX_OK) r = batch_force(b, precision, 0.0);
+        double* out[3] = {ax, ay, az};
+        const double* res[3] = {b->ax, b->ay, b->az};
+        for (int k = 0; k < 3 && r == GX_OK; ++k) {
+            e = cudaMemcpyAsync(out[k], res[k], (size_t)n * sizeof(double), kout, b->stream);
+            if (e != cudaSuccess) r = fail_cuda(e, fn);
+        }
+        if (r == GX_OK) {
+            e = cudaStreamSynchronize(b->stream);
+            if (e != cudaSuccess) r = fail_cuda(e, fn);
+        }
+        cudaEventDestroy(ev);
+    }
+    gx_batch_destroy(b);
+    return r;
+    GX_GUARD_END
+}

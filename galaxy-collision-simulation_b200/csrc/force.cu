@@ -1,0 +1,108 @@
+// force.cu -- one-system direct-sum kernels (grid = target tiles x source chunks), the
+// ordered j-split reduction and the table of compiled variants.  The arithmetic lives in
+// force_tile.cuh.
+#include "force_tile.cuh"
+
+#include <mutex>
+
+namespace gx {
+namespace {
+
+// Ordered reduction of the j-split partial sums, then G and the epilogue.
+__global__ void __launch_bounds__(256) force_reduce_kernel(const ForceArgs a) {
+    const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (t >= a.n_tgt) return;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int c = 0; c < a.nsplit; ++c) {
+        const size_t base = (size_t)c * 3 * (size_t)a.n_tgt + (size_t)t;
+        s[0] += a.part[base];
+        s[1] += a.part[base + (size_t)a.n_tgt];
+        s[2] += a.part[base + 2 * (size_t)a.n_tgt];
+    }
+    write_result(a, t, target_body(a, t), a.G * s[0], a.G * s[1], a.G * s[2]);
+}
+
+template <int BLOCK, int IPT, int JT, bool PACKED, bool EPS0>
+__global__ void __launch_bounds__(BLOCK) force_mixed_kernel(const ForceArgs a) {
+    mixed_tile<BLOCK, IPT, JT, PACKED, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+}
+
+template <int BLOCK, int IPT, int JT, bool EPS0>
+__global__ void __launch_bounds__(BLOCK) force_f64_kernel(const ForceArgs a) {
+    f64_tile<BLOCK, IPT, JT, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+}
+
+template <int BLOCK, int JT>
+__global__ void __launch_bounds__(BLOCK) force_exact_kernel(const ForceArgs a) {
+    exact_tile<BLOCK, JT>(a, (int64_t)blockIdx.x * BLOCK);
+}
+
+#define MIXED(B, I, J, P, E) {kMixed, B, I, J, P, E, (const void*)&force_mixed_kernel<B, I, J, P, E>}
+#define F64(B, I, J, E) {kF64, B, I, J, 0, E, (const void*)&force_f64_kernel<B, I, J, E>}
+#define EXACT(B, J) {kF64Exact, B, 1, J, 0, 1, (const void*)&force_exact_kernel<B, J>}
+
+const ForceVariant kVariants[] = {
+    MIXED(256, 4, 512, true, false),
+    MIXED(128, 4, 512, true, false),
+    MIXED(256, 2, 512, true, false),
+    MIXED(128, 8, 512, true, false),
+    MIXED(64, 4, 256, true, false),
+    MIXED(256, 4, 512, false, false),
+    MIXED(256, 4, 512, true, true),
+    MIXED(64, 4, 256, true, true),
+    F64(256, 2, 256, false),
+    F64(128, 2, 256, false),
+    F64(256, 1, 256, false),
+    F64(128, 4, 256, false),
+    F64(64, 2, 128, false),
+    F64(256, 2, 256, true),
+    F64(64, 2, 128, true),
+    EXACT(128, 256),
+    EXACT(64, 128),
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+}  // namespace
+
+const ForceVariant* force_variants(int* count) {
+    *count = kNumVariants;
+    return kVariants;
+}
+
+int force_variant_ids(int precision, int eps0, int* ids, int max_ids) {
+    int c = 0;
+    for (int i = 0; i < kNumVariants; ++i) {
+        const ForceVariant& v = kVariants[i];
+        if (v.precision != precision) continue;
+        if (precision != kF64Exact && v.eps0 != eps0) continue;
+        if (c < max_ids) ids[c] = i;
+        ++c;
+    }
+    return c;
+}
+
+cudaError_t force_launch(const ForceVariant& v, const ForceArgs& args, cudaStream_t stream) {
+    if (args.n_tgt <= 0) return cudaSuccess;
+    const int64_t tile = (int64_t)v.block * v.ipt;
+    dim3 grid((unsigned)((args.n_tgt + tile - 1) / tile), (unsigned)args.nsplit, 1);
+    ForceArgs a = args;
+    void* params[] = {(void*)&a};
+    cudaError_t e = cudaLaunchKernel(v.fn, grid, dim3(v.block), params, 0, stream);
+    if (e != cudaSuccess || args.nsplit <= 1) return e;
+    force_reduce_kernel<<<(unsigned)((args.n_tgt + 255) / 256), 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+int force_occupancy(const ForceVariant& v) {
+    static std::mutex mu;
+    static int cache[64] = {0};
+    const int idx = (int)(&v - kVariants);
+    std::lock_guard<std::mutex> lock(mu);
+    if (idx >= 0 && idx < 64 && cache[idx] > 0) return cache[idx];
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, v.fn, v.block, 0) != cudaSuccess || nb < 1) nb = 1;
+    if (idx >= 0 && idx < 64) cache[idx] = nb;
+    return nb;
+}
+
+}  // namespace gx

@@ -1,0 +1,61 @@
+// force.cuh -- host-visible description of the direct-force kernels (force.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "precision.cuh"
+
+namespace gx {
+
+// One launch of the tiled direct sum: targets (a range or an index list) against the
+// sources [0, n_src) of one SoA system.  blockIdx.y selects a chunk of the sources (the
+// j-split); with more than one chunk every CTA writes FP64 partial sums and
+// force_reduce() adds them in chunk order, so results do not depend on scheduling.
+struct ForceArgs {
+    const double* x;
+    const double* y;
+    const double* z;
+    const double* m;
+    int64_t n_src;
+    const int64_t* tgt_idx;  // nullable: targets are t_begin + t
+    int64_t t_begin;
+    int64_t n_tgt;
+    int64_t j_chunk;  // sources per chunk (a multiple of the kernel's j tile)
+    int nsplit;       // number of chunks (gridDim.y)
+    double* ax;       // results, indexed by target ordinal t
+    double* ay;
+    double* az;
+    double* part;     // nsplit * 3 * n_tgt partial sums when nsplit > 1
+    double* vx;       // optional closing kick v[body] += a * kick_dt (nullable)
+    double* vy;
+    double* vz;
+    double kick_dt;
+    double G;
+    double eps2;      // softening^2 in FP64
+    float eps2f;      // softening^2 rounded to FP32 (mixed precision)
+};
+
+struct ForceVariant {
+    int precision;
+    int block;
+    int ipt;   // targets per thread
+    int jt;    // j tile (sources staged per shared-memory pass)
+    int packed;
+    int eps0;  // guards s == 0 pairs (softening 0)
+    const void* fn;
+};
+
+// All compiled variants; eps0 variants are separate entries.
+const ForceVariant* force_variants(int* count);
+// Variants usable for (precision, eps0) in the order of gx_variant_* ids.
+int force_variant_ids(int precision, int eps0, int* ids, int max_ids);
+
+// Launches variant `v` over args (grid = ceil(n_tgt / (block*ipt)) x nsplit) and, when
+// nsplit > 1, the ordered partial-sum reduction with the epilogue.
+cudaError_t force_launch(const ForceVariant& v, const ForceArgs& args, cudaStream_t stream);
+
+// Resident CTAs per SM for a variant (occupancy query, cached).
+int force_occupancy(const ForceVariant& v);
+
+}  // namespace gx

@@ -1,0 +1,71 @@
+"""Target-range sharding of the direct KDK step over ranks (one process per GPU).
+
+Mirrors the reference's MPI decomposition (cpp/mpi/distributed_solver.cpp:68-79 ownership
+ranges, :114-123 MPI_Allgatherv of the state, cpp/core/main.cpp:240-253 step order): every
+rank holds all positions, owns the contiguous target range of ``ownership_range``, kicks
+and drifts only its own bodies, and the ranks exchange the drifted positions once per step.
+The reference gathers the full 11-double state three times a step; here one all-gather of
+the 3 FP64 position components of the owned bodies suffices (masses never change, and
+velocities/accelerations are only read by their owner).  The exchange is a
+``torch.distributed.all_gather_into_tensor`` (NCCL over NVLink on GPUs, gloo on CPU);
+ranges are padded to the largest one so the collective has equal chunks.
+
+The force is injected: on GPUs it is the engine's target-range kernel; the CPU tests pass
+a CPU function and a gloo group.
+"""
+from __future__ import annotations
+
+from typing import Callable
+
+import torch
+import torch.distributed as dist
+
+
+def ownership_range(count: int, rank: int, size: int) -> tuple[int, int]:
+    """ownership_for_rank (cpp/mpi/distributed_solver.cpp:68-79)."""
+    if size <= 1:
+        return 0, count
+    base, rem = divmod(count, size)
+    begin = rank * base + min(rank, rem)
+    return begin, begin + base + (1 if rank < rem else 0)
+
+
+# force(X_full (3, n), m (n,), begin, end) -> A_owned (3, end - begin)
+ForceFn = Callable[[torch.Tensor, torch.Tensor, int, int], torch.Tensor]
+
+
+class ShardedLeapfrog:
+    def __init__(self, n: int, force: ForceFn, rank: int | None = None, world: int | None = None, group=None):
+        self.n = n
+        self.force = force
+        self.group = group
+        self.rank = dist.get_rank(group) if rank is None else rank
+        self.world = dist.get_world_size(group) if world is None else world
+        self.begin, self.end = ownership_range(n, self.rank, self.world)
+        self.chunk = max(ownership_range(n, r, self.world)[1] - ownership_range(n, r, self.world)[0]
+                         for r in range(self.world))
+        self.ranges = [ownership_range(n, r, self.world) for r in range(self.world)]
+
+    def gather_positions(self, X: torch.Tensor) -> None:
+        """All ranks' owned columns of X (3, n) -> everyone's full X, in place."""
+        if self.world == 1:
+            return
+        send = torch.zeros(3, self.chunk, dtype=X.dtype, device=X.device)
+        send[:, : self.end - self.begin] = X[:, self.begin:self.end]
+        recv = torch.empty(self.world, 3, self.chunk, dtype=X.dtype, device=X.device)
+        dist.all_gather_into_tensor(recv, send.unsqueeze(0).contiguous(), group=self.group)
+        for r, (b, e) in enumerate(self.ranges):
+            X[:, b:e] = recv[r, :, : e - b]
+
+    def initial_accelerations(self, X: torch.Tensor, m: torch.Tensor) -> torch.Tensor:
+        return self.force(X, m, self.begin, self.end)
+
+    def step(self, X: torch.Tensor, V: torch.Tensor, A: torch.Tensor, m: torch.Tensor, dt: float) -> None:
+        """One KDK step.  X (3, n) full; V, A (3, n_owned) for the owned range; in place."""
+        h = 0.5 * dt
+        b, e = self.begin, self.end
+        V.add_(A * h)
+        X[:, b:e] += V * dt
+        self.gather_positions(X)
+        A.copy_(self.force(X, m, b, e))
+        V.add_(A * h)

@@ -1,0 +1,246 @@
+/*
+ * gx.h -- C ABI of the B200 softened-gravity engine (direct O(N^2) forces, fused
+ * kick-drift-kick integration, FMM P2P near-field leaves, FP64 diagnostics, batched
+ * ensembles and the adjoint of the direct force).
+ *
+ * Plain C: pointers, sizes and status codes only; no exceptions cross this boundary.
+ * Every function returns a gx_status; gx_last_error() gives the message of the last
+ * failure on the calling thread.  There is no CPU fallback: without a CUDA device
+ * every compute call returns GX_ERR_NO_DEVICE.
+ *
+ * Array arguments are structure-of-arrays FP64 (x, y, z, m, ...).  Unless a function
+ * says otherwise, all arrays of one call must be either all device memory (then the
+ * call is stream-ordered on `stream` and returns without synchronising) or all host
+ * memory (then the call copies in, computes and copies out, and returns after the
+ * stream has finished).  `stream` is a cudaStream_t; NULL means the legacy default
+ * stream.
+ *
+ * Reference interfaces replaced (ryan-charette/galaxy-collision-simulation):
+ *   cpp/cuda/cuda_solver.hpp:10-12        cuda_solver_available, compute_cuda_direct_accelerations,
+ *                                          cuda_direct_leapfrog_step
+ *   cpp/direct/direct_solver.hpp:22-28    compute_direct_accelerations[_for_targets]
+ *   cpp/core/integrator.hpp:11-21         kick, drift, leapfrog_step
+ *   cpp/core/diagnostics.hpp:11-21        Diagnostics, compute_diagnostics
+ *   cpp/fmm/fmm_solver.cpp:295-310        the P2P near-field loop of evaluate_particle
+ *   cpp/fmm/fmm_solver.hpp:37-47,71-83    the leaf lists (particle_indices, near_leaves)
+ */
+#ifndef GX_H
+#define GX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define GX_ABI_VERSION 1
+
+typedef enum gx_status {
+    GX_OK = 0,
+    GX_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, mixed host/device pointers ... */
+    GX_ERR_NO_DEVICE = 2,        /* no usable CUDA device (the reference fell back to the CPU) */
+    GX_ERR_CUDA = 3,             /* a CUDA runtime error; the message names the call */
+    GX_ERR_TIMEOUT = 4,          /* a bounded wait gave up (gx_session_synchronize_timeout) */
+    GX_ERR_OUT_OF_MEMORY = 5,    /* device or host allocation failed */
+    GX_ERR_UNSUPPORTED = 6       /* valid request this build does not implement */
+} gx_status;
+
+typedef enum gx_precision {
+    /* FP64 pair arithmetic, tiled; FMA contraction and a refined hardware rsqrt.
+     * Relative error vs the reference ~1e-15. */
+    GX_PRECISION_F64 = 0,
+    /* FP32 pair arithmetic on offsets from a per-tile FP64 origin, per-tile compensated
+     * (two-sum) accumulation, FP64 results.  Median relative error ~1e-7. */
+    GX_PRECISION_MIXED = 1,
+    /* FP64 with the reference's exact operation order, IEEE sqrt and division and no FMA
+     * contraction: bit-identical to compute_direct_accelerations_for_targets
+     * (cpp/direct/direct_solver.cpp:59-83) and, for P2P, to evaluate_particle. */
+    GX_PRECISION_F64_EXACT = 2
+} gx_precision;
+
+/* PhysicsParams (cpp/core/simulation_params.hpp:5-8). */
+typedef struct gx_physics {
+    double G;         /* gravitational_constant */
+    double softening; /* Plummer epsilon; eps^2 is added to |r|^2 */
+} gx_physics;
+
+/* Diagnostics (cpp/core/diagnostics.hpp:11-19), fields in diagnostics.csv column order. */
+typedef struct gx_diagnostics {
+    double total_mass;
+    double kinetic_energy;
+    double potential_energy;
+    double total_energy;
+    double momentum[3];
+    double center_of_mass[3];
+    double angular_momentum[3];
+} gx_diagnostics;
+
+/* ---- library -------------------------------------------------------------------- */
+const char* gx_last_error(void);
+int gx_abi_version(void);
+/* cuda_solver_available (cpp/cuda/cuda_solver.cu:185-189): *available = 1 when a CUDA
+ * device of compute capability 10.0 can be used. */
+int gx_device_available(int* available);
+
+/* ---- stateless direct sum --------------------------------------------------------- */
+/* compute_cuda_direct_accelerations (cpp/cuda/cuda_solver.cu:191-210) and
+ * compute_direct_accelerations (cpp/direct/direct_solver.cpp:38-57): a_i for every body. */
+int gx_direct_accel(int64_t n, const double* x, const double* y, const double* z,
+                    const double* m, gx_physics phys, int precision, double* ax, double* ay,
+                    double* az, void* stream);
+
+/* compute_direct_accelerations_for_targets (cpp/direct/direct_solver.cpp:59-83): targets
+ * [begin, end) against all n sources; results at ax[i - begin].  With `targets` non-null,
+ * targets[k] for k < n_targets instead of a range (begin/end ignored; n_targets used). */
+int gx_direct_accel_targets(int64_t n, const double* x, const double* y, const double* z,
+                            const double* m, int64_t begin, int64_t end, const int64_t* targets,
+                            int64_t n_targets, gx_physics phys, int precision, double* ax,
+                            double* ay, double* az, void* stream);
+
+/* cuda_direct_leapfrog_step (cpp/cuda/cuda_solver.cu:212-246) / leapfrog_step
+ * (cpp/core/integrator.cpp:33-42): one KDK step in place, reusing the caller's a as the
+ * first kick's acceleration; x, v and a are updated. */
+int gx_leapfrog_step(int64_t n, double* x, double* y, double* z, double* vx, double* vy,
+                     double* vz, double* ax, double* ay, double* az, const double* m,
+                     double dt, gx_physics phys, int precision, void* stream);
+
+/* kick (cpp/core/integrator.cpp:7-11): v += a*dt.  drift (:13-17): x += v*dt.
+ * kick_drift: v += a*kick_dt then x += v*drift_dt.  Device pointers only. */
+int gx_kick(int64_t n, double* vx, double* vy, double* vz, const double* ax,
+            const double* ay, const double* az, double dt, void* stream);
+int gx_drift(int64_t n, double* x, double* y, double* z, const double* vx, const double* vy,
+             const double* vz, double dt, void* stream);
+int gx_kick_drift(int64_t n, double* x, double* y, double* z, double* vx, double* vy,
+                  double* vz, const double* ax, const double* ay, const double* az,
+                  double kick_dt, double drift_dt, void* stream);
+
+/* compute_diagnostics (cpp/core/diagnostics.cpp:7-37) in FP64 on the device. */
+int gx_diagnostics_compute(int64_t n, const double* x, const double* y, const double* z,
+                           const double* vx, const double* vy, const double* vz,
+                           const double* m, gx_physics phys, gx_diagnostics* out,
+                           void* stream);
+
+/* ---- resident session (the step loop of cpp/core/main.cpp:172-184) ------------------ */
+/* The session owns device copies of the state; steps run as CUDA-graph launches with no
+ * host synchronisation; host copies happen only in set_state / get_state. */
+typedef struct gx_session gx_session;
+
+int gx_session_create(int64_t n, gx_physics phys, int device, gx_session** out);
+int gx_session_destroy(gx_session* s);
+/* Stream the session's work is ordered on (default: a stream the session creates). */
+int gx_session_set_stream(gx_session* s, void* stream);
+int gx_session_get_stream(gx_session* s, void** stream);
+/* Host or device arrays; a (ax..az) may be null (then accelerations are zeroed and the
+ * caller computes them with gx_session_compute_accelerations). */
+int gx_session_set_state(gx_session* s, const double* x, const double* y, const double* z,
+                         const double* vx, const double* vy, const double* vz,
+                         const double* m, const double* ax, const double* ay,
+                         const double* az);
+int gx_session_get_state(gx_session* s, double* x, double* y, double* z, double* vx,
+                         double* vy, double* vz, double* ax, double* ay, double* az);
+/* Device pointers of the resident arrays, in the order x,y,z,vx,vy,vz,ax,ay,az,m. */
+int gx_session_device_arrays(gx_session* s, double** ptrs10);
+int gx_session_compute_accelerations(gx_session* s, int precision);
+/* n_steps KDK steps (kick dt/2, drift dt, force, kick dt/2 per step). */
+int gx_session_step(gx_session* s, int64_t n_steps, double dt, int precision);
+int gx_session_diagnostics(gx_session* s, gx_diagnostics* out);
+int gx_session_synchronize(gx_session* s);
+/* Bounded host wait: GX_ERR_TIMEOUT if the stream is still busy after timeout_ms. */
+int gx_session_synchronize_timeout(gx_session* s, double timeout_ms);
+/* Force-kernel timing: when enabled, every force launch of the session is bracketed by
+ * CUDA events on the session stream (graphs are bypassed while enabled). */
+int gx_session_enable_timing(gx_session* s, int enable);
+int gx_session_force_timing(gx_session* s, double* total_ms, int64_t* launches);
+/* Kernel configuration used for `precision` (variant id, j-split count). */
+int gx_session_get_config(gx_session* s, int precision, int* variant, int* jsplit);
+int gx_session_set_config(gx_session* s, int precision, int variant, int jsplit);
+/* Times the candidate configurations on the session's own state and keeps the fastest;
+ * returns its time per force evaluation. */
+int gx_session_autotune(gx_session* s, int precision, double* best_ms);
+
+/* ---- FMM P2P near field (cpp/fmm/fmm_solver.cpp:295-310) --------------------------- */
+/* For every body i of leaf l (leaf_particles[leaf_offsets[l] .. leaf_offsets[l+1]]),
+ * adds sum over near leaves s of leaf l (near_leaves[near_offsets[l] .. [l+1]]) and their
+ * bodies j != i of the pair term to (ax[i], ay[i], az[i]).  Leaf ids are row numbers of
+ * leaf_offsets.  Pass the far field in a to get the reference's full FMM result. */
+int gx_p2p_leaves(int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, int32_t n_leaves, const int32_t* leaf_offsets,
+                  const int32_t* leaf_particles, const int32_t* near_offsets,
+                  const int32_t* near_leaves, gx_physics phys, int precision, double* ax,
+                  double* ay, double* az, void* stream);
+
+/* Leaf lists of the reference octree (FastMultipoleSolver::build, fmm_solver.cpp:48-98,
+ * 210-277) built on the host as CSR arrays for gx_p2p_leaves. Host arrays only. */
+typedef struct gx_leaf_lists gx_leaf_lists;
+int gx_leaf_lists_build(int64_t n, const double* x, const double* y, const double* z,
+                        const double* m, double softening, double theta,
+                        int64_t leaf_capacity, int max_depth, gx_leaf_lists** out);
+int gx_leaf_lists_info(const gx_leaf_lists* l, int32_t* n_leaves, int64_t* n_leaf_particles,
+                       int64_t* n_near, int64_t* n_far, int64_t* n_p2p_pairs);
+int gx_leaf_lists_export(const gx_leaf_lists* l, int32_t* leaf_offsets,
+                         int32_t* leaf_particles, int32_t* near_offsets,
+                         int32_t* near_leaves);
+int gx_leaf_lists_free(gx_leaf_lists* l);
+
+/* ---- batched ensembles (no reference counterpart) ---------------------------------- */
+/* n_instances independent systems concatenated in one SoA; instance b owns bodies
+ * offsets[b] .. offsets[b+1].  Forces never cross instances. */
+int gx_batch_accel(int32_t n_instances, const int64_t* offsets, const double* x,
+                   const double* y, const double* z, const double* m, gx_physics phys,
+                   int precision, double* ax, double* ay, double* az, void* stream);
+
+typedef struct gx_batch gx_batch;
+int gx_batch_create(int32_t n_instances, const int64_t* offsets, gx_physics phys, int device,
+                    gx_batch** out);
+int gx_batch_destroy(gx_batch* b);
+int gx_batch_set_stream(gx_batch* b, void* stream);
+int gx_batch_set_state(gx_batch* b, const double* x, const double* y, const double* z,
+                       const double* vx, const double* vy, const double* vz, const double* m);
+int gx_batch_get_state(gx_batch* b, double* x, double* y, double* z, double* vx, double* vy,
+                       double* vz, double* ax, double* ay, double* az);
+int gx_batch_device_arrays(gx_batch* b, double** ptrs10);
+int gx_batch_compute_accelerations(gx_batch* b, int precision);
+/* n_steps KDK steps of every instance; captured once as one CUDA graph and replayed. */
+int gx_batch_step(gx_batch* b, int64_t n_steps, double dt, int precision);
+/* Per-instance diagnostics, out[n_instances]. */
+int gx_batch_diagnostics(gx_batch* b, gx_diagnostics* out);
+int gx_batch_synchronize(gx_batch* b);
+int gx_batch_get_config(gx_batch* b, int precision, int* variant);
+int gx_batch_set_config(gx_batch* b, int precision, int variant);
+int gx_batch_autotune(gx_batch* b, int precision, double* best_ms);
+int gx_batch_enable_timing(gx_batch* b, int enable);
+int gx_batch_force_timing(gx_batch* b, double* total_ms, int64_t* launches);
+
+/* ---- adjoint of the direct force (no reference counterpart) ------------------------ */
+/* For cotangent l on the accelerations a(x, m):
+ *   gx_k = dL/dx_k = G sum_j [ s^-3/2 (m_k l_j - m_j l_k) - 3 s^-5/2 (m_k l_j.d - m_j l_k.d) d ]
+ *   gm_k = dL/dm_k = -G sum_j s^-3/2 l_j.d,      d = x_j - x_k, s = |d|^2 + eps^2.
+ * gm may be null.  Device or host arrays (all of one kind). */
+int gx_direct_vjp(int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, const double* lx, const double* ly, const double* lz,
+                  gx_physics phys, int precision, double* gx, double* gy, double* gz,
+                  double* gm, void* stream);
+
+/* ---- kernel variants ---------------------------------------------------------------- */
+/* Number of direct-force variants for a precision and a printable description. */
+int gx_variant_count(int precision, int* count);
+int gx_variant_describe(int precision, int variant, char* buf, int buflen);
+
+/* ---- fault injection for tests (host side only; never touches the GPU) ------------- */
+/* The next `count` device allocations made by the library fail with GX_ERR_OUT_OF_MEMORY. */
+int gx_debug_fail_allocations(int count);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GX_H */

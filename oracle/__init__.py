@@ -1,0 +1,231 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the parity checker.
+
+* ``port``  -- _build/liboracle.so, the plain-C restatement of the reference path
+               (gx_oracle.c; every function cites the reference file:line it follows);
+* ``ref``   -- _ref/libgxref.so, the reference's own C++ sources compiled unmodified
+               with ref_wrap.cpp (only where the reference tree was present at build time).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs may
+import this package.  The engine never calls it; it is the checker, not the product.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+PORT_PATH = ORACLE_DIR / "_build" / "liboracle.so"
+REF_PATH = ORACLE_DIR / "_ref" / "libgxref.so"
+REF_SIM_CPU = ORACLE_DIR / "_ref" / "fmm_galaxy_sim_cpu"
+REF_SIM_B200 = ORACLE_DIR / "_ref" / "fmm_galaxy_sim_b200"
+REF_SMOKE_B200 = ORACLE_DIR / "_ref" / "ref_smoke_tests_b200"
+
+_port = None
+_ref = None
+P = c_void_p
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def port():
+    global _port
+    if _port is None:
+        if not PORT_PATH.exists():
+            raise FileNotFoundError(f"{PORT_PATH} missing: run __graft_entry__.build() (make -C oracle)")
+        lib = ctypes.CDLL(str(PORT_PATH))
+        lib.oracle_direct_targets.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int64, c_int64, P, P, P]
+        lib.oracle_direct_indexed.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int64, P, P, P, P]
+        lib.oracle_direct_indexed_mt.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int64, P, P, P, P, c_int]
+        lib.oracle_direct_symmetric.argtypes = [c_int64, P, P, P, P, c_double, c_double, P, P, P]
+        lib.oracle_leapfrog.argtypes = [c_int64, P, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, c_int, c_int]
+        lib.oracle_diagnostics.argtypes = [c_int64, P, P, P, P, P, P, P, c_double, c_double, P]
+        lib.oracle_leaf_lists.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int64, c_int,
+                                          POINTER(c_int32), POINTER(c_void_p), POINTER(c_void_p), POINTER(c_void_p),
+                                          POINTER(c_void_p), POINTER(c_int64), POINTER(c_int64)]
+        lib.oracle_free.argtypes = [c_void_p]
+        lib.oracle_p2p_near.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int32, P, P, P, P, P, P, P]
+        lib.oracle_direct_vjp.argtypes = [c_int64, P, P, P, P, P, P, P, c_double, c_double, P, P, P, P]
+        lib.oracle_ownership.argtypes = [c_int64, c_int, c_int, POINTER(c_int64), POINTER(c_int64)]
+        _port = lib
+    return _port
+
+
+def ref_available() -> bool:
+    return REF_PATH.exists()
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not REF_PATH.exists():
+            raise FileNotFoundError(f"{REF_PATH} missing: the reference tree was absent at build time")
+        lib = ctypes.CDLL(str(REF_PATH))
+        lib.ref_direct.argtypes = [c_int64, P, P, P, P, c_double, c_double, P, P, P]
+        lib.ref_direct_targets_mt.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int64, c_int64, P, P, P, c_int]
+        lib.ref_leapfrog_direct.argtypes = [c_int64, P, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, c_int]
+        lib.ref_diagnostics.argtypes = [c_int64, P, P, P, P, P, P, P, c_double, c_double, P]
+        lib.ref_fmm.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, P, P, P]
+        lib.ref_fmm_split.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int,
+                                      POINTER(c_int32), POINTER(c_int64), P, P, P, P, P, P, P]
+        lib.ref_smoke80_inputs.argtypes = [P, P, P, P]
+        _ref = lib
+    return _ref
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ---- restatement (port) ------------------------------------------------------------
+def direct_targets(x, y, z, m, G, eps, begin=0, end=None):
+    x, y, z, m = map(_f, (x, y, z, m))
+    n = len(x)
+    end = n if end is None else end
+    out = [np.zeros(n) for _ in range(3)]
+    port().oracle_direct_targets(n, _p(x), _p(y), _p(z), _p(m), G, eps, begin, end, *map(_p, out))
+    return np.stack([o[begin:end] for o in out], 1)
+
+
+def direct_indexed(x, y, z, m, G, eps, targets, threads=1):
+    x, y, z, m = map(_f, (x, y, z, m))
+    t = np.ascontiguousarray(targets, np.int64)
+    out = [np.zeros(len(t)) for _ in range(3)]
+    if threads > 1:
+        port().oracle_direct_indexed_mt(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, len(t), _p(t), *map(_p, out), threads)
+    else:
+        port().oracle_direct_indexed(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, len(t), _p(t), *map(_p, out))
+    return np.stack(out, 1)
+
+
+def direct_symmetric(x, y, z, m, G, eps):
+    x, y, z, m = map(_f, (x, y, z, m))
+    out = [np.zeros(len(x)) for _ in range(3)]
+    port().oracle_direct_symmetric(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, *map(_p, out))
+    return np.stack(out, 1)
+
+
+def leapfrog(state: dict, m, G, eps, dt, steps, solver=0) -> dict:
+    """state: x,y,z,vx,vy,vz,ax,ay,az arrays (copied); solver 0 = symmetric, 1 = per-target."""
+    s = {k: _f(state[k]).copy() for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+    m = _f(m)
+    port().oracle_leapfrog(len(m), *(_p(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")),
+                           _p(m), G, eps, dt, steps, solver)
+    return s
+
+
+def diagnostics(x, y, z, vx, vy, vz, m, G, eps) -> np.ndarray:
+    arrs = list(map(_f, (x, y, z, vx, vy, vz, m)))
+    out = np.zeros(13)
+    port().oracle_diagnostics(len(arrs[0]), *map(_p, arrs), G, eps, _p(out))
+    return out
+
+
+def leaf_lists(x, y, z, m, eps, theta, leaf_capacity, max_depth=32):
+    x, y, z, m = map(_f, (x, y, z, m))
+    nl = c_int32()
+    ptrs = [c_void_p() for _ in range(4)]
+    nn, nf = c_int64(), c_int64()
+    rc = port().oracle_leaf_lists(len(x), _p(x), _p(y), _p(z), _p(m), eps, theta, leaf_capacity, max_depth,
+                                  ctypes.byref(nl), *(ctypes.byref(p) for p in ptrs), ctypes.byref(nn), ctypes.byref(nf))
+    if rc != 0:
+        raise RuntimeError("oracle_leaf_lists failed")
+    lo = np.ctypeslib.as_array(ctypes.cast(ptrs[0], POINTER(c_int32)), shape=(nl.value + 1,))
+    sizes = [nl.value + 1, int(lo[-1]), nl.value + 1, nn.value]
+    out = []
+    for p, s in zip(ptrs, sizes):
+        a = np.ctypeslib.as_array(ctypes.cast(p, POINTER(c_int32)), shape=(max(s, 1),))[:s].copy() if p.value else np.zeros(0, np.int32)
+        port().oracle_free(p)
+        out.append(a)
+    return dict(leaf_offsets=out[0], leaf_particles=out[1], near_offsets=out[2], near_leaves=out[3], n_far=nf.value)
+
+
+def p2p_near(x, y, z, m, G, eps, lists, acc=None):
+    x, y, z, m = map(_f, (x, y, z, m))
+    n = len(x)
+    a = [np.zeros(n) for _ in range(3)] if acc is None else [_f(acc[:, c]).copy() for c in range(3)]
+    L = {k: np.ascontiguousarray(lists[k], np.int32) for k in ("leaf_offsets", "leaf_particles", "near_offsets", "near_leaves")}
+    port().oracle_p2p_near(n, _p(x), _p(y), _p(z), _p(m), G, eps, len(L["leaf_offsets"]) - 1, _p(L["leaf_offsets"]),
+                           _p(L["leaf_particles"]), _p(L["near_offsets"]), _p(L["near_leaves"]), *map(_p, a))
+    return np.stack(a, 1)
+
+
+def direct_vjp(x, y, z, m, lx, ly, lz, G, eps):
+    arrs = list(map(_f, (x, y, z, m, lx, ly, lz)))
+    out = [np.zeros(len(x)) for _ in range(4)]
+    port().oracle_direct_vjp(len(x), *map(_p, arrs), G, eps, *map(_p, out))
+    return np.stack(out[:3], 1), out[3]
+
+
+def ownership(count, rank, size):
+    b, e = c_int64(), c_int64()
+    port().oracle_ownership(count, rank, size, ctypes.byref(b), ctypes.byref(e))
+    return b.value, e.value
+
+
+# ---- the reference itself (ref) ----------------------------------------------------
+def ref_direct(x, y, z, m, G, eps):
+    x, y, z, m = map(_f, (x, y, z, m))
+    out = [np.zeros(len(x)) for _ in range(3)]
+    ref().ref_direct(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, *map(_p, out))
+    return np.stack(out, 1)
+
+
+def ref_direct_targets(x, y, z, m, G, eps, begin, end, threads=1):
+    x, y, z, m = map(_f, (x, y, z, m))
+    out = [np.zeros(end - begin) for _ in range(3)]
+    ref().ref_direct_targets_mt(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, begin, end, *map(_p, out), threads)
+    return np.stack(out, 1)
+
+
+def ref_leapfrog(state: dict, m, G, eps, dt, steps) -> dict:
+    s = {k: _f(state[k]).copy() for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+    m = _f(m)
+    ref().ref_leapfrog_direct(len(m), *(_p(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")), _p(m),
+                              G, eps, dt, steps)
+    return s
+
+
+def ref_diagnostics(x, y, z, vx, vy, vz, m, G, eps) -> np.ndarray:
+    arrs = list(map(_f, (x, y, z, vx, vy, vz, m)))
+    out = np.zeros(13)
+    ref().ref_diagnostics(len(arrs[0]), *map(_p, arrs), G, eps, _p(out))
+    return out
+
+
+def ref_fmm(x, y, z, m, G, eps, theta, leaf_capacity, order=4):
+    x, y, z, m = map(_f, (x, y, z, m))
+    out = [np.zeros(len(x)) for _ in range(3)]
+    ref().ref_fmm(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, *map(_p, out))
+    return np.stack(out, 1)
+
+
+def ref_fmm_split(x, y, z, m, G, eps, theta, leaf_capacity, order=4):
+    x, y, z, m = map(_f, (x, y, z, m))
+    n = len(x)
+    nl, nn = c_int32(), c_int64()
+    ref().ref_fmm_split(n, _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, ctypes.byref(nl),
+                        ctypes.byref(nn), None, None, None, None, None, None, None)
+    lo = np.zeros(nl.value + 1, np.int32)
+    lp = np.zeros(n, np.int32)
+    no = np.zeros(nl.value + 1, np.int32)
+    nlv = np.zeros(max(nn.value, 1), np.int32)
+    far = [np.zeros(n) for _ in range(3)]
+    ref().ref_fmm_split(n, _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, ctypes.byref(nl),
+                        ctypes.byref(nn), _p(lo), _p(lp), _p(no), _p(nlv), *map(_p, far))
+    return dict(leaf_offsets=lo, leaf_particles=lp, near_offsets=no, near_leaves=nlv[: nn.value]), np.stack(far, 1)
+
+
+def ref_smoke80_inputs():
+    a = [np.zeros(80) for _ in range(4)]
+    ref().ref_smoke80_inputs(*map(_p, a))
+    return a
+
+
+def default_threads() -> int:
+    return len(os.sched_getaffinity(0))

@@ -1,0 +1,79 @@
+"""The multi-rank KDK step on CPU: world_size 2 over gloo, forces from the oracle.
+
+The sharded run (ownership ranges + one position all-gather per step) must reproduce the
+single-process per-target leapfrog of the oracle bit for bit.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import conftest  # noqa: F401  (registers the engine package as `gx` in spawned ranks too)
+import oracle
+from gx.sharded import ShardedLeapfrog, ownership_range
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _oracle_force(X, m, b, e):
+    Xn = X.numpy()
+    a = oracle.direct_targets(Xn[0], Xn[1], Xn[2], m.numpy(), 1.0, 0.05, b, e)
+    return torch.from_numpy(np.ascontiguousarray(a.T))
+
+
+def _worker(rank, world, port, n, steps, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import gx
+        p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 42, 0.05)
+        X = torch.from_numpy(np.stack([p.x, p.y, p.z]))
+        m = torch.from_numpy(p.m)
+        sh = ShardedLeapfrog(n, _oracle_force)
+        V = torch.from_numpy(np.stack([p.vx, p.vy, p.vz])[:, sh.begin:sh.end].copy())
+        A = sh.initial_accelerations(X, m)
+        for _ in range(steps):
+            sh.step(X, V, A, m, 0.005)
+        Vfull = [torch.zeros(3, sh.chunk, dtype=torch.float64) for _ in range(world)]
+        pad = torch.zeros(3, sh.chunk, dtype=torch.float64)
+        pad[:, : sh.end - sh.begin] = V
+        dist.all_gather(Vfull, pad)
+        if rank == 0:
+            v = np.concatenate([Vfull[r][:, : e - b].numpy() for r, (b, e) in enumerate(sh.ranges)], 1)
+            np.save(out, np.concatenate([X.numpy(), v]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_ownership_matches_reference():
+    for n in (0, 1, 7, 10, 1001):
+        for size in (1, 2, 3, 8):
+            rs = [ownership_range(n, r, size) for r in range(size)]
+            assert rs == [oracle.ownership(n, r, size) for r in range(size)]
+            assert rs[0][0] == 0 and rs[-1][1] == n
+
+
+@pytest.mark.parametrize("n", [101])
+def test_two_rank_step_matches_single_process(tmp_path, n):
+    steps = 3
+    out = str(tmp_path / "state.npy")
+    mp.start_processes(_worker, args=(2, _free_port(), n, steps, out), nprocs=2, start_method="spawn")
+    got = np.load(out)
+    import gx
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 42, 0.05)
+    a0 = oracle.direct_targets(p.x, p.y, p.z, p.m, 1.0, 0.05)
+    st = dict(x=p.x, y=p.y, z=p.z, vx=p.vx, vy=p.vy, vz=p.vz, ax=a0[:, 0], ay=a0[:, 1], az=a0[:, 2])
+    ref = oracle.leapfrog(st, p.m, 1.0, 0.05, 0.005, steps, solver=1)
+    expect = np.stack([ref[k] for k in ("x", "y", "z", "vx", "vy", "vz")])
+    assert np.array_equal(got, expect)
