@@ -36,6 +36,7 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
     const int tid = threadIdx.x;
     const int tb = a.leaf_off[leaf];
     const int nt = a.leaf_off[leaf + 1] - tb;
+    if (nt <= 0) return;  // block-uniform: an empty row has no targets
     const int nb = a.near_off[leaf], ne = a.near_off[leaf + 1];
     const int L = (MODE == kF64Exact) ? 1 : lanes_for(nt);
     const int slots = kP2PBlock / L;
