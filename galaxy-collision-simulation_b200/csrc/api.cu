@@ -18,6 +18,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <initializer_list>
 #include <map>
 #include <mutex>
@@ -186,12 +187,26 @@ bool eps0_of(int precision, const gx_physics& ph) {
     return e2 < 1e-200;
 }
 
-// Device scratch obtained from the stream-ordered pool and returned at scope exit.
+// Device scratch obtained from the stream-ordered pool and returned (stream-ordered) at
+// scope exit.  Move-only: a copy would free the allocation twice.
 struct AsyncBuf {
     void* p = nullptr;
     cudaStream_t st = nullptr;
+    AsyncBuf() = default;
+    AsyncBuf(const AsyncBuf&) = delete;
+    AsyncBuf& operator=(const AsyncBuf&) = delete;
+    AsyncBuf(AsyncBuf&& o) noexcept : p(o.p), st(o.st) { o.p = nullptr; }
+    AsyncBuf& operator=(AsyncBuf&& o) noexcept {
+        if (this != &o) {
+            if (p) cudaFreeAsync(p, st);
+            p = o.p;
+            st = o.st;
+            o.p = nullptr;
+        }
+        return *this;
+    }
     ~AsyncBuf() {
-        if (p) cudaFreeAsync(p, st);
+        if (p && cudaFreeAsync(p, st) != cudaSuccess) cudaGetLastError();  // nothing to report to
     }
     int alloc(size_t bytes, cudaStream_t s) {
         st = s;
@@ -359,6 +374,7 @@ int run_force(const ForceJob& j, const gx_physics& ph, int precision, Choice ch,
         part = tmp.d();
     }
     const ForceArgs a = make_args(j, ph, v, ch.nsplit, part);
+    GX_CUDA(cudaPeekAtLastError());  // a sticky error from earlier work surfaces here, not as a launch error
     GX_CUDA(force_launch(v, a, st));
     return GX_OK;
 }
@@ -368,7 +384,7 @@ int run_force(const ForceJob& j, const gx_physics& ph, int precision, Choice ch,
 // ======================================================================================
 struct HostStage {
     cudaStream_t st;
-    std::vector<AsyncBuf> bufs;
+    std::deque<AsyncBuf> bufs;  // stable addresses; released in reverse order at scope exit
     explicit HostStage(cudaStream_t s) : st(s) {}
     // Device copy of a host array (nullptr stays nullptr).
     int in(const double* h, int64_t n, double** d) {

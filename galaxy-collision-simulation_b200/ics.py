@@ -35,6 +35,8 @@ def _truncated_exponential_radii(u: np.ndarray, scale: float, rmax: float) -> np
 def exponential_disk(n: int, mass: float, rng: np.random.Generator, softening: float, G: float = 1.0,
                      scale: float = 1.0, rmax: float = 5.0, sigma_z: float = 0.05):
     """Positions (n,3), velocities (n,3), masses (n,) of one face-on disk centred at 0."""
+    if n <= 0:
+        return np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0)
     r = _truncated_exponential_radii(rng.random(n), scale, rmax)
     th = 2.0 * np.pi * rng.random(n)
     z = sigma_z * rng.standard_normal(n)
