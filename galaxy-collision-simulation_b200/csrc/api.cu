@@ -374,7 +374,7 @@ int run_force(const ForceJob& j, const gx_physics& ph, int precision, Choice ch,
         part = tmp.d();
     }
     const ForceArgs a = make_args(j, ph, v, ch.nsplit, part);
-    GX_CUDA(cudaPeekAtLastError());  // a sticky error from earlier work surfaces here, not as a launch error
+    (void)cudaGetLastError();  // drop a stale non-sticky error of unrelated earlier work; sticky ones resurface below
     GX_CUDA(force_launch(v, a, st));
     return GX_OK;
 }
