@@ -122,6 +122,7 @@ _SIGNATURES = {
     "gx_batch_enable_timing": [P, c_int],
     "gx_batch_force_timing": [P, POINTER(D), POINTER(I64)],
     "gx_direct_vjp": [I64, P, P, P, P, P, P, P, Physics, c_int, P, P, P, P, S],
+    "gx_direct_accel_noalloc": [I64, P, P, P, P, Physics, c_int, P, P, P, S],
     "gx_variant_count": [c_int, POINTER(c_int)],
     "gx_variant_describe": [c_int, c_int, c_char_p, c_int],
     "gx_debug_fail_allocations": [c_int],

@@ -1872,3 +1872,81 @@ extern "C" int gx_batch_accel(int32_t n_instances, const int64_t* offsets, const
     return r;
     GX_GUARD_END
 }
+
+// ======================================================================================
+// direct sum that allocates nothing
+// ======================================================================================
+// Some callers cannot allocate device memory when they call in: a process whose GPU memory
+// is entirely reserved up front by another framework's caching allocator, a real-time step
+// loop that must never enter the allocator, or code that runs while a stream is being
+// captured with allocation forbidden.  gx_direct_accel_noalloc serves them: it runs the same
+// tiled, source-split direct sum as gx_direct_accel on the caller's device arrays, but keeps
+// the split's partial sums in one fixed file-scope device array instead of allocating
+// scratch.  The array is part of the library's device image, so every GPU that loads the
+// library holds it (12 MiB) until the process exits.
+namespace {
+
+constexpr int64_t kNoAllocMaxBodies = 65536;  // largest n this entry point accepts
+constexpr int kNoAllocMaxSplit = 8;           // source chunks whose partials the array holds
+constexpr size_t kNoAllocScratchDoubles = (size_t)kNoAllocMaxSplit * 3 * (size_t)kNoAllocMaxBodies;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+std::mutex g_noalloc_mu;
+std::map<int, double*> g_noalloc_addr;  // device ordinal -> device address of the array
+
+// The array's name is only a host-side stand-in in host code; its device address is looked
+// up once per device, with that device current, and reused.
+int noalloc_scratch(int dev, double** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    auto it = g_noalloc_addr.find(dev);
+    if (it != g_noalloc_addr.end()) {
+        *out = it->second;
+        return GX_OK;
+    }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress (gx_direct_accel_noalloc scratch)");
+    g_noalloc_addr[dev] = (double*)p;
+    *out = (double*)p;
+    return GX_OK;
+}
+
+}  // namespace
+
+extern "C" int gx_direct_accel_noalloc(int64_t n, const double* x, const double* y, const double* z,
+                                       const double* m, gx_physics phys, int precision, double* ax, double* ay,
+                                       double* az, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_direct_accel_noalloc";
+    if (n < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n < 0", fn);
+    if (n > kNoAllocMaxBodies)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: n = %lld exceeds the fixed scratch limit of %lld bodies",
+                    fn, (long long)n, (long long)kNoAllocMaxBodies);
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision %d", fn, precision);
+    GX_TRY(check_phys(phys, fn));
+    if (n > 0 && (!x || !y || !z || !m || !ax || !ay || !az)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    if (n == 0) return GX_OK;
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, ax, ay, az}, &device, &dev, fn));
+    if (!device)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: device arrays only (host arrays would need staging buffers)", fn);
+    DeviceGuard guard(dev);
+    double* scratch = nullptr;
+    GX_TRY(noalloc_scratch(dev, &scratch));
+    int cnt;
+    const ForceVariant* all = force_variants(&cnt);
+    Choice ch = heuristic_choice(dev, precision, eps0_of(precision, phys), n, n);
+    ch.nsplit = std::min(ch.nsplit, kNoAllocMaxSplit);
+    const ForceVariant& v = all[ch.variant];
+    ForceJob j{x, y, z, m, n, nullptr, 0, n, ax, ay, az, nullptr, nullptr, nullptr, 0.0};
+    const ForceArgs a = make_args(j, phys, v, ch.nsplit, scratch);
+    if ((size_t)a.nsplit * 3 * (size_t)n > kNoAllocScratchDoubles)
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: partial sums exceed the fixed scratch array", fn);
+    (void)cudaGetLastError();
+    GX_CUDA(force_launch(v, a, (cudaStream_t)stream));
+    return GX_OK;
+    GX_GUARD_END
+}

@@ -226,6 +226,21 @@ int gx_direct_vjp(int64_t n, const double* x, const double* y, const double* z,
                   gx_physics phys, int precision, double* gx, double* gy, double* gz,
                   double* gm, void* stream);
 
+/* ---- direct sum without allocation (no counterpart in the reference) ---------------- */
+/* For callers that cannot allocate device memory at call time (memory reserved up front by
+ * another allocator, real-time loops that must stay out of the allocator, code running under
+ * a stream capture that forbids allocation).  Same result as gx_direct_accel on DEVICE arrays,
+ * but the partial sums of the source split live in one fixed 12 MiB device array that is part
+ * of the library (held by every GPU that loads it until exit) -- nothing is allocated or freed.
+ * Limits: n <= 65536 (larger n returns GX_ERR_INVALID_ARGUMENT); device pointers only.  The
+ * first call on a device looks up the array's device address; make that first call before any
+ * stream capture.  Every call shares the array and it keeps the last call's contents (each
+ * call overwrites every element it reads, so nothing needs clearing); calls that overlap on
+ * the GPU -- on different streams, or different host threads -- race on it. */
+int gx_direct_accel_noalloc(int64_t n, const double* x, const double* y, const double* z,
+                            const double* m, gx_physics phys, int precision, double* ax,
+                            double* ay, double* az, void* stream);
+
 /* ---- kernel variants ---------------------------------------------------------------- */
 /* Number of direct-force variants for a precision and a printable description. */
 int gx_variant_count(int precision, int* count);
