@@ -116,6 +116,17 @@ class ClockSampler:
                 "power_w_max": max(r["power"] for r in rows)}
 
 
+def other_gpu_processes():
+    """Compute processes on the visible GPUs other than this one (another tenant would skew timing)."""
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-compute-apps=pid", "--format=csv,noheader"],
+                             capture_output=True, text=True, timeout=10).stdout
+    except Exception:
+        return None
+    pids = [int(x) for x in out.split() if x.strip().isdigit()]
+    return len([p for p in pids if p != os.getpid()])
+
+
 # ---------------------------------------------------------------------------------------
 # CPU baseline: the reference's own per-target direct sum on the host cores
 # ---------------------------------------------------------------------------------------
@@ -176,6 +187,8 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "f64"], default="mixed")
     ap.add_argument("--quick", action="store_true", help="kernel timing only (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--variant", type=int, default=None, help="force a kernel variant id (skips autotuning)")
+    ap.add_argument("--jsplit", type=int, default=None, help="source split used with --variant")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
@@ -232,7 +245,9 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
     sess.set_stream(stream)
     sess.set_particles(p)
     tune_ms = None
-    if not args.no_autotune and not args.quick:
+    if args.variant is not None:
+        sess.set_config(prec, args.variant, args.jsplit or 1)
+    elif not args.no_autotune and not args.quick:
         tune_ms = sess.autotune(prec)
     variant, jsplit = sess.get_config(prec)
     sess.compute_accelerations(prec)  # the initial force evaluation
@@ -264,7 +279,8 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
     force_avg_s = force_ms / 1e3 / max(force_launches, 1)
     launches_per_step = 2 + (1 if jsplit > 1 else 0)
     out.update({"value": value, "ms_per_step": sum(step_ms) / args.steps, "steps_per_s": args.steps / total_s,
-                "gpu_launches": args.steps * launches_per_step})
+                "gpu_launches": args.steps * launches_per_step, "step_ms": [round(t, 3) for t in step_ms],
+                "other_gpu_processes": other_gpu_processes()})
     fp32_peak = sms * FP32_LANES_PER_SM * sm_max_mhz * 1e6 / 1e12
     achieved = pairs * FMA_PIPE_OPS_PER_INTERACTION / force_avg_s / 1e12
     roof = {"bound": "fp32_fma_pipe", "achieved": achieved,
