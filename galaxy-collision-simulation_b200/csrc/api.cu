@@ -461,7 +461,8 @@ extern "C" int gx_variant_describe(int precision, int variant, char* buf, int bu
     const ForceVariant& v = all[variant];
     const char* p = v.precision == kMixed ? "mixed" : v.precision == kF64 ? "f64" : "f64-exact";
     snprintf(buf, (size_t)buflen, "%s block=%d ipt=%d jt=%d%s%s", p, v.block, v.ipt, v.jt,
-             v.packed ? " f32x2" : "", v.eps0 && v.precision != kF64Exact ? " eps0" : "");
+             v.packed == 1 ? " f32x2" : v.packed == 2 ? " f32x2-targets" : "",
+             v.eps0 && v.precision != kF64Exact ? " eps0" : "");
     return GX_OK;
 }
 

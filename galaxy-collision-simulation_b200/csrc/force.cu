@@ -27,6 +27,11 @@ __global__ void __launch_bounds__(BLOCK) force_mixed_kernel(const ForceArgs a) {
     mixed_tile<BLOCK, IPT, JT, PACKED, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
 }
 
+template <int BLOCK, int IPT, int JT, bool EPS0, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) force_mixed_tp_kernel(const ForceArgs a) {
+    mixed_tp_tile<BLOCK, IPT, JT, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+}
+
 template <int BLOCK, int IPT, int JT, bool EPS0>
 __global__ void __launch_bounds__(BLOCK) force_f64_kernel(const ForceArgs a) {
     f64_tile<BLOCK, IPT, JT, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
@@ -38,18 +43,28 @@ __global__ void __launch_bounds__(BLOCK) force_exact_kernel(const ForceArgs a) {
 }
 
 #define MIXED(B, I, J, P, E) {kMixed, B, I, J, P, E, (const void*)&force_mixed_kernel<B, I, J, P, E>}
+#define MIXTP(B, I, J, E, MB) {kMixed, B, I, J, 2, E, (const void*)&force_mixed_tp_kernel<B, I, J, E, MB>}
 #define F64(B, I, J, E) {kF64, B, I, J, 0, E, (const void*)&force_f64_kernel<B, I, J, E>}
 #define EXACT(B, J) {kF64Exact, B, 1, J, 0, 1, (const void*)&force_exact_kernel<B, J>}
 
 const ForceVariant kVariants[] = {
+    MIXTP(128, 8, 512, false, 1),  // fastest measured at N = 2^20 (the untuned default)
+    MIXED(128, 8, 512, true, false),
     MIXED(256, 4, 512, true, false),
     MIXED(128, 4, 512, true, false),
     MIXED(256, 2, 512, true, false),
-    MIXED(128, 8, 512, true, false),
     MIXED(64, 4, 256, true, false),
     MIXED(256, 4, 512, false, false),
     MIXED(256, 4, 512, true, true),
     MIXED(64, 4, 256, true, true),
+    MIXTP(128, 8, 512, false, 3),
+    MIXTP(256, 8, 512, false, 1),
+    MIXTP(256, 6, 512, false, 1),
+    MIXTP(192, 8, 384, false, 2),
+    MIXTP(128, 12, 512, false, 1),
+    MIXTP(128, 6, 512, false, 4),
+    MIXTP(256, 4, 512, false, 2),
+    MIXTP(256, 4, 512, false, 3),
     F64(256, 2, 256, false),
     F64(128, 2, 256, false),
     F64(256, 1, 256, false),

@@ -41,7 +41,7 @@ struct ForceVariant {
     int block;
     int ipt;   // targets per thread
     int jt;    // j tile (sources staged per shared-memory pass)
-    int packed;
+    int packed;  // 0 scalar FP32, 1 two sources per f32x2, 2 two targets per f32x2
     int eps0;  // guards s == 0 pairs (softening 0)
     const void* fn;
 };

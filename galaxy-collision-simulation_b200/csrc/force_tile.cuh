@@ -254,6 +254,158 @@ __device__ __forceinline__ void mixed_tile(const ForceArgs& a, const int64_t t0,
 }
 
 // ---------------------------------------------------------------------------------------
+// Mixed precision, targets packed: the same arithmetic as mixed_tile, but each packed
+// .f32x2 instruction serves two TARGETS against one source.  Sources are staged in shared
+// memory already duplicated ((x, x, y, y), (z, z, m, m): two 16-byte loads per source), so a
+// target pair keeps one 64-bit register per coordinate and per accumulator instead of two:
+// 6 registers fewer per target, which buys occupancy or more targets per thread.
+// ---------------------------------------------------------------------------------------
+template <int BLOCK, int IPT, int JT, bool EPS0>
+__device__ __forceinline__ void mixed_tp_tile(const ForceArgs& a, const int64_t t0, const int chunk) {
+    static_assert(JT % BLOCK == 0 && BLOCK % 32 == 0 && IPT % 2 == 0, "tile shape");
+    constexpr int NW = BLOCK / 32;
+    constexpr int NP = IPT / 2;
+    __shared__ __align__(16) float4 sA[JT];  // (x, x, y, y)
+    __shared__ __align__(16) float4 sB[JT];  // (z, z, m, m)
+    __shared__ double sred[6][NW];
+
+    const int tid = threadIdx.x;
+    const int64_t first_body = target_body(a, t0);
+    double bx[IPT], by[IPT], bz[IPT];
+    int64_t body[IPT];
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        const int64_t t = t0 + k * BLOCK + tid;
+        body[k] = t < a.n_tgt ? target_body(a, t) : first_body;
+        bx[k] = a.x[body[k]];
+        by[k] = a.y[body[k]];
+        bz[k] = a.z[body[k]];
+        lo[0] = fmin(lo[0], bx[k]); hi[0] = fmax(hi[0], bx[k]);
+        lo[1] = fmin(lo[1], by[k]); hi[1] = fmax(hi[1], by[k]);
+        lo[2] = fmin(lo[2], bz[k]); hi[2] = fmax(hi[2], bz[k]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        lo[c] = warp_min(lo[c]);
+        hi[c] = warp_max(hi[c]);
+    }
+    if ((tid & 31) == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            sred[c][tid >> 5] = lo[c];
+            sred[3 + c][tid >> 5] = hi[c];
+        }
+    }
+    __syncthreads();
+    double org[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double l = sred[c][0], h = sred[3 + c][0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) {
+            l = fmin(l, sred[c][w]);
+            h = fmax(h, sred[3 + c][w]);
+        }
+        org[c] = 0.5 * (l + h);
+    }
+
+    f2 XI[NP], YI[NP], ZI[NP];
+    CompF cx[IPT], cy[IPT], cz[IPT];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+        XI[q] = pk2(__double2float_rn(bx[2 * q] - org[0]), __double2float_rn(bx[2 * q + 1] - org[0]));
+        YI[q] = pk2(__double2float_rn(by[2 * q] - org[1]), __double2float_rn(by[2 * q + 1] - org[1]));
+        ZI[q] = pk2(__double2float_rn(bz[2 * q] - org[2]), __double2float_rn(bz[2 * q + 1] - org[2]));
+    }
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        cx[k].init();
+        cy[k].init();
+        cz[k].init();
+    }
+
+    const int64_t jb = (int64_t)chunk * a.j_chunk;
+    const int64_t je = min(a.n_src, jb + a.j_chunk);
+    const f2 E2 = pk2(a.eps2f, a.eps2f);
+    const f2 Z0 = pk2(0.f, 0.f);
+
+    for (int64_t j0 = jb; j0 < je; j0 += JT) {
+#pragma unroll
+        for (int r = 0; r < JT / BLOCK; ++r) {
+            const int jj = r * BLOCK + tid;
+            const int64_t j = j0 + jj;
+            float qx = 0.f, qy = 0.f, qz = 0.f, qm = 0.f;
+            if (j < je) {
+                qx = __double2float_rn(a.x[j] - org[0]);
+                qy = __double2float_rn(a.y[j] - org[1]);
+                qz = __double2float_rn(a.z[j] - org[2]);
+                qm = __double2float_rn(a.m[j]);
+            }
+            sA[jj] = make_float4(qx, qx, qy, qy);
+            sB[jj] = make_float4(qz, qz, qm, qm);
+        }
+        __syncthreads();
+        f2 PX[NP], PY[NP], PZ[NP];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) PX[q] = PY[q] = PZ[q] = Z0;
+#pragma unroll 4
+        for (int jj = 0; jj < JT; ++jj) {
+            f2 X, Y, Z, M;
+            lds_v2b64(reinterpret_cast<const float*>(&sA[jj]), X, Y);
+            lds_v2b64(reinterpret_cast<const float*>(&sB[jj]), Z, M);
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const f2 dX = sub2(X, XI[q]);
+                const f2 dY = sub2(Y, YI[q]);
+                const f2 dZ = sub2(Z, ZI[q]);
+                f2 R = fma2(dX, dX, E2);
+                R = fma2(dY, dY, R);
+                R = fma2(dZ, dZ, R);
+                float r0, r1;
+                upk2(R, r0, r1);
+                float i0 = rsqrt_f32(r0), i1 = rsqrt_f32(r1);
+                if (EPS0) {
+                    i0 = (r0 == 0.f) ? 0.f : i0;
+                    i1 = (r1 == 0.f) ? 0.f : i1;
+                }
+                const f2 I = pk2(i0, i1);
+                f2 T = mul2(I, I);
+                T = mul2(T, I);
+                const f2 W = mul2(M, T);
+                PX[q] = fma2(dX, W, PX[q]);
+                PY[q] = fma2(dY, W, PY[q]);
+                PZ[q] = fma2(dZ, W, PZ[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            float p0, p1;
+            upk2(PX[q], p0, p1);
+            cx[2 * q].add(p0);
+            cx[2 * q + 1].add(p1);
+            upk2(PY[q], p0, p1);
+            cy[2 * q].add(p0);
+            cy[2 * q + 1].add(p1);
+            upk2(PZ[q], p0, p1);
+            cz[2 * q].add(p0);
+            cz[2 * q + 1].add(p1);
+        }
+        __syncthreads();
+    }
+
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        const int64_t t = t0 + k * BLOCK + tid;
+        if (t >= a.n_tgt) continue;
+        if (a.nsplit == 1)
+            write_result(a, t, body[k], a.G * cx[k].value(), a.G * cy[k].value(), a.G * cz[k].value());
+        else
+            write_partial(a, chunk, t, cx[k].value(), cy[k].value(), cz[k].value());
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // FP64 with a refined hardware rsqrt.
 // ---------------------------------------------------------------------------------------
 template <int BLOCK, int IPT, int JT, bool EPS0>

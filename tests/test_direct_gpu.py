@@ -97,7 +97,7 @@ def test_every_variant_and_split(prec):
     count = 0
     with gx.Session(n, gx.PhysicsParams(1.0, 0.02)) as s:
         s.set_particles(p)
-        for v in range(17):
+        for v in range(64):
             try:
                 desc = gx.describe_variant(prec, v)
             except gx.GxError:
