@@ -51,18 +51,12 @@ const ForceVariant kVariants[] = {
     MIXTP(128, 8, 512, false, 1),  // fastest measured at N = 2^20 (the untuned default)
     MIXED(128, 8, 512, true, false),
     MIXED(256, 4, 512, true, false),
-    MIXED(128, 4, 512, true, false),
-    MIXED(256, 2, 512, true, false),
     MIXED(64, 4, 256, true, false),
     MIXED(256, 4, 512, false, false),
     MIXED(256, 4, 512, true, true),
     MIXED(64, 4, 256, true, true),
     MIXTP(128, 8, 512, false, 3),
-    MIXTP(256, 8, 512, false, 1),
     MIXTP(256, 6, 512, false, 1),
-    MIXTP(192, 8, 384, false, 2),
-    MIXTP(128, 12, 512, false, 1),
-    MIXTP(128, 6, 512, false, 4),
     MIXTP(256, 4, 512, false, 2),
     MIXTP(256, 4, 512, false, 3),
     F64(256, 2, 256, false),
