@@ -190,6 +190,9 @@ def main():
     ap.add_argument("--variant", type=int, default=None, help="force a kernel variant id (skips autotuning)")
     ap.add_argument("--jsplit", type=int, default=None, help="source split used with --variant")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--workload", default="mixed-n1048576",
+                    choices=["mixed-n1048576", "ensemble", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
+                    help="headline (default) or one of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
 
@@ -201,6 +204,12 @@ def main():
 
     if args.impl == "reference":
         return reference_arm(args, rank, n, eps, dt)
+    if args.workload != "mixed-n1048576":
+        import torch
+        torch.cuda.set_device(local)
+        res = OTHER_WORKLOADS[args.workload](load_gx(), torch, args)
+        print(json.dumps(res), flush=True)
+        return
 
     import torch
     import torch.distributed as dist
@@ -474,6 +483,159 @@ def run_sharded(gx, torch, dist, p, args, rank, world, eps, dt, prec) -> dict:
             "config": {"workload": f"direct-mixed-n{n}", "n": n, "parallelism": f"targets{world}",
                        "exchange": "NCCL all-gather of FP64 positions (24 B/body/step)", "softening": eps, "dt": dt,
                        "l2": "state 80 MiB < L2; not flushed in the multi-GPU run (one exchange per step)"}}
+
+
+# ---------------------------------------------------------------------------------------
+# the other configurations (one JSON line each; not the headline)
+# ---------------------------------------------------------------------------------------
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def wl_ensemble(gx, torch, args) -> dict:
+    """512 independent encounters, N_b ~ U[1024, 16384], 200 KDK steps in one graph-captured
+    run of the persistent batched kernel, mixed precision, autotuned."""
+    off, p, meta = gx.ics.ensemble(512, seed=7)
+    steps = args.steps if args.steps != 10 else 200
+    pairs = float(np.sum(np.diff(off).astype(np.float64) * (np.diff(off) - 1)))
+    b = gx.Batch(off, gx.PhysicsParams(1.0, 0.05))
+    b.set_state(p.x, p.y, p.z, p.vx, p.vy, p.vz, p.m)
+    tune = b.autotune(gx.PRECISION_MIXED)
+    b.compute_accelerations(gx.PRECISION_MIXED)
+    d0 = b.diagnostics()
+    b.step(args.warmup, 0.005, gx.PRECISION_MIXED)
+    b.synchronize()
+    st = torch.cuda.Stream()
+    b.set_stream(st)
+    a, e = _events(torch)
+    a.record(st)
+    b.step(steps, 0.005, gx.PRECISION_MIXED)
+    e.record(st)
+    e.synchronize()
+    ms = a.elapsed_time(e)
+    d1 = b.diagnostics()
+    drift = [abs(x.total_energy - y.total_energy) / abs(y.total_energy) for x, y in zip(d1, d0)]
+    v = b.get_config(gx.PRECISION_MIXED)
+    b.close()
+    return {"metric": "Ginteractions/s (batched ensemble)", "value": steps * pairs / (ms / 1e3) / 1e9,
+            "unit": UNIT, "ms_per_step": ms / steps, "steps": steps, "instances": 512, "bodies": int(off[-1]),
+            "interactions_per_step": pairs, "autotune_ms_per_eval": tune, "kernel_variant": v,
+            "energy_drift": {"median": float(np.median(drift)), "max": float(np.max(drift))},
+            "config": {"workload": "ensemble-512", "dt": 0.005, "softening": 0.05, "precision": "mixed",
+                       "launch": "one CUDA graph of all steps (kick_drift + persistent force per step)"}}
+
+
+def wl_p2p(gx, torch, args) -> dict:
+    """FMM near field of the N = 65,536 two-disk workload: reference octree leaf lists
+    (leaf_capacity 64, theta 0.6) built on the host, P2P on the device."""
+    n = 65536
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, 0.02)
+    t0 = time.perf_counter()
+    lists = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 64)
+    build_s = time.perf_counter() - t0
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    dl = gx.LeafLists(T(lists.leaf_offsets), T(lists.leaf_particles), T(lists.near_offsets), T(lists.near_leaves))
+    X = {k: T(getattr(p, k)) for k in ("x", "y", "z", "m")}
+    acc = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(3)]
+    params = gx.PhysicsParams(1.0, 0.02)
+    # ordered source-target pairs minus self pairs
+    pairs = lists.n_pairs - n
+    out = {"metric": "Ginteractions/s (FMM P2P leaves)", "unit": UNIT, "n": n, "leaves": lists.n_leaves,
+           "near_pairs_of_leaves": int(len(lists.near_leaves)), "interactions": int(pairs),
+           "host_leaf_list_build_s": build_s, "config": {"workload": "p2p-n65536", "leaf_capacity": 64, "theta": 0.6}}
+    for name, prec in (("f64", gx.PRECISION_F64), ("mixed", gx.PRECISION_MIXED), ("f64_exact", gx.PRECISION_F64_EXACT)):
+        for _ in range(3):
+            gx.p2p_leaves(X["x"], X["y"], X["z"], X["m"], dl, params, *acc, prec)
+        a, e = _events(torch)
+        a.record()
+        reps = 20
+        for _ in range(reps):
+            gx.p2p_leaves(X["x"], X["y"], X["z"], X["m"], dl, params, *acc, prec)
+        e.record()
+        e.synchronize()
+        ms = a.elapsed_time(e) / reps
+        out[name] = {"ms": ms, "value": pairs / (ms / 1e3) / 1e9}
+    out["value"] = out["f64"]["value"]
+    return out
+
+
+def wl_direct(gx, torch, args, n, eps, dt, steps) -> dict:
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps)
+    params = gx.PhysicsParams(1.0, eps)
+    out = {"metric": f"Ginteractions/s (direct, N={n})", "unit": UNIT, "n": n, "steps": steps,
+           "config": {"workload": f"direct-n{n}", "softening": eps, "dt": dt}}
+    for name, prec in (("f64", gx.PRECISION_F64), ("mixed", gx.PRECISION_MIXED), ("f64_exact", gx.PRECISION_F64_EXACT)):
+        s = gx.Session(n, params)
+        s.set_particles(p)
+        if name != "f64_exact":
+            s.autotune(prec)
+        s.compute_accelerations(prec)
+        e0 = s.diagnostics().total_energy
+        s.step(3, dt, prec)
+        s.synchronize()
+        st = torch.cuda.Stream()
+        s.set_stream(st)
+        a, e = _events(torch)
+        a.record(st)
+        s.step(steps, dt, prec)
+        e.record(st)
+        e.synchronize()
+        ms = a.elapsed_time(e)
+        e1 = s.diagnostics().total_energy
+        out[name] = {"ms_per_step": ms / steps, "value": steps * n * (n - 1) / (ms / 1e3) / 1e9,
+                     "steps_per_s": steps / (ms / 1e3), "energy_drift": abs(e1 - e0) / abs(e0),
+                     "kernel": gx.describe_variant(prec, s.get_config(prec)[0])}
+        s.close()
+    out["value"] = out["mixed"]["value"]
+    return out
+
+
+def wl_fit(gx, torch, args) -> dict:
+    """Differentiable encounter: N = 16,384, 500 KDK steps, checkpoint every 50; forward and
+    backward (adjoint) of the loss over the 6 orbit parameters and all initial positions."""
+    from gx import adjoint
+
+    n, steps, dt, K = 16384, 500, 0.005, 50
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 16384, 0.05)
+    params = gx.PhysicsParams(1.0, 0.05)
+    pos = torch.tensor(p.positions, device="cuda")
+    vel = torch.tensor(p.velocities, device="cuda")
+    m = torch.tensor(p.m, device="cuda")
+    disk2 = torch.tensor(p.group_id == 1, device="cuda")
+    truth = torch.tensor([0.04, -0.02, 0.03, 0.02, -0.01, 0.01], dtype=torch.float64, device="cuda")
+    res = {"metric": "adjoint/forward cost (differentiable fit)", "unit": "ratio", "n": n, "steps": steps,
+           "checkpoint_every": K, "config": {"workload": "fit-n16384", "dt": dt, "softening": 0.05}}
+    for name, prec in (("mixed", gx.PRECISION_MIXED), ("f64", gx.PRECISION_F64)):
+        with torch.no_grad():
+            x0t, v0t = adjoint.encounter_initial_state(pos, vel, disk2, truth)
+            target, _ = adjoint.leapfrog(x0t, v0t, m, steps, dt, params, K, prec)
+        orbit = torch.zeros(6, dtype=torch.float64, device="cuda", requires_grad=True)
+        x0 = pos.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xs, vs = adjoint.encounter_initial_state(x0, vel, disk2, orbit)
+        xT, _ = adjoint.leapfrog(xs, vs, m, steps, dt, params, K, prec)
+        loss = ((xT - target) ** 2).sum(1).mean()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        fwd, bwd = t1 - t0, t2 - t1
+        res[name] = {"forward_s": fwd, "backward_s": bwd, "backward_over_forward": bwd / fwd,
+                     "adjoint_over_forward_excl_recompute": (bwd - fwd) / fwd, "loss": float(loss)}
+    res["adjoint_step"] = adjoint_ratio(gx, torch)
+    res["value"] = res["adjoint_step"]["ratio"]
+    return res
+
+
+OTHER_WORKLOADS = {
+    "ensemble": wl_ensemble,
+    "p2p-n65536": wl_p2p,
+    "direct-n65536": lambda gx, torch, args: wl_direct(gx, torch, args, 65536, 0.02, 0.002, 100),
+    "direct-n1000": lambda gx, torch, args: wl_direct(gx, torch, args, 1000, 0.05, 0.005, 20),
+    "fit-n16384": wl_fit,
+}
 
 
 def reference_arm(args, rank, n, eps, dt):
