@@ -196,15 +196,7 @@ struct AsyncBuf {
     AsyncBuf(const AsyncBuf&) = delete;
     AsyncBuf& operator=(const AsyncBuf&) = delete;
     AsyncBuf(AsyncBuf&& o) noexcept : p(o.p), st(o.st) { o.p = nullptr; }
-    AsyncBuf& operator=(AsyncBuf&& o) noexcept {
-        if (this != &o) {
-            if (p) cudaFreeAsync(p, st);
-            p = o.p;
-            st = o.st;
-            o.p = nullptr;
-        }
-        return *this;
-    }
+    AsyncBuf& operator=(AsyncBuf&&) = delete;
     ~AsyncBuf() {
         if (p && cudaFreeAsync(p, st) != cudaSuccess) cudaGetLastError();  // nothing to report to
     }
@@ -1205,11 +1197,13 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
     a.G = phys.G;
     a.eps2 = phys.softening * phys.softening;
     a.eps2f = (float)a.eps2;
+    AsyncBuf scratch;
+    GX_TRY(scratch.alloc(p2p_scratch_bytes(n, n_leaves), st));
     if (device) {
         a.x = x; a.y = y; a.z = z; a.m = m;
         a.leaf_off = leaf_offsets; a.leaf_part = leaf_particles; a.near_off = near_offsets; a.near_leaf = near_leaves;
         a.ax = ax; a.ay = ay; a.az = az;
-        GX_CUDA(launch_p2p(a, precision, st));
+        GX_CUDA(launch_p2p(a, n, precision, scratch.p, sm_count(dev), st));
         return GX_OK;
     }
     // Host arrays: validate the CSR (the kernel trusts it), then stage.
@@ -1241,7 +1235,7 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
     a.x = dx; a.y = dy; a.z = dz; a.m = dm;
     a.leaf_off = dlo; a.leaf_part = dlp; a.near_off = dno; a.near_leaf = dnl;
     a.ax = dax; a.ay = day; a.az = daz;
-    GX_CUDA(launch_p2p(a, precision, st));
+    GX_CUDA(launch_p2p(a, n, precision, scratch.p, sm_count(dev), st));
     GX_TRY(copy_back(ax, dax, n, st));
     GX_TRY(copy_back(ay, day, n, st));
     GX_TRY(copy_back(az, daz, n, st));

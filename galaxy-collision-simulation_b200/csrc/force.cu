@@ -27,9 +27,9 @@ __global__ void __launch_bounds__(BLOCK) force_mixed_kernel(const ForceArgs a) {
     mixed_tile<BLOCK, IPT, JT, PACKED, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
 }
 
-template <int BLOCK, int IPT, int JT, bool EPS0, int MINB>
+template <int BLOCK, int IPT, int JT, bool EPS0, int MINB, int UNROLL = 4>
 __global__ void __launch_bounds__(BLOCK, MINB) force_mixed_tp_kernel(const ForceArgs a) {
-    mixed_tp_tile<BLOCK, IPT, JT, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+    mixed_tp_tile<BLOCK, IPT, JT, EPS0, UNROLL>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
 }
 
 template <int BLOCK, int IPT, int JT, bool EPS0>
@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(BLOCK) force_exact_kernel(const ForceArgs a) {
 
 #define MIXED(B, I, J, P, E) {kMixed, B, I, J, P, E, (const void*)&force_mixed_kernel<B, I, J, P, E>}
 #define MIXTP(B, I, J, E, MB) {kMixed, B, I, J, 2, E, (const void*)&force_mixed_tp_kernel<B, I, J, E, MB>}
+#define MIXTPU(B, I, J, MB, U) {kMixed, B, I, J, 2, 0, (const void*)&force_mixed_tp_kernel<B, I, J, false, MB, U>}
 #define F64(B, I, J, E) {kF64, B, I, J, 0, E, (const void*)&force_f64_kernel<B, I, J, E>}
 #define EXACT(B, J) {kF64Exact, B, 1, J, 0, 1, (const void*)&force_exact_kernel<B, J>}
 
@@ -59,6 +60,12 @@ const ForceVariant kVariants[] = {
     MIXTP(256, 6, 512, false, 1),
     MIXTP(256, 4, 512, false, 2),
     MIXTP(256, 4, 512, false, 3),
+    MIXTPU(128, 8, 512, 1, 8),
+    MIXTPU(128, 8, 512, 1, 16),
+    MIXTPU(256, 6, 512, 1, 8),
+    MIXTPU(256, 4, 512, 2, 8),
+    MIXTPU(256, 4, 512, 2, 16),
+    MIXTPU(128, 6, 512, 2, 16),
     F64(256, 2, 256, false),
     F64(128, 2, 256, false),
     F64(256, 1, 256, false),

@@ -260,7 +260,7 @@ __device__ __forceinline__ void mixed_tile(const ForceArgs& a, const int64_t t0,
 // target pair keeps one 64-bit register per coordinate and per accumulator instead of two:
 // 6 registers fewer per target, which buys occupancy or more targets per thread.
 // ---------------------------------------------------------------------------------------
-template <int BLOCK, int IPT, int JT, bool EPS0>
+template <int BLOCK, int IPT, int JT, bool EPS0, int UNROLL = 4>
 __device__ __forceinline__ void mixed_tp_tile(const ForceArgs& a, const int64_t t0, const int chunk) {
     static_assert(JT % BLOCK == 0 && BLOCK % 32 == 0 && IPT % 2 == 0, "tile shape");
     constexpr int NW = BLOCK / 32;
@@ -349,7 +349,7 @@ __device__ __forceinline__ void mixed_tp_tile(const ForceArgs& a, const int64_t 
         f2 PX[NP], PY[NP], PZ[NP];
 #pragma unroll
         for (int q = 0; q < NP; ++q) PX[q] = PY[q] = PZ[q] = Z0;
-#pragma unroll 4
+#pragma unroll UNROLL
         for (int jj = 0; jj < JT; ++jj) {
             f2 X, Y, Z, M;
             lds_v2b64(reinterpret_cast<const float*>(&sA[jj]), X, Y);

@@ -4,13 +4,24 @@
 // (cpp/fmm/fmm_solver.cpp:295-310): for every body i of a target leaf, the pair terms of
 // all bodies j != i of the leaf's near leaves, in near-list order and leaf body order.
 //
-// One CTA per target leaf.  The bodies of the near leaves are gathered (by index, from the
-// SoA state) into shared memory JT at a time.  In the fast forms each target is served by
-// L adjacent lanes (L = 8, 4, 2, 1 for leaves of <= 16, 32, 64, more bodies) that split the
-// staged sources and are combined with warp shuffles at the end, so small leaves still
-// fill the CTA.  The exact form uses one lane per target and walks the sources in the
-// reference's order starting from the incoming acceleration (the far field), which makes
-// it bit-identical to the reference's evaluate_particle.
+// Work decomposition.  The bodies of a target leaf's near leaves form one source sequence
+// (near-list order, then leaf order).  Leaf costs are very uneven (in the N = 65,536
+// two-disk tree the heaviest leaf has 13x the mean number of sources), so a leaf's sequence
+// is cut into at most kMaxChunks chunks of at least kMinChunk sources.  A plan computed on
+// the device (p2p_count_kernel + p2p_scan_kernel) numbers the (leaf, chunk) items; a
+// persistent grid takes items from a ticket counter.  A leaf with one chunk adds its sums to
+// the accelerations directly.  A split leaf writes per-chunk partial sums to scratch; the CTA
+// that finishes the leaf's last chunk (a per-leaf counter, after a memory fence) adds the
+// partials in chunk order -- no CTA ever waits for another, and the order of summation does
+// not depend on scheduling.
+//
+// Inside an item: a warp scan of the near leaves' sizes lets every thread gather its own
+// slots of the chunk (by index, from the SoA state) into shared memory JT at a time.  In the
+// fast forms each target is served by L adjacent lanes (L = 8, 4, 2, 1 for leaves of <= 16,
+// 32, 64, more bodies) that split the staged sources and are combined with warp shuffles.
+// The exact form uses one chunk per leaf and one lane per target and walks the sources in
+// the reference's order starting from the incoming acceleration (the far field), which
+// makes it bit-identical to the reference's evaluate_particle.
 #include "gx_device.cuh"
 #include "p2p.cuh"
 
@@ -18,10 +29,93 @@ namespace gx {
 namespace {
 
 constexpr int kP2PBlock = 128;
-constexpr int kP2PJT = 256;
+constexpr int kP2PJT = 512;      // sources staged per shared-memory pass
+constexpr int kNearBatch = 256;  // near leaves whose (start, length) sit in shared memory at once
+constexpr int kMaxChunks = 8;    // a leaf's source sequence is split into at most this many items
+constexpr int kMinChunk = 2048;  // ... of at least this many sources
+constexpr int kScanBlock = 1024;
 
 __device__ __forceinline__ int lanes_for(int nt) {
     return nt <= 16 ? 8 : nt <= 32 ? 4 : nt <= 64 ? 2 : 1;
+}
+
+// Per leaf: number of sources, number of chunks, scratch demand (split leaves only).
+__global__ void p2p_count_kernel(const P2PArgs a, int exact) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= a.n_leaves) return;
+    int64_t src = 0;
+    for (int q = a.near_off[l]; q < a.near_off[l + 1]; ++q) {
+        const int s = a.near_leaf[q];
+        src += a.leaf_off[s + 1] - a.leaf_off[s];
+    }
+    const int nt = a.leaf_off[l + 1] - a.leaf_off[l];
+    int chunks = 0;
+    if (nt > 0 && src > 0) {
+        const int64_t c = (src + kMinChunk - 1) / kMinChunk;
+        chunks = exact ? 1 : (int)(c < kMaxChunks ? c : kMaxChunks);
+    }
+    a.plan_src[l] = src;
+    a.plan_chunks[l] = chunks;
+    a.plan_scratch[l] = chunks > 1 ? (int64_t)chunks * nt : 0;
+}
+
+// Single-block exclusive scans: item offsets (plan_item_off, n_leaves + 1 entries) and
+// scratch offsets (plan_scratch rewritten in place as offsets, in units of targets).
+__global__ void __launch_bounds__(kScanBlock) p2p_scan_kernel(const P2PArgs a) {
+    __shared__ int64_t s_a[kScanBlock];
+    __shared__ int64_t s_b[kScanBlock];
+    const int n = a.n_leaves;
+    const int per = (n + kScanBlock - 1) / kScanBlock;
+    const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
+    int64_t ta = 0, tb = 0;
+    for (int l = b0; l < b1; ++l) {
+        ta += a.plan_chunks[l];
+        tb += a.plan_scratch[l];
+    }
+    s_a[threadIdx.x] = ta;
+    s_b[threadIdx.x] = tb;
+    __syncthreads();
+    // Capacity guard: if the split leaves would need more partial sums than the scratch holds
+    // (rows that repeat bodies can do that), every leaf falls back to a single chunk.
+    __shared__ int64_t s_demand;
+    if (threadIdx.x == 0) {
+        int64_t d = 0;
+        for (int w = 0; w < kScanBlock; ++w) d += s_b[w];
+        s_demand = d;
+    }
+    __syncthreads();
+    if (s_demand > a.scratch_capacity) {
+        ta = 0;
+        for (int l = b0; l < b1; ++l) {
+            if (a.plan_chunks[l] > 1) a.plan_chunks[l] = 1;
+            a.plan_scratch[l] = 0;
+            ta += a.plan_chunks[l];
+        }
+        s_a[threadIdx.x] = ta;
+        s_b[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    for (int o = 1; o < kScanBlock; o <<= 1) {  // Hillis-Steele inclusive scan
+        const int64_t va = threadIdx.x >= (unsigned)o ? s_a[threadIdx.x - o] : 0;
+        const int64_t vb = threadIdx.x >= (unsigned)o ? s_b[threadIdx.x - o] : 0;
+        __syncthreads();
+        s_a[threadIdx.x] += va;
+        s_b[threadIdx.x] += vb;
+        __syncthreads();
+    }
+    int64_t ra = threadIdx.x ? s_a[threadIdx.x - 1] : 0;
+    int64_t rb = threadIdx.x ? s_b[threadIdx.x - 1] : 0;
+    for (int l = b0; l < b1; ++l) {
+        const int64_t ca = a.plan_chunks[l], cb = a.plan_scratch[l];
+        a.plan_item_off[l] = (int)ra;
+        a.plan_scratch[l] = rb;
+        ra += ca;
+        rb += cb;
+    }
+    if (threadIdx.x == kScanBlock - 1) {
+        a.plan_item_off[n] = (int)s_a[kScanBlock - 1];
+        *a.plan_n_items = (int)s_a[kScanBlock - 1];
+    }
 }
 
 template <int MODE, bool EPS0>
@@ -31,144 +125,195 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
     __shared__ __align__(16) double szd[kP2PJT];
     __shared__ __align__(16) double smd[kP2PJT];
     __shared__ int sidx[kP2PJT];
+    __shared__ int s_beg[kNearBatch];
+    __shared__ int s_pre[kNearBatch + 1];
+    __shared__ int s_item, s_last;
 
-    const int leaf = blockIdx.x;
     const int tid = threadIdx.x;
-    const int tb = a.leaf_off[leaf];
-    const int nt = a.leaf_off[leaf + 1] - tb;
-    if (nt <= 0) return;  // block-uniform: an empty row has no targets
-    const int nb = a.near_off[leaf], ne = a.near_off[leaf + 1];
-    const int L = (MODE == kF64Exact) ? 1 : lanes_for(nt);
-    const int slots = kP2PBlock / L;
-    const int slot = tid / L, lane = tid % L;
-    // Origin of the mixed form: the leaf's first body (near sources are close to it).
-    const int first = a.leaf_part[tb];
-    const double ox = a.x[first], oy = a.y[first], oz = a.z[first];
-
-    for (int pass = 0; pass * slots < nt; ++pass) {
-        const int t = pass * slots + slot;
-        const bool ok = t < nt;
-        const int i = ok ? a.leaf_part[tb + t] : first;
-        const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
-        const float xf = __double2float_rn(xi - ox), yf = __double2float_rn(yi - oy),
-                    zf = __double2float_rn(zi - oz);
-        double fx = 0.0, fy = 0.0, fz = 0.0;
-        if (MODE == kF64Exact && ok) {
-            fx = a.ax[i];
-            fy = a.ay[i];
-            fz = a.az[i];
+    const int n_items = *a.plan_n_items;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(a.ticket, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= n_items) return;
+        // leaf owning the item: largest l with plan_item_off[l] <= item
+        int lo = 0, hi = a.n_leaves;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (a.plan_item_off[mid] <= item) lo = mid;
+            else hi = mid;
         }
-        CompF cx, cy, cz;
-        cx.init();
-        cy.init();
-        cz.init();
+        const int leaf = lo;
+        const int chunks = a.plan_chunks[leaf];
+        const int chunk = item - a.plan_item_off[leaf];
+        const int64_t src = a.plan_src[leaf];
+        const int64_t per = (src + chunks - 1) / chunks;
+        const int64_t c_lo = (int64_t)chunk * per;
+        const int64_t c_hi = min(src, c_lo + per);
 
-        int fill = 0;
-        auto compute = [&](int cnt) {
-            if (MODE == kF64Exact) {
-                for (int jj = 0; jj < cnt; ++jj) {
-                    if (sidx[jj] == i) continue;
-                    const double rx = dsub(sxd[jj], xi), ry = dsub(syd[jj], yi), rz = dsub(szd[jj], zi);
-                    const double s2 = dadd(dadd(dadd(dmul(rx, rx), dmul(ry, ry)), dmul(rz, rz)), a.eps2);
-                    if (s2 == 0.0) {
-                        fx = dadd(fx, 0.0);
-                        fy = dadd(fy, 0.0);
-                        fz = dadd(fz, 0.0);
-                        continue;
+        const int tb = a.leaf_off[leaf];
+        const int nt = a.leaf_off[leaf + 1] - tb;
+        const int nb = a.near_off[leaf], ne = a.near_off[leaf + 1];
+        const int L = (MODE == kF64Exact) ? 1 : lanes_for(nt);
+        const int slots = kP2PBlock / L;
+        const int slot = tid / L, lane = tid % L;
+        // Origin of the mixed form: the leaf's first body (near sources are close to it).
+        const int first = a.leaf_part[tb];
+        const double ox = a.x[first], oy = a.y[first], oz = a.z[first];
+
+        for (int pass = 0; pass * slots < nt; ++pass) {
+            const int t = pass * slots + slot;
+            const bool ok = t < nt;
+            const int i = ok ? a.leaf_part[tb + t] : first;
+            const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
+            const float xf = __double2float_rn(xi - ox), yf = __double2float_rn(yi - oy),
+                        zf = __double2float_rn(zi - oz);
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            if (MODE == kF64Exact && ok) {
+                fx = a.ax[i];
+                fy = a.ay[i];
+                fz = a.az[i];
+            }
+            CompF cx, cy, cz;
+            cx.init();
+            cy.init();
+            cz.init();
+
+            auto compute = [&](int cnt) {
+                if (MODE == kF64Exact) {
+                    for (int jj = 0; jj < cnt; ++jj) {
+                        if (sidx[jj] == i) continue;
+                        const double rx = dsub(sxd[jj], xi), ry = dsub(syd[jj], yi), rz = dsub(szd[jj], zi);
+                        const double s2 = dadd(dadd(dadd(dmul(rx, rx), dmul(ry, ry)), dmul(rz, rz)), a.eps2);
+                        if (s2 == 0.0) {
+                            fx = dadd(fx, 0.0);
+                            fy = dadd(fy, 0.0);
+                            fz = dadd(fz, 0.0);
+                            continue;
+                        }
+                        const double inv = __ddiv_rn(1.0, __dsqrt_rn(s2));
+                        const double inv3 = dmul(dmul(inv, inv), inv);
+                        const double scale = dmul(dmul(a.G, smd[jj]), inv3);
+                        fx = dadd(fx, dmul(rx, scale));
+                        fy = dadd(fy, dmul(ry, scale));
+                        fz = dadd(fz, dmul(rz, scale));
                     }
-                    const double inv = __ddiv_rn(1.0, __dsqrt_rn(s2));
-                    const double inv3 = dmul(dmul(inv, inv), inv);
-                    const double scale = dmul(dmul(a.G, smd[jj]), inv3);
-                    fx = dadd(fx, dmul(rx, scale));
-                    fy = dadd(fy, dmul(ry, scale));
-                    fz = dadd(fz, dmul(rz, scale));
+                } else if (MODE == kF64) {
+#pragma unroll 4
+                    for (int jj = lane; jj < cnt; jj += L) {
+                        const double dx = sxd[jj] - xi, dy = syd[jj] - yi, dz = szd[jj] - zi;
+                        double r = fma(dx, dx, a.eps2);
+                        r = fma(dy, dy, r);
+                        r = fma(dz, dz, r);
+                        double y = rsqrt_f64(r);
+                        if (EPS0) y = (r == 0.0 || sidx[jj] == i) ? 0.0 : y;
+                        const double w = smd[jj] * (y * y * y);
+                        fx = fma(dx, w, fx);
+                        fy = fma(dy, w, fy);
+                        fz = fma(dz, w, fz);
+                    }
+                } else {
+                    float px = 0.f, py = 0.f, pz = 0.f;
+                    const float* sxf = reinterpret_cast<const float*>(sxd);
+                    const float* syf = reinterpret_cast<const float*>(syd);
+                    const float* szf = reinterpret_cast<const float*>(szd);
+                    const float* smf = reinterpret_cast<const float*>(smd);
+#pragma unroll 4
+                    for (int jj = lane; jj < cnt; jj += L) {
+                        const float dx = sxf[jj] - xf, dy = syf[jj] - yf, dz = szf[jj] - zf;
+                        float r = fmaf(dx, dx, a.eps2f);
+                        r = fmaf(dy, dy, r);
+                        r = fmaf(dz, dz, r);
+                        float iv = rsqrt_f32(r);
+                        if (EPS0) iv = (r == 0.f || sidx[jj] == i) ? 0.f : iv;
+                        const float w = smf[jj] * (iv * iv * iv);
+                        px = fmaf(dx, w, px);
+                        py = fmaf(dy, w, py);
+                        pz = fmaf(dz, w, pz);
+                    }
+                    cx.add(px);
+                    cy.add(py);
+                    cz.add(pz);
                 }
-            } else if (MODE == kF64) {
-                for (int jj = lane; jj < cnt; jj += L) {
-                    const double dx = sxd[jj] - xi, dy = syd[jj] - yi, dz = szd[jj] - zi;
-                    double r = fma(dx, dx, a.eps2);
-                    r = fma(dy, dy, r);
-                    r = fma(dz, dz, r);
-                    double y = rsqrt_f64(r);
-                    if (EPS0) y = (r == 0.0 || sidx[jj] == i) ? 0.0 : y;
-                    const double w = smd[jj] * (y * y * y);
-                    fx = fma(dx, w, fx);
-                    fy = fma(dy, w, fy);
-                    fz = fma(dz, w, fz);
+            };
+            auto stage = [&](int c, int j) {
+                sidx[c] = j;
+                if (MODE == kMixed) {
+                    float* sxf = reinterpret_cast<float*>(sxd);
+                    float* syf = reinterpret_cast<float*>(syd);
+                    float* szf = reinterpret_cast<float*>(szd);
+                    float* smf = reinterpret_cast<float*>(smd);
+                    sxf[c] = __double2float_rn(a.x[j] - ox);
+                    syf[c] = __double2float_rn(a.y[j] - oy);
+                    szf[c] = __double2float_rn(a.z[j] - oz);
+                    smf[c] = __double2float_rn(a.m[j]);
+                } else {
+                    sxd[c] = a.x[j];
+                    syd[c] = a.y[j];
+                    szd[c] = a.z[j];
+                    smd[c] = a.m[j];
                 }
-            } else {
-                float px = 0.f, py = 0.f, pz = 0.f;
-                const float* sxf = reinterpret_cast<const float*>(sxd);
-                const float* syf = reinterpret_cast<const float*>(syd);
-                const float* szf = reinterpret_cast<const float*>(szd);
-                const float* smf = reinterpret_cast<const float*>(smd);
-                for (int jj = lane; jj < cnt; jj += L) {
-                    const float dx = sxf[jj] - xf, dy = syf[jj] - yf, dz = szf[jj] - zf;
-                    float r = fmaf(dx, dx, a.eps2f);
-                    r = fmaf(dy, dy, r);
-                    r = fmaf(dz, dz, r);
-                    float iv = rsqrt_f32(r);
-                    if (EPS0) iv = (r == 0.f || sidx[jj] == i) ? 0.f : iv;
-                    const float w = smf[jj] * (iv * iv * iv);
-                    px = fmaf(dx, w, px);
-                    py = fmaf(dy, w, py);
-                    pz = fmaf(dz, w, pz);
-                }
-                cx.add(px);
-                cy.add(py);
-                cz.add(pz);
-            }
-        };
-        auto stage = [&](int slot_base, int j) {
-            sidx[slot_base] = j;
-            if (MODE == kMixed) {
-                float* sxf = reinterpret_cast<float*>(sxd);
-                float* syf = reinterpret_cast<float*>(syd);
-                float* szf = reinterpret_cast<float*>(szd);
-                float* smf = reinterpret_cast<float*>(smd);
-                sxf[slot_base] = __double2float_rn(a.x[j] - ox);
-                syf[slot_base] = __double2float_rn(a.y[j] - oy);
-                szf[slot_base] = __double2float_rn(a.z[j] - oz);
-                smf[slot_base] = __double2float_rn(a.m[j]);
-            } else {
-                sxd[slot_base] = a.x[j];
-                syd[slot_base] = a.y[j];
-                szd[slot_base] = a.z[j];
-                smd[slot_base] = a.m[j];
-            }
-        };
+            };
 
-        for (int q = nb; q < ne; ++q) {
-            const int s = a.near_leaf[q];
-            const int sb = a.leaf_off[s];
-            const int ns = a.leaf_off[s + 1] - sb;
-            int o = 0;
-            while (o < ns) {
-                const int take = min(ns - o, kP2PJT - fill);
-                for (int c = tid; c < take; c += kP2PBlock) stage(fill + c, a.leaf_part[sb + o + c]);
-                fill += take;
-                o += take;
-                if (fill == kP2PJT) {
-                    __syncthreads();
-                    compute(fill);
-                    __syncthreads();
-                    fill = 0;
+            // Walk the near list in batches; stage only the slots of this item's chunk.
+            int64_t base = 0;  // slots before the current near batch
+            for (int qb = nb; qb < ne && base < c_hi; qb += kNearBatch) {
+                const int cnt = min(kNearBatch, ne - qb);
+                for (int q = tid; q < cnt; q += kP2PBlock) {
+                    const int s = a.near_leaf[qb + q];
+                    const int b = a.leaf_off[s];
+                    s_beg[q] = b;
+                    s_pre[q + 1] = a.leaf_off[s + 1] - b;
                 }
+                if (tid == 0) s_pre[0] = 0;
+                __syncthreads();
+                if (tid < 32) {  // inclusive scan of the lengths s_pre[1..cnt] by warp 0
+                    int carry = 0;
+                    for (int k0 = 1; k0 <= cnt; k0 += 32) {
+                        const int k = k0 + tid;
+                        int v = k <= cnt ? s_pre[k] : 0;
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const int u = __shfl_up_sync(0xffffffffu, v, o);
+                            if (tid >= o) v += u;
+                        }
+                        if (k <= cnt) s_pre[k] = v + carry;
+                        carry += __shfl_sync(0xffffffffu, v, 31);
+                    }
+                }
+                __syncthreads();
+                const int total = s_pre[cnt];
+                // this batch covers slots [base, base + total) of the sequence; keep [c_lo, c_hi)
+                const int b_lo = (int)max((int64_t)0, c_lo - base);
+                const int b_hi = (int)min((int64_t)total, c_hi - base);
+                for (int c0 = b_lo; c0 < b_hi; c0 += kP2PJT) {
+                    const int take = min(kP2PJT, b_hi - c0);
+                    for (int c = tid; c < take; c += kP2PBlock) {
+                        const int sl = c0 + c;
+                        int l2 = 0, h2 = cnt;  // s_pre[l2] <= sl < s_pre[h2]
+                        while (h2 - l2 > 1) {
+                            const int mid = (l2 + h2) >> 1;
+                            if (s_pre[mid] <= sl) l2 = mid;
+                            else h2 = mid;
+                        }
+                        stage(c, a.leaf_part[s_beg[l2] + (sl - s_pre[l2])]);
+                    }
+                    __syncthreads();
+                    compute(take);
+                    __syncthreads();
+                }
+                base += total;
+                __syncthreads();  // s_beg / s_pre are rewritten by the next batch
             }
-        }
-        if (fill > 0) {
-            __syncthreads();
-            compute(fill);
-            __syncthreads();
-        }
 
-        if (MODE == kF64Exact) {
-            if (ok) {
-                a.ax[i] = fx;
-                a.ay[i] = fy;
-                a.az[i] = fz;
+            if (MODE == kF64Exact) {
+                if (ok) {
+                    a.ax[i] = fx;
+                    a.ay[i] = fy;
+                    a.az[i] = fz;
+                }
+                continue;
             }
-        } else {
             if (MODE == kMixed) {
                 fx = cx.value();
                 fy = cy.value();
@@ -181,29 +326,102 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
                 fz += __shfl_xor_sync(0xffffffffu, fz, o);
             }
             if (ok && lane == 0) {
-                a.ax[i] = a.ax[i] + a.G * fx;
-                a.ay[i] = a.ay[i] + a.G * fy;
-                a.az[i] = a.az[i] + a.G * fz;
+                if (chunks == 1) {
+                    a.ax[i] = a.ax[i] + a.G * fx;
+                    a.ay[i] = a.ay[i] + a.G * fy;
+                    a.az[i] = a.az[i] + a.G * fz;
+                } else {
+                    const size_t k = (size_t)(a.plan_scratch[leaf] + (int64_t)chunk * nt + t) * 3;
+                    a.scratch[k] = fx;
+                    a.scratch[k + 1] = fy;
+                    a.scratch[k + 2] = fz;
+                }
             }
+        }
+        if (MODE == kF64Exact || chunks == 1) continue;
+        // Split leaf: the CTA that completes its last chunk adds the partials in chunk order.
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = (atomicAdd(&a.plan_done[leaf], 1) == chunks - 1);
+        __syncthreads();
+        if (!s_last) continue;
+        __threadfence();
+        for (int t = tid; t < nt; t += kP2PBlock) {
+            const int i = a.leaf_part[tb + t];
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            for (int c = 0; c < chunks; ++c) {
+                const size_t k = (size_t)(a.plan_scratch[leaf] + (int64_t)c * nt + t) * 3;
+                sx += __ldcg(&a.scratch[k]);
+                sy += __ldcg(&a.scratch[k + 1]);
+                sz += __ldcg(&a.scratch[k + 2]);
+            }
+            a.ax[i] = a.ax[i] + a.G * sx;
+            a.ay[i] = a.ay[i] + a.G * sy;
+            a.az[i] = a.az[i] + a.G * sz;
         }
     }
 }
 
+template <int MODE, bool EPS0>
+int p2p_occupancy() {
+    static int occ = 0;
+    if (occ == 0) {
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, p2p_kernel<MODE, EPS0>, kP2PBlock, 0) != cudaSuccess ||
+            nb < 1)
+            nb = 1;
+        occ = nb;
+    }
+    return occ;
+}
+
+template <int MODE, bool EPS0>
+cudaError_t launch_main(const P2PArgs& a, int sms, cudaStream_t st) {
+    const int grid = sms * p2p_occupancy<MODE, EPS0>();
+    p2p_kernel<MODE, EPS0><<<grid, kP2PBlock, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-cudaError_t launch_p2p(const P2PArgs& a, int precision, cudaStream_t st) {
+size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves) {
+    // plan arrays (src and scratch offsets int64; chunks, item offsets, done counters int),
+    // n_items + ticket, and the partial sums: a split leaf holds at most kMaxChunks partials
+    // for each of its bodies.
+    const size_t nl = (size_t)n_leaves + 1;
+    return nl * (8 + 8 + 4 + 4 + 4) + 128 + (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n;
+}
+
+cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch, int sms, cudaStream_t st) {
     if (a.n_leaves <= 0) return cudaSuccess;
     const bool eps0 = precision == kMixed ? (a.eps2f < 1e-24f) : (a.eps2 < 1e-200);
-    dim3 grid((unsigned)a.n_leaves);
-    if (precision == kF64Exact)
-        p2p_kernel<kF64Exact, false><<<grid, kP2PBlock, 0, st>>>(a);
-    else if (precision == kF64)
-        eps0 ? p2p_kernel<kF64, true><<<grid, kP2PBlock, 0, st>>>(a)
-             : p2p_kernel<kF64, false><<<grid, kP2PBlock, 0, st>>>(a);
-    else
-        eps0 ? p2p_kernel<kMixed, true><<<grid, kP2PBlock, 0, st>>>(a)
-             : p2p_kernel<kMixed, false><<<grid, kP2PBlock, 0, st>>>(a);
-    return cudaGetLastError();
+    const size_t nl = (size_t)a.n_leaves + 1;
+    char* p = (char*)scratch;
+    a.plan_src = (int64_t*)p;
+    p += nl * 8;
+    a.plan_scratch = (int64_t*)p;
+    p += nl * 8;
+    a.plan_chunks = (int*)p;
+    p += nl * 4;
+    a.plan_item_off = (int*)p;
+    p += nl * 4;
+    a.plan_done = (int*)p;
+    p += nl * 4;
+    p = (char*)(((uintptr_t)p + 63) & ~(uintptr_t)63);
+    a.plan_n_items = (int*)p;
+    a.ticket = (int*)p + 1;
+    p += 64;
+    a.scratch = (double*)p;
+    a.scratch_capacity = (int64_t)kMaxChunks * n_bodies;
+    cudaError_t e = cudaMemsetAsync(a.plan_done, 0, nl * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    p2p_count_kernel<<<(a.n_leaves + 255) / 256, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0);
+    p2p_scan_kernel<<<1, kScanBlock, 0, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (precision == kF64Exact) return launch_main<kF64Exact, false>(a, sms, st);
+    if (precision == kF64) return eps0 ? launch_main<kF64, true>(a, sms, st) : launch_main<kF64, false>(a, sms, st);
+    return eps0 ? launch_main<kMixed, true>(a, sms, st) : launch_main<kMixed, false>(a, sms, st);
 }
 
 }  // namespace gx

@@ -22,8 +22,21 @@ struct P2PArgs {
     double G;
     double eps2;
     float eps2f;
+    // work plan and partial sums, carved from the scratch passed to launch_p2p
+    int64_t* plan_src;      // sources per leaf
+    int64_t* plan_scratch;  // per-leaf offset of its partial sums (split leaves), in targets
+    int* plan_chunks;       // items per leaf
+    int* plan_item_off;     // n_leaves + 1 item offsets
+    int* plan_done;         // chunks finished per leaf
+    int* plan_n_items;
+    int* ticket;
+    double* scratch;
+    int64_t scratch_capacity;  // partial-sum slots (targets) the scratch holds
 };
 
-cudaError_t launch_p2p(const P2PArgs& a, int precision, cudaStream_t st);
+// Device scratch launch_p2p needs for n bodies and n_leaves leaves.
+size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves);
+// Stream-ordered: plan on the device, then the persistent leaf kernel (sms x occupancy CTAs).
+cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch, int sms, cudaStream_t st);
 
 }  // namespace gx
