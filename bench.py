@@ -190,6 +190,8 @@ def main():
     ap.add_argument("--variant", type=int, default=None, help="force a kernel variant id (skips autotuning)")
     ap.add_argument("--jsplit", type=int, default=None, help="source split used with --variant")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--sharded", action="store_true",
+                    help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
     ap.add_argument("--workload", default="mixed-n1048576",
                     choices=["mixed-n1048576", "ensemble", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
                     help="headline (default) or one of the other configurations")
@@ -216,18 +218,23 @@ def main():
 
     gx = load_gx()
     torch.cuda.set_device(local)
-    if world > 1:
+    sharded = world > 1 or args.sharded
+    if sharded:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps, mass1=1.0, mass2=1.0 / 3.0)
     prec = gx.PRECISION_MIXED if args.precision == "mixed" else gx.PRECISION_F64
-    if world > 1:
+    if sharded:
         res = run_sharded(gx, torch, dist, p, args, rank, world, eps, dt, prec)
     else:
         res = run_single(gx, torch, p, args, eps, dt, prec)
     if rank == 0:
         print(json.dumps(res), flush=True)
-    if world > 1:
+    if sharded:
         dist.barrier()
         dist.destroy_process_group()
 
@@ -370,7 +377,7 @@ def fp64_rate(gx, torch, sess, p, dt, flush, steps: int = 2) -> dict:
             "steps": steps, "kernel": gx.describe_variant(gx.PRECISION_F64, v), "jsplit": js}
 
 
-def e2e_rate(gx, torch, p, params, dt, prec, steps: int = 2) -> dict:
+def e2e_rate(gx, torch, p, params, dt, prec, steps: int = 3) -> dict:
     """gx_leapfrog_step on pinned host arrays: copies in, step, copies out, every step."""
     n = len(p)
     host = {}
@@ -390,7 +397,7 @@ def e2e_rate(gx, torch, p, params, dt, prec, steps: int = 2) -> dict:
         gx.cuda_direct_leapfrog_step(q, dt, params, prec)
         times.append(time.perf_counter() - t0)
     return {"value": steps * n * (n - 1) / sum(times) / 1e9, "unit": UNIT, "h2d_bytes_per_step": 10 * 8 * n,
-            "d2h_bytes_per_step": 9 * 8 * n, "steps": steps,
+            "d2h_bytes_per_step": 9 * 8 * n, "steps": steps, "step_ms": [round(t * 1e3, 3) for t in times],
             "api": "gx_leapfrog_step (cuda_direct_leapfrog_step) on pinned host arrays, wall clock"}
 
 

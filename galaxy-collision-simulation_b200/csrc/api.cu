@@ -137,6 +137,23 @@ int sm_count(int dev) {
     return v;
 }
 
+// Stream-ordered scratch comes from the device's default pool; keep freed blocks in the pool
+// (release threshold = unlimited) so repeated calls on host arrays do not remap memory.
+void keep_pool_memory(int dev) {
+    static std::mutex mu;
+    static std::map<int, bool> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    done[dev] = true;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) != cudaSuccess) cudaGetLastError();
+    } else {
+        cudaGetLastError();
+    }
+}
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {
@@ -202,6 +219,8 @@ struct AsyncBuf {
     }
     int alloc(size_t bytes, cudaStream_t s) {
         st = s;
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) keep_pool_memory(dev);
         cudaError_t e = dev_alloc_async(&p, bytes, s);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -274,8 +293,20 @@ int best_split(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int sms) {
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int64_t>, Choice> g_tuned;  // (device, precision, eps0, n)
 
-// Untuned choice: the wave model over all variants of the precision, with a small penalty
-// for every variant but the first (the one measured fastest per interaction on B200).
+// Time per interaction of a variant relative to the fastest of its precision, measured on B200
+// at N = 2^20 (the wave model cannot see instruction-level differences between variants).
+double variant_rate_penalty(const ForceVariant& v) {
+    if (v.precision == kMixed) {
+        if (v.packed == 2) return v.block * v.ipt >= 1024 ? 1.0 : 1.02;  // targets packed
+        if (v.packed == 1) return v.block * v.ipt >= 1024 ? 1.04 : 1.10;  // sources packed
+        return 1.25;                                                      // scalar FP32
+    }
+    if (v.precision == kF64) return v.block * v.ipt >= 512 ? 1.0 : 1.05;
+    return 1.0;
+}
+
+// Untuned choice: the wave model over all variants of the precision, weighted by each
+// variant's measured per-interaction rate.
 Choice heuristic_choice(int dev, int precision, bool eps0, int64_t n_tgt, int64_t n_src) {
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -293,7 +324,7 @@ Choice heuristic_choice(int dev, int precision, bool eps0, int64_t n_tgt, int64_
         const ForceVariant& v = all[ids[k]];
         if (precision == kMixed && !v.packed) continue;  // the scalar form is kept for measurement only
         const int ns = best_split(v, n_tgt, n_src, sms);
-        const double cost = split_cost(v, n_tgt, n_src, ns, sms) * (k == 0 ? 1.0 : 1.08);
+        const double cost = split_cost(v, n_tgt, n_src, ns, sms) * variant_rate_penalty(v);
         if (cost < bc) {
             bc = cost;
             best.variant = ids[k];
@@ -1134,27 +1165,48 @@ extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms
     Choice best;
     double bms = 1e300;
     int status = GX_OK;
+    const bool large = (double)s->n * (double)s->n > 4.0e10;
+    // Phase 1: every variant at the split the wave model prefers for it (small systems also try
+    // a few fixed splits).  Phase 2 (large systems): other splits for the three best variants.
+    std::vector<std::pair<double, Choice>> ranked;
     for (int k = 0; k < c && status == GX_OK; ++k) {
         const ForceVariant& v = all[ids[k]];
         std::vector<int> splits = {best_split(v, s->n, s->n, sms)};
-        if (splits[0] != 1) splits.push_back(1);
-        for (int ns : {2, 4, 8}) {
-            if (std::find(splits.begin(), splits.end(), ns) == splits.end() && (int64_t)ns * v.jt <= s->n) splits.push_back(ns);
+        if (!large) {
+            for (int ns : {1, 2, 4, 8})
+                if (std::find(splits.begin(), splits.end(), ns) == splits.end() && (int64_t)ns * v.jt <= s->n)
+                    splits.push_back(ns);
         }
         for (int ns : splits) {
-            Choice ch{ids[k], ns};
+            const Choice ch{ids[k], ns};
             double ms;
-            // A large system is timed once per candidate at the model's split only.
-            const bool large = (double)s->n * (double)s->n > 4.0e10;
-            if (large && ns != splits[0]) continue;
             status = time_choice(s, precision, ch, s->n, large ? 1 : 3, &ms);
             if (status != GX_OK) break;
-            if (ms < bms) {
-                bms = ms;
-                best = ch;
-            }
+            ranked.emplace_back(ms, ch);
         }
     }
+    if (status == GX_OK && large && !ranked.empty()) {
+        std::sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        const size_t top = std::min<size_t>(3, ranked.size());
+        std::vector<std::pair<double, Choice>> extra;
+        for (size_t r = 0; r < top && status == GX_OK; ++r) {
+            const ForceVariant& v = all[ranked[r].second.variant];
+            for (int ns : {1, 2, 4, 8}) {
+                if (ns == ranked[r].second.nsplit || (int64_t)ns * v.jt > s->n) continue;
+                const Choice ch{ranked[r].second.variant, ns};
+                double ms;
+                status = time_choice(s, precision, ch, s->n, 1, &ms);
+                if (status != GX_OK) break;
+                extra.emplace_back(ms, ch);
+            }
+        }
+        ranked.insert(ranked.end(), extra.begin(), extra.end());
+    }
+    for (const auto& r : ranked)
+        if (r.first < bms) {
+            bms = r.first;
+            best = r.second;
+        }
     cudaMemcpyAsync(s->ax, save, (size_t)s->n * 3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
     cudaStreamSynchronize(s->stream);
     cudaFree(save);
