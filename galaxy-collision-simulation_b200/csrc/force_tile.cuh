@@ -57,10 +57,6 @@ __device__ __forceinline__ void write_partial(const ForceArgs& a, int chunk, int
     a.part[base + 2 * (size_t)a.n_tgt] = sz;
 }
 
-__device__ __forceinline__ void lds_v2b64(const float* p, f2& a, f2& b) {
-    const unsigned addr = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"(addr));
-}
 
 // ---------------------------------------------------------------------------------------
 // Mixed precision.

@@ -62,6 +62,12 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
     return d;
 }
 
+// 16-byte shared-memory load of two packed pairs (p must be 16-byte aligned shared memory).
+__device__ __forceinline__ void lds_v2b64(const float* p, f2& a, f2& b) {
+    const unsigned addr = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"(addr));
+}
+
 // Knuth's TwoSum: s + e == a + b exactly (round-to-nearest, no overflow).
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
