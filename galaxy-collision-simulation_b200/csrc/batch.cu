@@ -15,7 +15,7 @@
 namespace gx {
 namespace {
 
-template <int MODE, int BLOCK, int IPT, int JT, bool EPS0, bool TP = false>
+template <int MODE, int BLOCK, int IPT, int JT, bool EPS0, bool TP = false, int UNROLL = 4>
 __global__ void __launch_bounds__(BLOCK) batch_force_kernel(const BatchArgs b) {
     __shared__ int s_item;
     for (;;) {
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(BLOCK) batch_force_kernel(const BatchArgs b) {
         a.eps2f = b.eps2f;
         const int64_t t0 = (int64_t)w.y * (BLOCK * IPT);
         if constexpr (MODE == kMixed && TP)
-            mixed_tp_tile<BLOCK, IPT, JT, EPS0>(a, t0, 0);
+            mixed_tp_tile<BLOCK, IPT, JT, EPS0, UNROLL>(a, t0, 0);
         else if constexpr (MODE == kMixed)
             mixed_tile<BLOCK, IPT, JT, true, EPS0>(a, t0, 0);
         else
@@ -175,11 +175,12 @@ __global__ void __launch_bounds__(256) batch_moments_kernel(const BatchArgs b, c
 
 #define BMIX(B, I, J, E) {kMixed, B, I, J, E, (const void*)&batch_force_kernel<kMixed, B, I, J, E>}
 #define BMTP(B, I, J, E) {kMixed, B, I, J, E, (const void*)&batch_force_kernel<kMixed, B, I, J, E, true>}
+#define BMTPU(B, I, J, U) {kMixed, B, I, J, 0, (const void*)&batch_force_kernel<kMixed, B, I, J, false, true, U>}
 #define BF64(B, I, J, E) {kF64, B, I, J, E, (const void*)&batch_force_kernel<kF64, B, I, J, E>}
 
 const BatchVariant kBatchVariants[] = {
-    BMTP(128, 8, 512, false), BMTP(256, 4, 512, false), BMIX(128, 8, 512, false),
-    BMIX(256, 4, 512, false), BMIX(128, 4, 512, false), BMTP(64, 8, 256, false), BMIX(64, 4, 256, false),
+    BMTPU(256, 6, 512, 8), BMTPU(128, 8, 512, 8), BMTP(128, 8, 512, false), BMTP(256, 4, 512, false),
+    BMIX(128, 8, 512, false), BMTPU(64, 8, 256, 8), BMIX(64, 4, 256, false),
     BMIX(256, 4, 512, true),
     BF64(256, 2, 256, false), BF64(128, 2, 256, false), BF64(64, 2, 128, false),
     BF64(256, 2, 256, true),

@@ -74,6 +74,8 @@ def ref():
         lib.ref_fmm_split.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int,
                                       POINTER(c_int32), POINTER(c_int64), P, P, P, P, P, P, P]
         lib.ref_smoke80_inputs.argtypes = [P, P, P, P]
+        lib.ref_leapfrog_fmm.argtypes = [c_int64, P, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, c_int,
+                                         c_double, c_int64, c_int]
         _ref = lib
     return _ref
 
@@ -188,6 +190,14 @@ def ref_leapfrog(state: dict, m, G, eps, dt, steps) -> dict:
     m = _f(m)
     ref().ref_leapfrog_direct(len(m), *(_p(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")), _p(m),
                               G, eps, dt, steps)
+    return s
+
+
+def ref_leapfrog_fmm(state: dict, m, G, eps, dt, steps, theta, leaf_capacity, order=4) -> dict:
+    s = {k: _f(state[k]).copy() for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+    m = _f(m)
+    ref().ref_leapfrog_fmm(len(m), *(_p(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")), _p(m),
+                           G, eps, dt, steps, theta, leaf_capacity, order)
     return s
 
 

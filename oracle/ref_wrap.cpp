@@ -106,6 +106,26 @@ void ref_leapfrog_direct(int64_t n, double* x, double* y, double* z, double* vx,
     }
 }
 
+// `steps` reference leapfrog_step calls with the FMM force (compute_fmm_accelerations,
+// fmm_solver.cpp:315-322), the CLI's "fmm" solver.
+void ref_leapfrog_fmm(int64_t n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                      double* ax, double* ay, double* az, const double* m, double G, double eps, double dt,
+                      int steps, double theta, int64_t leaf_capacity, int order) {
+    auto p = to_particles(n, x, y, z, m, vx, vy, vz, ax, ay, az);
+    const PhysicsParams ph = physics(G, eps);
+    fmmgalaxy::FmmOptions o;
+    o.theta = theta;
+    o.leaf_capacity = static_cast<std::size_t>(leaf_capacity);
+    o.expansion_order = order;
+    auto force = [&ph, &o](std::vector<Particle>& s) { fmmgalaxy::compute_fmm_accelerations(s, ph, o); };
+    for (int s = 0; s < steps; ++s) fmmgalaxy::leapfrog_step(p, dt, force);
+    for (int64_t i = 0; i < n; ++i) {
+        x[i] = p[i].position.x; y[i] = p[i].position.y; z[i] = p[i].position.z;
+        vx[i] = p[i].velocity.x; vy[i] = p[i].velocity.y; vz[i] = p[i].velocity.z;
+        ax[i] = p[i].acceleration.x; ay[i] = p[i].acceleration.y; az[i] = p[i].acceleration.z;
+    }
+}
+
 // compute_diagnostics (diagnostics.cpp:7-37) -> 13 doubles in diagnostics.csv column order.
 void ref_diagnostics(int64_t n, const double* x, const double* y, const double* z,
                      const double* vx, const double* vy, const double* vz, const double* m,

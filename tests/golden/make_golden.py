@@ -57,9 +57,12 @@ def smoke80():
 
 def fmm1000():
     s = load_csv(BENCH / "fmm_1000_r1" / "snapshot_000000.csv")
+    s20 = load_csv(BENCH / "fmm_1000_r1" / "snapshot_000020.csv")
     lists, far = oracle.ref_fmm_split(s["x"], s["y"], s["z"], s["m"], 1.0, 0.025, 0.58, 16, 4)
     np.savez_compressed(OUT / "fmm1000.npz", x=s["x"], y=s["y"], z=s["z"], m=s["m"], ax=s["ax"], ay=s["ay"],
-                        az=s["az"], far=far, theta=0.58, leaf_capacity=16, softening=0.025, **lists)
+                        az=s["az"], vx=s["vx"], vy=s["vy"], vz=s["vz"], far=far, theta=0.58, leaf_capacity=16,
+                        softening=0.025, dt=0.01, steps=20,
+                        **{f"{k}20": s20[k] for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}, **lists)
 
 
 def cfg0():
