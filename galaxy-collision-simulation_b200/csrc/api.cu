@@ -253,16 +253,15 @@ void split_layout(int64_t n_src, int jt, int want, int64_t* chunk, int* nsplit) 
 // target at full rate".  The CTAs are spread evenly over the SMs (L per SM); an SM runs
 // them in rounds of `occupancy` concurrent CTAs, and a round with fewer CTAs than needed to
 // cover latency (about 12 warps) runs at a proportionally lower rate.
-double split_cost(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int ns, int sms) {
-    const int64_t tile = (int64_t)v.block * v.ipt;
+double rounds_cost(int block, int ipt, int jt, int occ, int64_t n_tgt, int64_t n_src, int ns, int sms) {
+    const int64_t tile = (int64_t)block * ipt;
     const int64_t T = (n_tgt + tile - 1) / tile;
-    const int occ = force_occupancy(v);
     int64_t chunk;
     int nse;
-    split_layout(n_src, v.jt, ns, &chunk, &nse);
+    split_layout(n_src, jt, ns, &chunk, &nse);
     const int64_t L = (T * nse + sms - 1) / sms;
-    const double W = (double)tile * (double)(chunk + v.jt);
-    const double warps = v.block / 32.0;
+    const double W = (double)tile * (double)(chunk + jt);
+    const double warps = block / 32.0;
     auto eff = [&](int64_t c) { return std::min(1.0, (double)c * warps / 12.0); };
     const int64_t full = L / occ, rem = L % occ;
     double t = (double)full * (double)occ * W / eff(occ);
@@ -270,6 +269,10 @@ double split_cost(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int ns, i
     // the ordered reduction pass reads nse partials per target
     if (nse > 1) t += 0.05 * (double)nse * (double)n_tgt * 64.0 / sms;
     return t;
+}
+
+double split_cost(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int ns, int sms) {
+    return rounds_cost(v.block, v.ipt, v.jt, force_occupancy(v), n_tgt, n_src, ns, sms);
 }
 
 int best_split(const ForceVariant& v, int64_t n_tgt, int64_t n_src, int sms) {
@@ -1340,10 +1343,24 @@ extern "C" int gx_direct_vjp(int64_t n, const double* x, const double* y, const 
     a.G = phys.G;
     a.eps2 = phys.softening * phys.softening;
     a.eps2f = (float)a.eps2;
-    // j-split so that at least ~2 waves of CTAs exist.
+    // source split chosen by the same per-SM-rounds model as the forward kernels
     const int sms = sm_count(dev);
-    const int64_t tiles = (n + vjp_tile(precision) - 1) / vjp_tile(precision);
-    int want = (int)std::min<int64_t>(64, std::max<int64_t>(1, (4 * sms + tiles - 1) / tiles));
+    int want = 1;
+    {
+        const VjpShape sh = vjp_shape(precision);
+        double best = rounds_cost(sh.block, sh.ipt, sh.jt, sh.occupancy, n, n, 1, sms);
+        for (int ns = 2; ns <= 64; ++ns) {
+            int64_t chunk;
+            int nse;
+            split_layout(n, sh.jt, ns, &chunk, &nse);
+            if (nse != ns) continue;
+            const double c = rounds_cost(sh.block, sh.ipt, sh.jt, sh.occupancy, n, n, ns, sms);
+            if (c < best * 0.995) {
+                best = c;
+                want = ns;
+            }
+        }
+    }
     split_layout(n, vjp_jt(precision), want, &a.j_chunk, &a.nsplit);
     AsyncBuf part;
     a.part = nullptr;

@@ -397,6 +397,24 @@ cudaError_t launch_shape(const VjpArgs& a, bool eps0, cudaStream_t st) {
 int vjp_tile(int precision) { return precision == kMixed ? 128 * 4 : 128 * 2; }
 int vjp_jt(int precision) { return precision == kMixed ? 256 : 256; }
 
+VjpShape vjp_shape(int precision) {
+    static int occ[2] = {0, 0};
+    const int k = precision == kMixed ? 1 : 0;
+    if (occ[k] == 0) {
+        int nb = 0;
+        const cudaError_t e = k ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                      &nb, vjp_mixed_tp_kernel<128, 4, 256, false>, 128, 0)
+                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                      &nb, vjp_kernel<128, 2, 256, false, false>, 128, 0);
+        if (e != cudaSuccess || nb < 1) {
+            cudaGetLastError();
+            nb = 1;
+        }
+        occ[k] = nb;
+    }
+    return k ? VjpShape{128, 4, 256, occ[1]} : VjpShape{128, 2, 256, occ[0]};
+}
+
 cudaError_t launch_vjp(const VjpArgs& a, int precision, cudaStream_t st) {
     if (a.n <= 0) return cudaSuccess;
     cudaError_t e;

@@ -29,6 +29,11 @@ struct VjpArgs {
 
 int vjp_tile(int precision);  // targets per CTA
 int vjp_jt(int precision);    // sources per shared-memory pass
+
+struct VjpShape {
+    int block, ipt, jt, occupancy;
+};
+VjpShape vjp_shape(int precision);  // launch shape and resident CTAs per SM
 cudaError_t launch_vjp(const VjpArgs& a, int precision, cudaStream_t st);
 
 }  // namespace gx
