@@ -8,6 +8,7 @@ of its FMM.  Compute runs in hand-written sm_100a CUDA kernels behind the C ABI 
                   compute_cuda_direct_accelerations, cuda_direct_leapfrog_step, ...)
 * ``session``  -- device-resident sessions and batched ensembles (CUDA graphs)
 * ``fmm_p2p``  -- reference-octree leaf lists and the GPU near field
+* ``fmm``      -- the reference FMM solver (moments, far field and near field on the GPU)
 * ``adjoint``  -- autograd Function over the leapfrog with the adjoint kernel (needs torch)
 * ``ics``      -- seeded two-disk initial conditions
 """
@@ -17,6 +18,8 @@ from ._ffi import (GX_ERR_CUDA, GX_ERR_INVALID_ARGUMENT, GX_ERR_NO_DEVICE, GX_ER
 from .engine import (Diagnostics, ParticleSet, PhysicsParams, compute_cuda_direct_accelerations,
                      compute_diagnostics, compute_direct_accelerations_for_targets, cuda_direct_leapfrog_step,
                      cuda_solver_available, indexed_accelerations)
+from .fmm import (FastMultipoleSolver, FmmOptions, FmmStats, compute_fmm_accelerations,
+                  compute_fmm_accelerations_for_targets)
 from .fmm_p2p import LeafLists, build_leaf_lists, p2p_leaves
 from .session import Batch, Session, batch_accelerations, describe_variant
 from . import ics
@@ -26,5 +29,7 @@ __all__ = [
     "cuda_solver_available", "compute_cuda_direct_accelerations", "compute_direct_accelerations_for_targets",
     "cuda_direct_leapfrog_step", "compute_diagnostics", "indexed_accelerations", "build_leaf_lists", "p2p_leaves",
     "batch_accelerations", "describe_variant", "device_available", "load", "ics",
+    "FastMultipoleSolver", "FmmOptions", "FmmStats", "compute_fmm_accelerations",
+    "compute_fmm_accelerations_for_targets",
     "PRECISION_F64", "PRECISION_MIXED", "PRECISION_F64_EXACT",
 ]

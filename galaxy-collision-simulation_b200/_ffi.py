@@ -65,6 +65,20 @@ class DiagnosticsStruct(ctypes.Structure):
     ]
 
 
+class FmmOptionsStruct(ctypes.Structure):
+    """gx_fmm_options: FmmOptions of the reference (cpp/fmm/fmm_solver.hpp:15-20)."""
+
+    _fields_ = [("theta", c_double), ("leaf_capacity", c_int64), ("max_depth", c_int32),
+                ("expansion_order", c_int32)]
+
+
+class FmmStatsStruct(ctypes.Structure):
+    """gx_fmm_stats: FmmStats of the reference (cpp/fmm/fmm_solver.hpp:22-27)."""
+
+    _fields_ = [("node_count", c_int64), ("leaf_count", c_int64), ("far_interactions", c_int64),
+                ("near_interactions", c_int64)]
+
+
 P = c_void_p  # any array: numpy .ctypes.data, torch .data_ptr(), or None
 PP = POINTER(c_void_p)
 I64 = c_int64
@@ -101,6 +115,9 @@ _SIGNATURES = {
     "gx_session_set_config": [P, c_int, c_int, c_int],
     "gx_session_autotune": [P, c_int, POINTER(D)],
     "gx_p2p_leaves": [I64, P, P, P, P, c_int32, P, P, P, P, Physics, c_int, P, P, P, S],
+    "gx_fmm_accel": [I64, P, P, P, P, Physics, FmmOptionsStruct, c_int, I64, I64, P, P, P, POINTER(FmmStatsStruct),
+                     S],
+    "gx_fmm_moments": [I64, P, P, P, P, Physics, FmmOptionsStruct, I64, P, POINTER(I64)],
     "gx_leaf_lists_build": [I64, P, P, P, P, D, D, I64, c_int, PP],
     "gx_leaf_lists_info": [P, POINTER(c_int32), POINTER(I64), POINTER(I64), POINTER(I64), POINTER(I64)],
     "gx_leaf_lists_export": [P, P, P, P, P],

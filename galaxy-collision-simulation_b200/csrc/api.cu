@@ -6,6 +6,8 @@
 #include "gx.h"
 
 #include "batch.cuh"
+#include "fmm.cuh"
+#include "fmm_tree.hpp"
 #include "force.cuh"
 #include "integrate.cuh"
 #include "p2p.cuh"
@@ -20,6 +22,7 @@
 #include <cstring>
 #include <deque>
 #include <initializer_list>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <new>
@@ -1249,6 +1252,8 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
     cudaStream_t st = (cudaStream_t)stream;
     P2PArgs a;
     a.n_leaves = n_leaves;
+    a.t_begin = 0;
+    a.t_end = n;
     a.G = phys.G;
     a.eps2 = phys.softening * phys.softening;
     a.eps2f = (float)a.eps2;
@@ -1295,6 +1300,217 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
     GX_TRY(copy_back(ay, day, n, st));
     GX_TRY(copy_back(az, daz, n, st));
     GX_CUDA(cudaStreamSynchronize(st));
+    return GX_OK;
+    GX_GUARD_END
+}
+
+// ======================================================================================
+// FMM: reference octree and lists on the host, moments, far field and near field on the
+// device
+// ======================================================================================
+extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                            gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
+                            double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_fmm_accel";
+    if (stats) *stats = gx_fmm_stats{0, 0, 0, 0};
+    if (n < 0 || begin < 0 || end < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: negative size or range", fn);
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (!(opt.theta == opt.theta)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: theta is NaN", fn);
+    end = std::min(end, n);  // compute_targets (fmm_solver.cpp:24-33)
+    if (n == 0 || begin >= end) return GX_OK;
+    if (!x || !y || !z || !m || !ax || !ay || !az) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, ax, ay, az}, &device, &dev, fn));
+    DeviceGuard g(dev);
+    cudaStream_t st = (cudaStream_t)stream;
+
+    // The octree is built on the host from host copies of the positions and masses.
+    std::vector<double> hbuf;
+    const double *hx = x, *hy = y, *hz = z, *hm = m;
+    if (device) {
+        hbuf.resize((size_t)n * 4);
+        const double* src[4] = {x, y, z, m};
+        for (int k = 0; k < 4; ++k)
+            GX_CUDA(cudaMemcpyAsync(hbuf.data() + (size_t)k * n, src[k], (size_t)n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, st));
+        GX_CUDA(cudaStreamSynchronize(st));
+        hx = hbuf.data();
+        hy = hx + n;
+        hz = hy + n;
+        hm = hz + n;
+    }
+    FmmTree T;
+    GX_TRY(build_fmm_tree(n, hx, hy, hz, hm, phys.softening, opt.theta, opt.leaf_capacity, opt.max_depth, true, &T));
+    const int32_t nl = T.n_leaves(), nn = T.n_nodes();
+    if (stats) {
+        stats->node_count = T.all_nodes;
+        stats->leaf_count = nl;
+        stats->far_interactions = T.n_far;
+        stats->near_interactions = (int64_t)T.near_leaf.size();
+    }
+
+    // far-field work items for the leaves that hold a target in [begin, end)
+    std::vector<M2PItem> items;
+    int64_t slots = 0;
+    for (int32_t l = 0; l < nl; ++l) {
+        const int32_t fb = T.far_off[l], fe = T.far_off[l + 1];
+        if (fe == fb) continue;
+        bool any = false;
+        for (int32_t k = T.leaf_off[l]; k < T.leaf_off[l + 1] && !any; ++k)
+            any = T.leaf_part[k] >= begin && T.leaf_part[k] < end;
+        if (!any) continue;
+        const int32_t nch = (fe - fb + kM2PChunk - 1) / kM2PChunk;
+        const int64_t base = nch > 1 ? slots : 0;
+        if (nch > 1) slots += (int64_t)nch * (T.leaf_off[l + 1] - T.leaf_off[l]);
+        for (int32_t c = 0; c < nch; ++c) {
+            M2PItem it;
+            it.leaf = l;
+            it.fb = fb + c * kM2PChunk;
+            it.fe = std::min(fe, it.fb + kM2PChunk);
+            it.chunk = c;
+            it.nchunks = nch;
+            it.pad = 0;
+            it.scratch = base;
+            items.push_back(it);
+        }
+    }
+    if (items.size() > (size_t)std::numeric_limits<int32_t>::max())
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: too many far-field work items", fn);
+
+    HostStage hs(st);
+    const double *dx = x, *dy = y, *dz = z, *dm = m;
+    double *dax = ax, *day = ay, *daz = az;
+    if (!device) {
+        double *tx, *ty, *tz, *tm;
+        GX_TRY(hs.in(x, n, &tx));
+        GX_TRY(hs.in(y, n, &ty));
+        GX_TRY(hs.in(z, n, &tz));
+        GX_TRY(hs.in(m, n, &tm));
+        dx = tx; dy = ty; dz = tz; dm = tm;
+        GX_TRY(hs.out(&dax, n));
+        GX_TRY(hs.out(&day, n));
+        GX_TRY(hs.out(&daz, n));
+    }
+    // reset_accelerations over the target range (fmm_solver.cpp:31); the far and near
+    // fields are then added
+    for (double* p : {dax, day, daz}) GX_CUDA(cudaMemsetAsync(p + begin, 0, (size_t)(end - begin) * sizeof(double), st));
+
+    if (nl > 0) {
+        int32_t *d_lo, *d_lp, *d_ln, *d_nc, *d_nnc, *d_fn, *d_lv, *d_no, *d_nlf;
+        GX_TRY(hs.in_any(T.leaf_off.data(), (int64_t)T.leaf_off.size(), &d_lo));
+        GX_TRY(hs.in_any(T.leaf_part.data(), (int64_t)T.leaf_part.size(), &d_lp));
+        GX_TRY(hs.in_any(T.leaf_node.data(), (int64_t)T.leaf_node.size(), &d_ln));
+        GX_TRY(hs.in_any(T.node_child.data(), (int64_t)nn, &d_nc));
+        GX_TRY(hs.in_any(T.node_nchild.data(), (int64_t)nn, &d_nnc));
+        GX_TRY(hs.in_any(T.far_node.data(), (int64_t)T.far_node.size(), &d_fn));
+        GX_TRY(hs.in_any(T.level_node.data(), (int64_t)T.level_node.size(), &d_lv));
+        GX_TRY(hs.in_any(T.near_off.data(), (int64_t)T.near_off.size(), &d_no));
+        GX_TRY(hs.in_any(T.near_leaf.data(), (int64_t)T.near_leaf.size(), &d_nlf));
+        M2PItem* d_items = nullptr;
+        if (!items.empty()) GX_TRY(hs.in_any(items.data(), (int64_t)items.size(), &d_items));
+        AsyncBuf rec, part, done, p2p_scratch;
+        GX_TRY(rec.alloc((size_t)nn * kFmmRec * sizeof(double), st));
+        GX_TRY(part.alloc((size_t)std::max<int64_t>(slots, 1) * 3 * sizeof(double), st));
+        GX_TRY(done.alloc((size_t)nl * sizeof(int), st));
+        GX_CUDA(cudaMemsetAsync(done.p, 0, (size_t)nl * sizeof(int), st));
+
+        FmmArgs fa;
+        fa.x = dx; fa.y = dy; fa.z = dz; fa.m = dm;
+        fa.leaf_off = d_lo; fa.leaf_part = d_lp; fa.leaf_node = d_ln;
+        fa.node_child = d_nc; fa.node_nchild = d_nnc; fa.far_node = d_fn;
+        fa.n_leaves = nl;
+        fa.rec = rec.d();
+        fa.items = d_items;
+        fa.n_items = (int32_t)items.size();
+        fa.scratch = part.d();
+        fa.done = (int*)done.p;
+        fa.ax = dax; fa.ay = day; fa.az = daz;
+        fa.t_begin = begin;
+        fa.t_end = end;
+        fa.G = phys.G;
+        fa.eps2 = phys.softening * phys.softening;
+        fa.order = fmm_effective_order(std::min(4, std::max(0, opt.expansion_order)));
+        GX_CUDA(launch_fmm_moments(fa, T.level_off.data(), (int)T.level_off.size() - 1, d_lv, st));
+        GX_CUDA(launch_fmm_m2p(fa, st));
+
+        P2PArgs pa;
+        pa.x = dx; pa.y = dy; pa.z = dz; pa.m = dm;
+        pa.leaf_off = d_lo; pa.leaf_part = d_lp; pa.near_off = d_no; pa.near_leaf = d_nlf;
+        pa.n_leaves = nl;
+        pa.ax = dax; pa.ay = day; pa.az = daz;
+        pa.t_begin = begin;
+        pa.t_end = end;
+        pa.G = phys.G;
+        pa.eps2 = phys.softening * phys.softening;
+        pa.eps2f = (float)pa.eps2;
+        GX_TRY(p2p_scratch.alloc(p2p_scratch_bytes(n, nl), st));
+        GX_CUDA(launch_p2p(pa, n, precision, p2p_scratch.p, sm_count(dev), st));
+    }
+    if (!device) {
+        GX_TRY(copy_back(ax + begin, dax + begin, end - begin, st));
+        GX_TRY(copy_back(ay + begin, day + begin, end - begin, st));
+        GX_TRY(copy_back(az + begin, daz + begin, end - begin, st));
+        GX_CUDA(cudaStreamSynchronize(st));
+    }
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gx_fmm_moments(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                              gx_physics phys, gx_fmm_options opt, int64_t capacity, double* records,
+                              int64_t* n_nodes) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_fmm_moments";
+    if (!n_nodes) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n_nodes is null", fn);
+    *n_nodes = 0;
+    if (n < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: n < 0", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (n == 0) return GX_OK;
+    if (!x || !y || !z || !m) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    bool device;
+    int dev;
+    GX_TRY(require_device());
+    GX_TRY(classify({x, y, z, m, records}, &device, &dev, fn));
+    if (device) return fail(GX_ERR_INVALID_ARGUMENT, "%s: host arrays only", fn);
+    DeviceGuard g(dev);
+    FmmTree T;
+    GX_TRY(build_fmm_tree(n, x, y, z, m, phys.softening, opt.theta, opt.leaf_capacity, opt.max_depth, false, &T));
+    const int32_t nn = T.n_nodes(), nl = T.n_leaves();
+    *n_nodes = nn;
+    if (!records || nn == 0) return GX_OK;
+    if (capacity < nn) return fail(GX_ERR_INVALID_ARGUMENT, "%s: records hold %lld nodes, the tree has %d", fn,
+                                   (long long)capacity, nn);
+    cudaStream_t st = nullptr;
+    HostStage hs(st);
+    double *dx, *dy, *dz, *dm;
+    GX_TRY(hs.in(x, n, &dx));
+    GX_TRY(hs.in(y, n, &dy));
+    GX_TRY(hs.in(z, n, &dz));
+    GX_TRY(hs.in(m, n, &dm));
+    int32_t *d_lo, *d_lp, *d_ln, *d_nc, *d_nnc, *d_lv;
+    GX_TRY(hs.in_any(T.leaf_off.data(), (int64_t)T.leaf_off.size(), &d_lo));
+    GX_TRY(hs.in_any(T.leaf_part.data(), (int64_t)T.leaf_part.size(), &d_lp));
+    GX_TRY(hs.in_any(T.leaf_node.data(), (int64_t)T.leaf_node.size(), &d_ln));
+    GX_TRY(hs.in_any(T.node_child.data(), (int64_t)nn, &d_nc));
+    GX_TRY(hs.in_any(T.node_nchild.data(), (int64_t)nn, &d_nnc));
+    GX_TRY(hs.in_any(T.level_node.data(), (int64_t)T.level_node.size(), &d_lv));
+    AsyncBuf rec;
+    GX_TRY(rec.alloc((size_t)nn * kFmmRec * sizeof(double), st));
+    FmmArgs fa{};
+    fa.x = dx; fa.y = dy; fa.z = dz; fa.m = dm;
+    fa.leaf_off = d_lo; fa.leaf_part = d_lp; fa.leaf_node = d_ln;
+    fa.node_child = d_nc; fa.node_nchild = d_nnc;
+    fa.n_leaves = nl;
+    fa.rec = rec.d();
+    GX_CUDA(launch_fmm_moments(fa, T.level_off.data(), (int)T.level_off.size() - 1, d_lv, st));
+    std::vector<double> h((size_t)nn * kFmmRec);
+    GX_CUDA(cudaMemcpyAsync(h.data(), rec.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    for (int32_t k = 0; k < nn; ++k) std::copy(&h[(size_t)k * kFmmRec], &h[(size_t)k * kFmmRec] + 35, records + (size_t)k * 35);
     return GX_OK;
     GX_GUARD_END
 }

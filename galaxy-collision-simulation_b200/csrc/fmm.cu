@@ -1,0 +1,373 @@
+// fmm.cu -- FMM far field on the device: leaf moments (P2M), the upward pass (M2M) and
+// the multipole evaluation at every target (M2P).
+//
+// Moments.  FastMultipoleSolver::p2m_m2m / compute_multipole_moments
+// (cpp/fmm/fmm_solver.cpp:157-208) with add_multipole_point / add_multipole_shifted_child
+// (cpp/fmm/multipole.cpp:218-252) are restated with the reference's operations in the
+// reference's order and no contraction (dadd/dmul), so masses, centres of mass and the 31
+// moments of every node are bit-identical to the reference's.  One warp per node; lane k
+// owns moment 4 + k.  Leaves first, then one launch per tree level, deepest first.
+//
+// M2P.  multipole_acceleration (multipole.cpp:254-296) builds the degree-4 Taylor
+// polynomial of (d + u)_c |d + u|_eps^-3 in the source offset u by truncated polynomial
+// products and contracts it with the moments.  Those Taylor coefficients are the
+// Cartesian derivatives of the softened potential phi(r) = (r.r + eps^2)^-1/2:
+//     a_c = -G sum_k 1/k! M^(k)_{i1..ik} d^(k+1) phi / dr_i1..dr_ik dr_c  at r = d,
+// with d = centre of mass - target and M^(k) the raw k-th moment tensor (M^(0) = mass,
+// M^(1) = 0 about the centre of mass).  Writing g_n = (-1)^n (2n-1)!! s^-(2n+1)/2,
+// s = d.d + eps^2, the derivative tensors are sums of g_n times products of d's and
+// Kronecker deltas, and the contraction per order is
+//     k=0: -m g1 d
+//     k=2: -1/2  [ g3 M[dd] d + g2 (tr M d + 2 M[d]) ]
+//     k=3: -1/6  [ g4 O[ddd] d + g3 (3 (w.d) d + 3 O[dd]) + 3 g2 w ]
+//     k=4: -1/24 [ g5 H[dddd] d + g4 (6 T2[dd] d + 4 H[ddd]) + g3 (3 tr2 d + 12 T2[d]) ]
+// (w, T2, tr2 are the traces stored in the node record).  This is the same polynomial,
+// evaluated in about 170 FP64 operations per (target, node) pair instead of the
+// reference's polynomial algebra; only rounding differs.  Moments of degree above the
+// effective order are left out exactly as evaluate_component does (:205-216).
+#include "fmm.cuh"
+#include "gx_device.cuh"
+
+#include <algorithm>
+
+namespace gx {
+namespace {
+
+constexpr int kMomBlock = 256;  // 8 warps, one node each
+constexpr int kM2PBlock = 128;
+
+// Multi-index of moment slot k (0..34) in the reference's exponent order: degree
+// ascending, then the x exponent descending, then the y exponent descending.
+__device__ __forceinline__ void exponent_of(int k, int& ex, int& ey, int& ez) {
+    int d = 0;
+    while ((d + 1) * (d + 2) * (d + 3) / 6 <= k) ++d;
+    int r = k - d * (d + 1) * (d + 2) / 6;
+    ex = d;
+    while (r > d - ex) {
+        r -= d - ex + 1;
+        --ex;
+    }
+    ey = d - ex - r;
+    ez = d - ex - ey;
+}
+
+// pow_int (multipole.cpp:43-49): 1.0 multiplied by v, e times.
+__device__ __forceinline__ double pow_int(double v, int e) {
+    double r = 1.0;
+    for (int i = 0; i < e; ++i) r = dmul(r, v);
+    return r;
+}
+
+// binomial (multipole.cpp:57-76) for n <= 4.
+__device__ __forceinline__ int binom4(int n, int k) {
+    if (k < 0 || k > n) return 0;
+    if (k == 0 || k == n) return 1;
+    if (n == 2) return 2;
+    if (n == 3) return 3;
+    return k == 2 ? 6 : 4;
+}
+
+// Traces of the moments (record slots 35..45) from slots 4..34.
+__device__ __forceinline__ void write_traces(double* r) {
+    r[kRecTrQ] = r[4] + r[7] + r[9];
+    r[kRecW + 0] = r[10] + r[13] + r[15];
+    r[kRecW + 1] = r[11] + r[16] + r[18];
+    r[kRecW + 2] = r[12] + r[17] + r[19];
+    const double txx = r[20] + r[23] + r[25], tyy = r[23] + r[30] + r[32], tzz = r[25] + r[32] + r[34];
+    r[kRecT2 + 0] = txx;
+    r[kRecT2 + 1] = r[21] + r[26] + r[28];
+    r[kRecT2 + 2] = r[22] + r[27] + r[29];
+    r[kRecT2 + 3] = tyy;
+    r[kRecT2 + 4] = r[24] + r[31] + r[33];
+    r[kRecT2 + 5] = tzz;
+    r[kRecTr2] = txx + tyy + tzz;
+}
+
+// Leaf moments: p2m_m2m leaf branch (fmm_solver.cpp:162-167, 180-181) and
+// compute_multipole_moments leaf branch (:187-193).
+__global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
+    const int w = (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= a.n_leaves) return;
+    const int b = a.leaf_off[w], e = a.leaf_off[w + 1];
+    double* r = a.rec + (size_t)a.leaf_node[w] * kFmmRec;
+    double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    for (int k = b; k < e; ++k) {
+        const int i = a.leaf_part[k];
+        const double mi = a.m[i];
+        mass = dadd(mass, mi);
+        wx = dadd(wx, dmul(a.x[i], mi));
+        wy = dadd(wy, dmul(a.y[i], mi));
+        wz = dadd(wz, dmul(a.z[i], mi));
+    }
+    // leaves in the list have mass > 0 (collect_leaves, :210-216)
+    const double cx = __ddiv_rn(wx, mass), cy = __ddiv_rn(wy, mass), cz = __ddiv_rn(wz, mass);
+    if (lane < 31) {
+        int ex, ey, ez;
+        exponent_of(4 + lane, ex, ey, ez);
+        double v = 0.0;
+        for (int k = b; k < e; ++k) {
+            const int i = a.leaf_part[k];
+            const double ox = dsub(a.x[i], cx), oy = dsub(a.y[i], cy), oz = dsub(a.z[i], cz);
+            const double mono = dmul(dmul(pow_int(ox, ex), pow_int(oy, ey)), pow_int(oz, ez));
+            v = dadd(v, dmul(a.m[i], mono));
+        }
+        r[4 + lane] = v;
+    } else {
+        r[0] = cx;
+        r[1] = cy;
+        r[2] = cz;
+        r[kRecMass] = mass;
+    }
+    __syncwarp();
+    if (lane == 0) write_traces(r);
+}
+
+// Internal node: p2m_m2m (fmm_solver.cpp:168-181) over the massive children in child
+// order, then add_multipole_shifted_child per child (multipole.cpp:227-252).  Massless
+// children add exact zeros in the reference and are not visited.
+__global__ void __launch_bounds__(kMomBlock) fmm_m2m_kernel(const FmmArgs a, const int32_t* nodes, int count) {
+    const int w = (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= count) return;
+    const int node = nodes[w];
+    const int c0 = a.node_child[node], nc = a.node_nchild[node];
+    double* r = a.rec + (size_t)node * kFmmRec;
+    double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    for (int c = 0; c < nc; ++c) {
+        const double* cr = a.rec + (size_t)(c0 + c) * kFmmRec;
+        const double cm = cr[kRecMass];
+        mass = dadd(mass, cm);
+        wx = dadd(wx, dmul(cr[0], cm));
+        wy = dadd(wy, dmul(cr[1], cm));
+        wz = dadd(wz, dmul(cr[2], cm));
+    }
+    const double cx = __ddiv_rn(wx, mass), cy = __ddiv_rn(wy, mass), cz = __ddiv_rn(wz, mass);
+    if (lane < 31) {
+        const int ka = 4 + lane;
+        int ax, ay, az;
+        exponent_of(ka, ax, ay, az);
+        const int da = ax + ay + az;
+        const int nbeta = (da + 1) * (da + 2) * (da + 3) / 6;  // slots of degree <= da
+        double total = 0.0;
+        for (int c = 0; c < nc; ++c) {
+            const double* cr = a.rec + (size_t)(c0 + c) * kFmmRec;
+            const double sx = dsub(cr[0], cx), sy = dsub(cr[1], cy), sz = dsub(cr[2], cz);
+            const double cm = cr[kRecMass];
+            double value = 0.0;
+            for (int kb = 0; kb < nbeta; ++kb) {
+                int bx, by, bz;
+                exponent_of(kb, bx, by, bz);
+                if (bx > ax || by > ay || bz > az) continue;  // multinomial_shift == 0
+                const double bin = (double)(binom4(ax, bx) * binom4(ay, by) * binom4(az, bz));
+                const double sf = dmul(dmul(dmul(bin, pow_int(sx, ax - bx)), pow_int(sy, ay - by)), pow_int(sz, az - bz));
+                if (sf == 0.0) continue;
+                const int db = bx + by + bz;
+                const double mv = db == 0 ? cm : (db == 1 ? 0.0 : cr[kb]);
+                value = dadd(value, dmul(sf, mv));
+            }
+            total = dadd(total, value);
+        }
+        r[ka] = total;
+    } else {
+        r[0] = cx;
+        r[1] = cy;
+        r[2] = cz;
+        r[kRecMass] = mass;
+    }
+    __syncwarp();
+    if (lane == 0) write_traces(r);
+}
+
+// One far node's contribution at one target (without the factor G).
+template <int P>
+__device__ __forceinline__ void m2p_one(const double* __restrict__ r, double tx, double ty, double tz, double eps2,
+                                        double& fx, double& fy, double& fz) {
+    const double dx = r[0] - tx, dy = r[1] - ty, dz = r[2] - tz;
+    const double s = dx * dx + dy * dy + dz * dz + eps2;
+    if (s == 0.0) return;  // h0 == 0 (multipole.cpp:272-275)
+    const double ri = rsqrt_f64(s);
+    const double r2 = ri * ri;
+    const double g1 = -ri * r2;
+    double cd = -r[kRecMass] * g1;  // coefficient of d
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+    if (P >= 2) {
+        const double g2 = -3.0 * g1 * r2, g3 = -5.0 * g2 * r2;
+        const double mx = r[4] * dx + r[5] * dy + r[6] * dz;
+        const double my = r[5] * dx + r[7] * dy + r[8] * dz;
+        const double mz = r[6] * dx + r[8] * dy + r[9] * dz;
+        const double mdd = dx * mx + dy * my + dz * mz;
+        cd -= 0.5 * (g3 * mdd + g2 * r[kRecTrQ]);
+        vx -= g2 * mx;
+        vy -= g2 * my;
+        vz -= g2 * mz;
+        if (P >= 4) {
+            const double g4 = -7.0 * g3 * r2, g5 = -9.0 * g4 * r2;
+            // degree-2 monomials of d weighted 2/nu!
+            const double qxx = dx * dx, qxy = 2.0 * dx * dy, qxz = 2.0 * dx * dz, qyy = dy * dy,
+                         qyz = 2.0 * dy * dz, qzz = dz * dz;
+            const double ox = r[10] * qxx + r[11] * qxy + r[12] * qxz + r[13] * qyy + r[14] * qyz + r[15] * qzz;
+            const double oy = r[11] * qxx + r[13] * qxy + r[14] * qxz + r[16] * qyy + r[17] * qyz + r[18] * qzz;
+            const double oz = r[12] * qxx + r[14] * qxy + r[15] * qxz + r[17] * qyy + r[18] * qyz + r[19] * qzz;
+            const double oddd = dx * ox + dy * oy + dz * oz;
+            const double wd = r[kRecW] * dx + r[kRecW + 1] * dy + r[kRecW + 2] * dz;
+            cd -= g4 * oddd * (1.0 / 6.0) + 0.5 * g3 * wd;
+            vx -= 0.5 * (g3 * ox + g2 * r[kRecW]);
+            vy -= 0.5 * (g3 * oy + g2 * r[kRecW + 1]);
+            vz -= 0.5 * (g3 * oz + g2 * r[kRecW + 2]);
+            // degree-3 monomials of d weighted 6/mu!
+            const double cxxx = qxx * dx, cxxy = 3.0 * qxx * dy, cxxz = 3.0 * qxx * dz, cxyy = 3.0 * dx * qyy,
+                         cxyz = 3.0 * qxy * dz, cxzz = 3.0 * dx * qzz, cyyy = qyy * dy, cyyz = 3.0 * qyy * dz,
+                         cyzz = 3.0 * dy * qzz, czzz = qzz * dz;
+            const double hx = r[20] * cxxx + r[21] * cxxy + r[22] * cxxz + r[23] * cxyy + r[24] * cxyz +
+                              r[25] * cxzz + r[26] * cyyy + r[27] * cyyz + r[28] * cyzz + r[29] * czzz;
+            const double hy = r[21] * cxxx + r[23] * cxxy + r[24] * cxxz + r[26] * cxyy + r[27] * cxyz +
+                              r[28] * cxzz + r[30] * cyyy + r[31] * cyyz + r[32] * cyzz + r[33] * czzz;
+            const double hz = r[22] * cxxx + r[24] * cxxy + r[25] * cxxz + r[27] * cxyy + r[28] * cxyz +
+                              r[29] * cxzz + r[31] * cyyy + r[32] * cyyz + r[33] * cyzz + r[34] * czzz;
+            const double hdddd = dx * hx + dy * hy + dz * hz;
+            const double* T = r + kRecT2;  // xx xy xz yy yz zz
+            const double tx2 = T[0] * dx + T[1] * dy + T[2] * dz;
+            const double ty2 = T[1] * dx + T[3] * dy + T[4] * dz;
+            const double tz2 = T[2] * dx + T[4] * dy + T[5] * dz;
+            const double tdd = dx * tx2 + dy * ty2 + dz * tz2;
+            cd -= g5 * hdddd * (1.0 / 24.0) + 0.25 * g4 * tdd + 0.125 * g3 * r[kRecTr2];
+            const double k4 = g4 * (1.0 / 6.0), k3 = 0.5 * g3;
+            vx -= k4 * hx + k3 * tx2;
+            vy -= k4 * hy + k3 * ty2;
+            vz -= k4 * hz + k3 * tz2;
+        }
+    }
+    fx += cd * dx + vx;
+    fy += cd * dy + vy;
+    fz += cd * dz + vz;
+}
+
+// Work item = (target leaf, up to kM2PChunk far nodes).  The item's node records are
+// staged in shared memory; thread t evaluates target t % W against nodes t / W,
+// t / W + S, ... (W = targets rounded up to a power of two, S = block / W); the S partial
+// sums of a target are added in slot order, so results do not depend on scheduling.
+template <int P>
+__global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
+    constexpr int NEED = P == 0 ? 4 : (P == 2 ? kRecTrQ + 1 : kRecTr2 + 1);
+    __shared__ __align__(16) double s_rec[kM2PChunk * kFmmRec];
+    __shared__ double s_red[kM2PBlock * 3];
+    __shared__ int s_last;
+    const int tid = threadIdx.x;
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const M2PItem w = a.items[it];
+        const int cnt = w.fe - w.fb;
+        for (int k = tid; k < cnt * NEED; k += kM2PBlock) {
+            const int j = k / NEED, c = k - j * NEED;
+            s_rec[j * kFmmRec + c] = a.rec[(size_t)a.far_node[w.fb + j] * kFmmRec + c];
+        }
+        __syncthreads();
+        const int tb = a.leaf_off[w.leaf], nt = a.leaf_off[w.leaf + 1] - tb;
+        int W = 1;
+        while (W < nt && W < kM2PBlock) W <<= 1;
+        const int S = kM2PBlock / W;
+        const int q = tid / W, tl = tid % W;
+        for (int t0 = 0; t0 < nt; t0 += W) {
+            const int t = t0 + tl;
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            int i = -1;
+            if (t < nt) {
+                i = a.leaf_part[tb + t];
+                if (i >= a.t_begin && i < a.t_end) {
+                    const double tx = a.x[i], ty = a.y[i], tz = a.z[i];
+                    for (int j = q; j < cnt; j += S) m2p_one<P>(s_rec + j * kFmmRec, tx, ty, tz, a.eps2, fx, fy, fz);
+                } else {
+                    i = -1;
+                }
+            }
+            s_red[tid * 3 + 0] = fx;
+            s_red[tid * 3 + 1] = fy;
+            s_red[tid * 3 + 2] = fz;
+            __syncthreads();
+            if (q == 0 && i >= 0) {
+                double sx = 0.0, sy = 0.0, sz = 0.0;
+                for (int k = 0; k < S; ++k) {
+                    const int o = (k * W + tl) * 3;
+                    sx += s_red[o];
+                    sy += s_red[o + 1];
+                    sz += s_red[o + 2];
+                }
+                if (w.nchunks == 1) {
+                    a.ax[i] = a.ax[i] + a.G * sx;
+                    a.ay[i] = a.ay[i] + a.G * sy;
+                    a.az[i] = a.az[i] + a.G * sz;
+                } else {
+                    const size_t o = (size_t)(w.scratch + (int64_t)w.chunk * nt + t) * 3;
+                    a.scratch[o] = sx;
+                    a.scratch[o + 1] = sy;
+                    a.scratch[o + 2] = sz;
+                }
+            }
+            __syncthreads();
+        }
+        if (w.nchunks > 1) {
+            // The CTA that completes the leaf's last chunk adds the partials in chunk order.
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = (atomicAdd(&a.done[w.leaf], 1) == w.nchunks - 1);
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                for (int t = tid; t < nt; t += kM2PBlock) {
+                    const int i = a.leaf_part[tb + t];
+                    if (i < a.t_begin || i >= a.t_end) continue;
+                    double sx = 0.0, sy = 0.0, sz = 0.0;
+                    for (int c = 0; c < w.nchunks; ++c) {
+                        const size_t o = (size_t)(w.scratch + (int64_t)c * nt + t) * 3;
+                        sx += __ldcg(&a.scratch[o]);
+                        sy += __ldcg(&a.scratch[o + 1]);
+                        sz += __ldcg(&a.scratch[o + 2]);
+                    }
+                    a.ax[i] = a.ax[i] + a.G * sx;
+                    a.ay[i] = a.ay[i] + a.G * sy;
+                    a.az[i] = a.az[i] + a.G * sz;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace
+
+int fmm_effective_order(int expansion_order) {
+    int p = std::min(4, std::max(0, expansion_order));
+    if (p == 1 || p == 3) ++p;
+    return p;
+}
+
+cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels,
+                               const int32_t* level_node_dev, cudaStream_t st) {
+    constexpr int wpb = kMomBlock / 32;
+    if (a.n_leaves > 0) {
+        fmm_leaf_kernel<<<(a.n_leaves + wpb - 1) / wpb, kMomBlock, 0, st>>>(a);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    for (int d = n_levels - 1; d >= 0; --d) {
+        const int count = level_off_host[d + 1] - level_off_host[d];
+        if (count == 0) continue;
+        fmm_m2m_kernel<<<(count + wpb - 1) / wpb, kMomBlock, 0, st>>>(a, level_node_dev + level_off_host[d], count);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st) {
+    if (a.n_items == 0) return cudaSuccess;
+    const int grid = std::min(a.n_items, 1 << 20);
+    switch (a.order) {
+        case 0: fmm_m2p_kernel<0><<<grid, kM2PBlock, 0, st>>>(a); break;
+        case 2: fmm_m2p_kernel<2><<<grid, kM2PBlock, 0, st>>>(a); break;
+        default: fmm_m2p_kernel<4><<<grid, kM2PBlock, 0, st>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace gx

@@ -1,0 +1,67 @@
+// fmm.cuh -- launchers of the FMM far field: leaf moments (P2M), the upward pass (M2M)
+// and the multipole evaluation at the targets (M2P).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gx {
+
+// One node record, 48 doubles (384 B):
+//   [0..2]   centre of mass        [3]      mass
+//   [4..34]  raw moments sum m u^a, u = body - centre of mass, for the 31 multi-indices a
+//            of degree 2..4 in the reference's exponent order (multipole.cpp:16-26),
+//            so record[k] is the reference's moment values[k]
+//   [35]     trace of the degree-2 moments            sum m |u|^2
+//   [36..38] traces of the degree-3 moments           sum m |u|^2 u_i
+//   [39..44] traces of the degree-4 moments (xx xy xz yy yz zz)  sum m |u|^2 u_i u_j
+//   [45]     double trace                             sum m |u|^4
+constexpr int kFmmRec = 48;
+constexpr int kRecMass = 3, kRecMom = 4, kRecTrQ = 35, kRecW = 36, kRecT2 = 39, kRecTr2 = 45;
+
+// Far-field work item: one target leaf and a chunk of its far list.
+struct M2PItem {
+    int32_t leaf;
+    int32_t fb, fe;   // far_node[fb .. fe)
+    int32_t chunk;    // index of this chunk among the leaf's chunks
+    int32_t nchunks;
+    int32_t pad;
+    int64_t scratch;  // first partial-sum slot of the leaf (targets), when nchunks > 1
+};
+
+struct FmmArgs {
+    const double* x;
+    const double* y;
+    const double* z;
+    const double* m;
+    const int32_t* leaf_off;
+    const int32_t* leaf_part;
+    const int32_t* leaf_node;
+    const int32_t* node_child;
+    const int32_t* node_nchild;
+    const int32_t* far_node;
+    int32_t n_leaves;
+    double* rec;  // n_nodes * kFmmRec
+    const M2PItem* items;
+    int32_t n_items;
+    double* scratch;  // partial sums of split leaves: 3 doubles per (chunk, target)
+    int* done;        // chunks finished per leaf (zeroed before the launch)
+    double* ax;       // accumulated into
+    double* ay;
+    double* az;
+    int64_t t_begin, t_end;  // only bodies in [t_begin, t_end) are written
+    double G;
+    double eps2;
+    int order;  // effective expansion order: 0, 2 or 4
+};
+
+// Effective expansion order of multipole_acceleration (multipole.cpp:261-265).
+int fmm_effective_order(int expansion_order);
+constexpr int kM2PChunk = 64;  // far nodes per work item
+
+// Stream-ordered: leaf moments, then one launch per level (deepest first), then M2P.
+cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels,
+                               const int32_t* level_node_dev, cudaStream_t st);
+cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st);
+
+}  // namespace gx

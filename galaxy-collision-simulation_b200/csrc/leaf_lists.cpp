@@ -12,6 +12,7 @@
 // massless subtrees.  The tree must be identical, not merely similar: the P2P sum of the
 // drop-in runs over exactly these lists.
 #include "gx.h"
+#include "fmm_tree.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -24,9 +25,7 @@
 extern "C" int gxi_fail(int code, const char* msg);
 
 struct gx_leaf_lists {
-    std::vector<int32_t> leaf_offsets, leaf_particles, near_offsets, near_leaves;
-    int64_t n_far = 0;
-    int64_t n_pairs = 0;
+    gx::FmmTree t;
 };
 
 namespace {
@@ -38,6 +37,7 @@ struct Node {
     int child0;  // first of 8 consecutive children, -1 for a leaf
     int64_t beg, end;
     int leaf_id;
+    int id;  // breadth-first number among massive nodes, -1 when massless
 };
 
 struct Builder {
@@ -119,32 +119,33 @@ struct Builder {
         return comb / dist < theta;
     }
 
-    void walk(int target, int source, std::vector<int32_t>& near, int64_t& n_far) const {
+    void walk(int target, int source, std::vector<int32_t>& near, std::vector<int32_t>* far, int64_t& n_far) const {
         const Node& s = nodes[source];
         if (s.mass <= 0.0) return;
         if (source != target && well_separated(nodes[target], s)) {
             ++n_far;
+            if (far) far->push_back(s.id);
             return;
         }
         if (s.child0 < 0) {
             near.push_back(s.leaf_id);
             return;
         }
-        for (int c = 0; c < 8; ++c) walk(target, s.child0 + c, near, n_far);
+        for (int c = 0; c < 8; ++c) walk(target, s.child0 + c, near, far, n_far);
     }
 };
 
 }  // namespace
 
-extern "C" int gx_leaf_lists_build(int64_t n, const double* x, const double* y, const double* z,
-                                   const double* m, double softening, double theta,
-                                   int64_t leaf_capacity, int max_depth, gx_leaf_lists** out) {
-    if (!out) return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: out is null");
-    *out = nullptr;
-    if (n <= 0 || !x || !y || !z || !m)
-        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: need n > 0 and x, y, z, m");
+namespace gx {
+
+int build_fmm_tree(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                   double softening, double theta, int64_t leaf_capacity, int max_depth, bool want_far,
+                   FmmTree* out) {
+    if (n <= 0 || !x || !y || !z || !m || !out)
+        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "octree: need n > 0 and x, y, z, m");
     if (n > (int64_t)std::numeric_limits<int32_t>::max())
-        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: n exceeds the int32 index range");
+        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "octree: n exceeds the int32 index range");
     try {
         Builder b;
         b.x = x;
@@ -169,6 +170,7 @@ extern "C" int gx_leaf_lists_build(int64_t n, const double* x, const double* y, 
             mx[1] = std::max(mx[1], y[i]);
             mx[2] = std::max(mx[2], z[i]);
         }
+        // root cell (fmm_solver.cpp:77-85)
         Node root{};
         for (int c = 0; c < 3; ++c) root.c[c] = (mn[c] + mx[c]) * 0.5;
         root.hw = 0.5 * std::max({mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]});
@@ -184,57 +186,130 @@ extern "C" int gx_leaf_lists_build(int64_t n, const double* x, const double* y, 
         std::vector<int> leaves;
         b.collect(0, leaves);
 
-        gx_leaf_lists* L = new gx_leaf_lists();
-        L->leaf_offsets.resize(leaves.size() + 1);
-        L->near_offsets.resize(leaves.size() + 1);
-        L->leaf_particles.reserve((size_t)n);
-        std::vector<int32_t> near;
-        for (size_t l = 0; l < leaves.size(); ++l) {
+        FmmTree& T = *out;
+        T = FmmTree();
+        T.all_nodes = (int64_t)b.nodes.size();
+        // breadth-first numbering of the massive nodes; children of one node stay consecutive
+        std::vector<int> bfs, depth;
+        for (Node& nd : b.nodes) nd.id = -1;
+        if (b.nodes[0].mass > 0.0) {
+            bfs.push_back(0);
+            depth.push_back(0);
+            b.nodes[0].id = 0;
+        }
+        for (size_t k = 0; k < bfs.size(); ++k) {
+            const Node& nd = b.nodes[bfs[k]];
+            if (nd.child0 < 0) continue;
+            for (int c = 0; c < 8; ++c) {
+                Node& ch = b.nodes[nd.child0 + c];
+                if (ch.mass <= 0.0) continue;
+                ch.id = (int)bfs.size();
+                bfs.push_back(nd.child0 + c);
+                depth.push_back(depth[k] + 1);
+            }
+        }
+        const int nn = (int)bfs.size();
+        T.node_child.assign(nn, -1);
+        T.node_nchild.assign(nn, 0);
+        int max_level = 0;
+        for (int k = 0; k < nn; ++k) {
+            const Node& nd = b.nodes[bfs[k]];
+            max_level = std::max(max_level, depth[k]);
+            if (nd.child0 < 0) continue;
+            for (int c = 0; c < 8; ++c) {
+                const Node& ch = b.nodes[nd.child0 + c];
+                if (ch.mass <= 0.0) continue;
+                if (T.node_child[k] < 0) T.node_child[k] = ch.id;
+                T.node_nchild[k]++;
+            }
+        }
+        T.level_off.assign(max_level + 2, 0);
+        for (int k = 0; k < nn; ++k)
+            if (T.node_child[k] >= 0) T.level_off[depth[k] + 1]++;
+        for (int d = 0; d <= max_level; ++d) T.level_off[d + 1] += T.level_off[d];
+        T.level_node.resize(T.level_off[max_level + 1]);
+        {
+            std::vector<int32_t> fill(T.level_off.begin(), T.level_off.end() - 1);
+            for (int k = 0; k < nn; ++k)
+                if (T.node_child[k] >= 0) T.level_node[fill[depth[k]]++] = k;
+        }
+
+        const size_t nl = leaves.size();
+        T.leaf_off.resize(nl + 1);
+        T.near_off.resize(nl + 1);
+        T.far_off.resize(nl + 1);
+        T.leaf_node.resize(nl);
+        T.leaf_part.reserve((size_t)n);
+        for (size_t l = 0; l < nl; ++l) {
             const Node& nd = b.nodes[leaves[l]];
-            L->leaf_offsets[l] = (int32_t)L->leaf_particles.size();
-            for (int64_t k = nd.beg; k < nd.end; ++k) L->leaf_particles.push_back((int32_t)b.perm[(size_t)k]);
+            T.leaf_node[l] = nd.id;
+            T.leaf_off[l] = (int32_t)T.leaf_part.size();
+            for (int64_t k = nd.beg; k < nd.end; ++k) T.leaf_part.push_back((int32_t)b.perm[(size_t)k]);
         }
-        L->leaf_offsets[leaves.size()] = (int32_t)L->leaf_particles.size();
-        for (size_t l = 0; l < leaves.size(); ++l) {
-            L->near_offsets[l] = (int32_t)L->near_leaves.size();
+        T.leaf_off[nl] = (int32_t)T.leaf_part.size();
+        std::vector<int32_t> near;
+        for (size_t l = 0; l < nl; ++l) {
+            T.near_off[l] = (int32_t)T.near_leaf.size();
+            T.far_off[l] = (int32_t)T.far_node.size();
             near.clear();
-            b.walk(leaves[l], 0, near, L->n_far);
-            const int64_t nt = L->leaf_offsets[l + 1] - L->leaf_offsets[l];
+            b.walk(leaves[l], 0, near, want_far ? &T.far_node : nullptr, T.n_far);
+            const int64_t nt = T.leaf_off[l + 1] - T.leaf_off[l];
             for (int32_t s : near) {
-                L->near_leaves.push_back(s);
-                L->n_pairs += nt * (int64_t)(L->leaf_offsets[s + 1] - L->leaf_offsets[s]);
+                T.near_leaf.push_back(s);
+                T.n_pairs += nt * (int64_t)(T.leaf_off[s + 1] - T.leaf_off[s]);
             }
-            if (L->near_leaves.size() > (size_t)std::numeric_limits<int32_t>::max()) {
-                delete L;
-                return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: near lists exceed the int32 range");
-            }
+            if (T.near_leaf.size() > (size_t)std::numeric_limits<int32_t>::max() ||
+                T.far_node.size() > (size_t)std::numeric_limits<int32_t>::max())
+                return gxi_fail(GX_ERR_INVALID_ARGUMENT, "octree: interaction lists exceed the int32 range");
         }
-        L->near_offsets[leaves.size()] = (int32_t)L->near_leaves.size();
-        *out = L;
+        T.near_off[nl] = (int32_t)T.near_leaf.size();
+        T.far_off[nl] = (int32_t)T.far_node.size();
         return GX_OK;
     } catch (const std::bad_alloc&) {
-        return gxi_fail(GX_ERR_OUT_OF_MEMORY, "gx_leaf_lists_build: host allocation failed");
+        return gxi_fail(GX_ERR_OUT_OF_MEMORY, "octree: host allocation failed");
     }
+}
+
+}  // namespace gx
+
+extern "C" int gx_leaf_lists_build(int64_t n, const double* x, const double* y, const double* z,
+                                   const double* m, double softening, double theta,
+                                   int64_t leaf_capacity, int max_depth, gx_leaf_lists** out) {
+    if (!out) return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: out is null");
+    *out = nullptr;
+    if (n <= 0 || !x || !y || !z || !m)
+        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: need n > 0 and x, y, z, m");
+    if (n > (int64_t)std::numeric_limits<int32_t>::max())
+        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build: n exceeds the int32 index range");
+    gx_leaf_lists* L = new (std::nothrow) gx_leaf_lists();
+    if (!L) return gxi_fail(GX_ERR_OUT_OF_MEMORY, "gx_leaf_lists_build: host allocation failed");
+    const int rc = gx::build_fmm_tree(n, x, y, z, m, softening, theta, leaf_capacity, max_depth, false, &L->t);
+    if (rc != GX_OK) {
+        delete L;
+        return rc;
+    }
+    *out = L;
+    return GX_OK;
 }
 
 extern "C" int gx_leaf_lists_info(const gx_leaf_lists* l, int32_t* n_leaves, int64_t* n_leaf_particles,
                                   int64_t* n_near, int64_t* n_far, int64_t* n_p2p_pairs) {
     if (!l) return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_info: null handle");
-    if (n_leaves) *n_leaves = (int32_t)(l->leaf_offsets.size() - 1);
-    if (n_leaf_particles) *n_leaf_particles = (int64_t)l->leaf_particles.size();
-    if (n_near) *n_near = (int64_t)l->near_leaves.size();
-    if (n_far) *n_far = l->n_far;
-    if (n_p2p_pairs) *n_p2p_pairs = l->n_pairs;
+    if (n_leaves) *n_leaves = l->t.n_leaves();
+    if (n_leaf_particles) *n_leaf_particles = (int64_t)l->t.leaf_part.size();
+    if (n_near) *n_near = (int64_t)l->t.near_leaf.size();
+    if (n_far) *n_far = l->t.n_far;
+    if (n_p2p_pairs) *n_p2p_pairs = l->t.n_pairs;
     return GX_OK;
 }
 
 extern "C" int gx_leaf_lists_export(const gx_leaf_lists* l, int32_t* leaf_offsets, int32_t* leaf_particles,
                                     int32_t* near_offsets, int32_t* near_leaves) {
     if (!l) return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_export: null handle");
-    if (leaf_offsets) std::copy(l->leaf_offsets.begin(), l->leaf_offsets.end(), leaf_offsets);
-    if (leaf_particles) std::copy(l->leaf_particles.begin(), l->leaf_particles.end(), leaf_particles);
-    if (near_offsets) std::copy(l->near_offsets.begin(), l->near_offsets.end(), near_offsets);
-    if (near_leaves) std::copy(l->near_leaves.begin(), l->near_leaves.end(), near_leaves);
+    if (leaf_offsets) std::copy(l->t.leaf_off.begin(), l->t.leaf_off.end(), leaf_offsets);
+    if (leaf_particles) std::copy(l->t.leaf_part.begin(), l->t.leaf_part.end(), leaf_particles);
+    if (near_offsets) std::copy(l->t.near_off.begin(), l->t.near_off.end(), near_offsets);
+    if (near_leaves) std::copy(l->t.near_leaf.begin(), l->t.near_leaf.end(), near_leaves);
     return GX_OK;
 }
 

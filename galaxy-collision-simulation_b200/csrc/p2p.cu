@@ -164,8 +164,8 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
 
         for (int pass = 0; pass * slots < nt; ++pass) {
             const int t = pass * slots + slot;
-            const bool ok = t < nt;
-            const int i = ok ? a.leaf_part[tb + t] : first;
+            const int i = t < nt ? a.leaf_part[tb + t] : first;
+            const bool ok = t < nt && i >= a.t_begin && i < a.t_end;
             const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
             const float xf = __double2float_rn(xi - ox), yf = __double2float_rn(yi - oy),
                         zf = __double2float_rn(zi - oz);
@@ -348,6 +348,7 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
         __threadfence();
         for (int t = tid; t < nt; t += kP2PBlock) {
             const int i = a.leaf_part[tb + t];
+            if (i < a.t_begin || i >= a.t_end) continue;
             double sx = 0.0, sy = 0.0, sz = 0.0;
             for (int c = 0; c < chunks; ++c) {
                 const size_t k = (size_t)(a.plan_scratch[leaf] + (int64_t)c * nt + t) * 3;

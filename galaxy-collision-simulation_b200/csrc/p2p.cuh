@@ -19,6 +19,7 @@ struct P2PArgs {
     double* ax;  // accumulated into
     double* ay;
     double* az;
+    int64_t t_begin, t_end;  // only bodies in [t_begin, t_end) are written
     double G;
     double eps2;
     float eps2f;

@@ -174,6 +174,43 @@ int gx_p2p_leaves(int64_t n, const double* x, const double* y, const double* z,
                   const int32_t* near_leaves, gx_physics phys, int precision, double* ax,
                   double* ay, double* az, void* stream);
 
+/* ---- FMM (cpp/fmm/fmm_solver.hpp:15-20, fmm_solver.cpp:315-333) --------------------- */
+/* FmmOptions with the reference's defaults: theta 0.6, leaf_capacity 16, max_depth 32,
+ * expansion_order 4. */
+typedef struct gx_fmm_options {
+    double theta;
+    int64_t leaf_capacity;
+    int32_t max_depth;
+    int32_t expansion_order;
+} gx_fmm_options;
+
+/* FmmStats (fmm_solver.hpp:22-27). */
+typedef struct gx_fmm_stats {
+    int64_t node_count;
+    int64_t leaf_count;
+    int64_t far_interactions;
+    int64_t near_interactions;
+} gx_fmm_stats;
+
+/* compute_fmm_accelerations_for_targets (fmm_solver.cpp:324-333); begin = 0, end = n is
+ * compute_fmm_accelerations (:315-322).  The reference octree and its interaction lists
+ * are built on the host; the node moments (bit-identical to the reference's), the
+ * multipole far field (FP64) and the P2P near field (in `precision`) run on the device.
+ * Only bodies in [begin, min(end, n)) are written; bodies of massless leaves get zero, as
+ * in the reference.  Host or device arrays; `stats` may be NULL. */
+int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                 gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
+                 double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream);
+
+/* Node data of the reference octree (p2m_m2m / compute_multipole_moments,
+ * fmm_solver.cpp:157-208), computed on the device: for every node with mass > 0, numbered
+ * breadth-first from the root with children in octant order, 35 doubles: centre of mass
+ * (3), mass, and moment values[4..34] in the reference's exponent order.  Bit-identical
+ * to the reference's.  Host arrays only; records == NULL returns the node count. */
+int gx_fmm_moments(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                   gx_physics phys, gx_fmm_options opt, int64_t capacity, double* records,
+                   int64_t* n_nodes);
+
 /* Leaf lists of the reference octree (FastMultipoleSolver::build, fmm_solver.cpp:48-98,
  * 210-277) built on the host as CSR arrays for gx_p2p_leaves. Host arrays only. */
 typedef struct gx_leaf_lists gx_leaf_lists;

@@ -74,6 +74,10 @@ def ref():
         lib.ref_fmm_split.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int,
                                       POINTER(c_int32), POINTER(c_int64), P, P, P, P, P, P, P]
         lib.ref_smoke80_inputs.argtypes = [P, P, P, P]
+        lib.ref_fmm_moments.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, c_int64, P,
+                                        POINTER(c_int64), P]
+        lib.ref_fmm_timed.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, c_int64, c_int,
+                                      P, P, P, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]
         lib.ref_leapfrog_fmm.argtypes = [c_int64, P, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, c_int,
                                          c_double, c_int64, c_int]
         _ref = lib
@@ -229,6 +233,31 @@ def ref_fmm_split(x, y, z, m, G, eps, theta, leaf_capacity, order=4):
     ref().ref_fmm_split(n, _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, ctypes.byref(nl),
                         ctypes.byref(nn), _p(lo), _p(lp), _p(no), _p(nlv), *map(_p, far))
     return dict(leaf_offsets=lo, leaf_particles=lp, near_offsets=no, near_leaves=nlv[: nn.value]), np.stack(far, 1)
+
+
+def ref_fmm_moments(x, y, z, m, G, eps, theta, leaf_capacity, order=4):
+    """(records (n_nodes, 35), stats (4,)) of the reference tree's massive nodes, breadth-first."""
+    x, y, z, m = map(_f, (x, y, z, m))
+    nn = c_int64()
+    stats = np.zeros(4, np.int64)
+    ref().ref_fmm_moments(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, 0, None,
+                          ctypes.byref(nn), _p(stats))
+    rec = np.zeros((max(nn.value, 1), 35))
+    ref().ref_fmm_moments(len(x), _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, nn.value, _p(rec),
+                          ctypes.byref(nn), _p(stats))
+    return rec[: nn.value], stats
+
+
+def ref_fmm_timed(x, y, z, m, G, eps, theta, leaf_capacity, order, stride, threads):
+    """Reference build + evaluate_particle on every stride-th body (leaf order) over threads.
+    Returns (accelerations (n, 3) with NaN where not evaluated, build_s, eval_s, n_evaluated)."""
+    x, y, z, m = map(_f, (x, y, z, m))
+    n = len(x)
+    out = [np.full(n, np.nan) for _ in range(3)]
+    b, e, k = c_double(), c_double(), c_int64()
+    ref().ref_fmm_timed(n, _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, stride, threads,
+                        *map(_p, out), ctypes.byref(b), ctypes.byref(e), ctypes.byref(k))
+    return np.stack(out, 1), b.value, e.value, k.value
 
 
 def ref_smoke80_inputs():

@@ -10,6 +10,7 @@
 // GPU" exactly as the drop-in does) this translation unit alone re-opens the class with
 // `#define private public` before including the reference header.  Nothing in the
 // reference is changed or copied.
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <random>
@@ -205,6 +206,85 @@ int ref_fmm_split(int64_t n, const double* x, const double* y, const double* z, 
         }
     }
     return 0;
+}
+
+// Node data of the reference tree after FastMultipoleSolver::build: every node with
+// mass > 0, breadth-first from the root with children in octant order, 35 doubles each
+// (centre of mass, mass, moments.values[4..34]); stats = FmmStats (fmm_solver.hpp:22-27).
+int ref_fmm_moments(int64_t n, const double* x, const double* y, const double* z, const double* m, double G,
+                    double eps, double theta, int64_t leaf_capacity, int order, int64_t capacity, double* records,
+                    int64_t* n_nodes, int64_t* stats) {
+    auto p = to_particles(n, x, y, z, m);
+    fmmgalaxy::FmmOptions o;
+    o.theta = theta;
+    o.leaf_capacity = static_cast<std::size_t>(leaf_capacity);
+    o.expansion_order = order;
+    fmmgalaxy::FastMultipoleSolver solver(physics(G, eps), o);
+    solver.build(p);
+    const auto& nodes = solver.nodes_;
+    std::vector<int> bfs;
+    if (!nodes.empty() && nodes[0].mass > 0.0) bfs.push_back(0);
+    for (std::size_t k = 0; k < bfs.size(); ++k)
+        for (int c : nodes[bfs[k]].children)
+            if (c >= 0 && nodes[c].mass > 0.0) bfs.push_back(c);
+    *n_nodes = static_cast<int64_t>(bfs.size());
+    const auto& s = solver.stats();
+    stats[0] = static_cast<int64_t>(s.node_count);
+    stats[1] = static_cast<int64_t>(s.leaf_count);
+    stats[2] = static_cast<int64_t>(s.far_interactions);
+    stats[3] = static_cast<int64_t>(s.near_interactions);
+    if (!records || capacity < static_cast<int64_t>(bfs.size())) return 0;
+    for (std::size_t k = 0; k < bfs.size(); ++k) {
+        const auto& nd = nodes[bfs[k]];
+        double* r = records + k * 35;
+        r[0] = nd.center_of_mass.x; r[1] = nd.center_of_mass.y; r[2] = nd.center_of_mass.z;
+        r[3] = nd.mass;
+        for (int j = 4; j < 35; ++j) r[j] = nd.moments.values[j];
+    }
+    return 0;
+}
+
+// Times the reference FMM on the host: FastMultipoleSolver::build once, then
+// evaluate_particle (fmm_solver.cpp:279-310, a const method) for every stride-th body in
+// leaf order, those bodies split over `threads` host threads.  The evaluated
+// accelerations are written to (ax, ay, az) (others are left untouched) so a caller can
+// check them.
+void ref_fmm_timed(int64_t n, const double* x, const double* y, const double* z, const double* m, double G,
+                   double eps, double theta, int64_t leaf_capacity, int order, int64_t stride, int threads,
+                   double* ax, double* ay, double* az, double* build_s, double* eval_s, int64_t* n_eval) {
+    auto p = to_particles(n, x, y, z, m);
+    fmmgalaxy::FmmOptions o;
+    o.theta = theta;
+    o.leaf_capacity = static_cast<std::size_t>(leaf_capacity);
+    o.expansion_order = order;
+    fmmgalaxy::FastMultipoleSolver solver(physics(G, eps), o);
+    const auto t0 = std::chrono::steady_clock::now();
+    solver.build(p);
+    const auto t1 = std::chrono::steady_clock::now();
+    std::vector<std::pair<std::size_t, int>> work;  // (body, leaf node)
+    int64_t k = 0;
+    for (int li : solver.leaf_indices_)
+        for (std::size_t q : solver.nodes_[li].particle_indices)
+            if (k++ % stride == 0) work.emplace_back(q, li);
+    if (threads < 1) threads = 1;
+    std::vector<std::thread> pool;
+    const auto t2 = std::chrono::steady_clock::now();
+    for (int r = 0; r < threads; ++r) {
+        const auto own = fmmgalaxy::ownership_for_rank(work.size(), r, threads);
+        pool.emplace_back([&, own] {
+            for (std::size_t w = own.begin; w < own.end; ++w) {
+                const auto a = solver.evaluate_particle(work[w].first, solver.nodes_[work[w].second]);
+                ax[work[w].first] = a.x;
+                ay[work[w].first] = a.y;
+                az[work[w].first] = a.z;
+            }
+        });
+    }
+    for (auto& t : pool) t.join();
+    const auto t3 = std::chrono::steady_clock::now();
+    *build_s = std::chrono::duration<double>(t1 - t0).count();
+    *eval_s = std::chrono::duration<double>(t3 - t2).count();
+    *n_eval = static_cast<int64_t>(work.size());
 }
 
 // The inputs of the reference smoke test's solver-agreement case (smoke_tests.cpp:83-89):

@@ -1,0 +1,187 @@
+"""The reference FMM on B200 (gx_fmm_accel) vs the reference itself.
+
+Node masses, centres of mass and moments are bit-identical to the reference's
+(p2m_m2m / compute_multipole_moments, cpp/fmm/fmm_solver.cpp:157-208).  The far field is
+the same degree-4 polynomial as multipole_acceleration (cpp/fmm/multipole.cpp:254-296)
+evaluated in closed form, so full accelerations agree with the reference FMM to rounding:
+FP64 form, relative error per body <= 1e-12 (median <= 1e-14).
+"""
+import numpy as np
+import pytest
+import torch
+
+import gx
+import oracle
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+F64, MIX, EXACT = gx.PRECISION_F64, gx.PRECISION_MIXED, gx.PRECISION_F64_EXACT
+need_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+
+
+def fmm(x, y, z, m, eps, theta, cap, order=4, prec=F64, begin=0, end=None, G=1.0):
+    a = [np.zeros(len(x)) for _ in range(3)]
+    st = gx.fmm.fmm_accelerations(x, y, z, m, *a, gx.PhysicsParams(G, eps), gx.FmmOptions(theta, cap, 32, order), prec,
+                                  begin, end)
+    return np.stack(a, 1), st
+
+
+def test_reference_fmm_fixture(golden):
+    g = golden("fmm1000.npz")
+    eps, theta, cap = float(g["softening"]), float(g["theta"]), int(g["leaf_capacity"])
+    ref = np.stack([g["ax"], g["ay"], g["az"]], 1)
+    a, _ = fmm(g["x"], g["y"], g["z"], g["m"], eps, theta, cap)
+    e = rel_err(a, ref)
+    assert e.max() <= 1e-12 and np.median(e) <= 1e-14
+
+
+@need_ref
+@pytest.mark.parametrize("n,cap,theta", [(4000, 16, 0.6), (20000, 64, 0.6), (6000, 8, 0.35), (3000, 200, 0.9)])
+def test_fmm_vs_reference(n, cap, theta):
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, n + cap, 0.02)
+    ref = oracle.ref_fmm(p.x, p.y, p.z, p.m, 1.0, 0.02, theta, cap)
+    a, st = fmm(p.x, p.y, p.z, p.m, 0.02, theta, cap)
+    e = rel_err(a, ref)
+    assert e.max() <= 1e-12 and np.median(e) <= 1e-14
+    _, rs = oracle.ref_fmm_moments(p.x, p.y, p.z, p.m, 1.0, 0.02, theta, cap)
+    assert (st.node_count, st.leaf_count, st.far_interactions, st.near_interactions) == tuple(rs)
+
+
+@need_ref
+@pytest.mark.parametrize("order", [0, 1, 2, 3, 4, 7, -2])
+def test_expansion_orders(order):
+    p = gx.ics.two_disk_encounter(1500, 1500, 5, 0.03)
+    ref = oracle.ref_fmm(p.x, p.y, p.z, p.m, 1.0, 0.03, 0.6, 16, order)
+    a, _ = fmm(p.x, p.y, p.z, p.m, 0.03, 0.6, 16, order)
+    assert rel_err(a, ref).max() <= 1e-12
+
+
+@need_ref
+@pytest.mark.parametrize("n,cap", [(5000, 16), (30000, 64), (700, 1)])
+def test_moments_bit_identical(n, cap):
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 3 * n + cap, 0.02)
+    ref, _ = oracle.ref_fmm_moments(p.x, p.y, p.z, p.m, 1.0, 0.02, 0.6, cap)
+    xs = [np.ascontiguousarray(v) for v in (p.x, p.y, p.z, p.m)]
+    nn = gx._ffi.ctypes.c_int64()
+    opt = gx.FmmOptions(0.6, cap).ffi()
+    gx._ffi.call("gx_fmm_moments", n, *(gx._ffi.ptr(v) for v in xs), gx.PhysicsParams(1.0, 0.02).ffi(), opt, 0, None,
+                 gx._ffi.ctypes.byref(nn))
+    got = np.zeros((nn.value, 35))
+    gx._ffi.call("gx_fmm_moments", n, *(gx._ffi.ptr(v) for v in xs), gx.PhysicsParams(1.0, 0.02).ffi(), opt, nn.value,
+                 gx._ffi.ptr(got), gx._ffi.ctypes.byref(nn))
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref)
+
+
+def test_target_range_writes_only_the_range():
+    p = gx.ics.two_disk_encounter(3000, 2000, 11, 0.02)
+    full, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
+    a = [np.full(len(p), 7.0) for _ in range(3)]
+    gx.fmm.fmm_accelerations(p.x, p.y, p.z, p.m, *a, gx.PhysicsParams(1.0, 0.02), gx.FmmOptions(0.6, 16), F64, 1234,
+                             3210)
+    a = np.stack(a, 1)
+    assert np.array_equal(a[1234:3210], full[1234:3210])
+    assert np.all(a[:1234] == 7.0) and np.all(a[3210:] == 7.0)
+    # end beyond n clamps (compute_targets, fmm_solver.cpp:29); an empty range writes nothing
+    b, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 16, begin=4000, end=10 ** 9)
+    assert np.array_equal(b[4000:], full[4000:]) and not b[:4000].any()
+    c = [np.full(len(p), 7.0) for _ in range(3)]
+    gx.fmm.fmm_accelerations(p.x, p.y, p.z, p.m, *c, gx.PhysicsParams(1.0, 0.02), gx.FmmOptions(0.6, 16), F64, 10, 10)
+    assert all(np.all(v == 7.0) for v in c)
+
+
+def test_device_arrays_match_host_arrays():
+    p = gx.ics.two_disk_encounter(6000, 2000, 12, 0.02)
+    host, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 32)
+    T = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("x", "y", "z", "m")}
+    A = [torch.zeros(len(p), dtype=torch.float64, device="cuda") for _ in range(3)]
+    gx.fmm.fmm_accelerations(T["x"], T["y"], T["z"], T["m"], *A, gx.PhysicsParams(1.0, 0.02), gx.FmmOptions(0.6, 32))
+    torch.cuda.synchronize()
+    assert np.array_equal(torch.stack(A, 1).cpu().numpy(), host)
+
+
+@need_ref
+def test_massless_bodies_and_zero_softening():
+    p = gx.ics.two_disk_encounter(1000, 1000, 13, 0.02)
+    p.m[::7] = 0.0
+    p.m[1500:] = 0.0  # the second disk is test particles: its leaves are skipped by the reference
+    p.x[3], p.y[3], p.z[3] = p.x[4], p.y[4], p.z[4]
+    ref = oracle.ref_fmm(p.x, p.y, p.z, p.m, 1.0, 0.0, 0.6, 16)
+    a, _ = fmm(p.x, p.y, p.z, p.m, 0.0, 0.6, 16)
+    assert np.all(np.isfinite(a))
+    assert np.array_equal(a == 0.0, ref == 0.0)
+    nz = np.any(ref != 0.0, axis=1)
+    assert rel_err(a[nz], ref[nz]).max() <= 1e-12
+
+
+def test_single_body_and_all_massless():
+    a, st = fmm(np.array([0.5]), np.array([0.1]), np.array([-0.2]), np.array([2.0]), 0.01, 0.6, 16)
+    assert not a.any() and st.leaf_count == 1
+    z = np.zeros(50)
+    b, st = fmm(np.linspace(0, 1, 50), z, z, z, 0.01, 0.6, 4)
+    assert not b.any() and st.leaf_count == 0
+
+
+def test_smoke80_solver_agreement(golden):
+    """The reference smoke test's agreement case (smoke_tests.cpp:83-123): FMM vs direct
+    mean relative error below the reference's bound of 1e-2 at theta 0.6, leaf 16."""
+    g = golden("smoke80.npz")
+    a, _ = fmm(g["x"], g["y"], g["z"], g["m"], 0.03, 0.6, 16)
+    d = oracle.direct_targets(g["x"], g["y"], g["z"], g["m"], 1.0, 0.03)
+    assert np.mean(rel_err(a, d)) < 1e-2
+
+
+@pytest.mark.parametrize("prec", [MIX, EXACT])
+def test_near_field_precisions(prec):
+    p = gx.ics.two_disk_encounter(4000, 4000, 14, 0.02)
+    f64, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 32)
+    a, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 32, prec=prec)
+    e = rel_err(a, f64)
+    if prec == MIX:
+        assert np.median(e) <= 1e-6
+    else:
+        assert e.max() <= 1e-12
+
+
+@need_ref
+def test_fmm_trajectory_matches_reference():
+    """20 KDK steps with the GPU FMM as the force (leapfrog_step, integrator.cpp:33-42)
+    against the reference's own FMM trajectory."""
+    p = gx.ics.two_disk_encounter(1000, 1000, 15, 0.025)
+    st = dict(x=p.x.copy(), y=p.y.copy(), z=p.z.copy(), vx=p.vx.copy(), vy=p.vy.copy(), vz=p.vz.copy())
+    a0, _ = fmm(p.x, p.y, p.z, p.m, 0.025, 0.6, 16)
+    st.update(ax=a0[:, 0].copy(), ay=a0[:, 1].copy(), az=a0[:, 2].copy())
+    ref = oracle.ref_leapfrog_fmm({k: v.copy() for k, v in st.items()}, p.m, 1.0, 0.025, 0.01, 20, 0.6, 16)
+    for _ in range(20):
+        st["vx"] = st["vx"] + st["ax"] * 0.005
+        st["vy"] = st["vy"] + st["ay"] * 0.005
+        st["vz"] = st["vz"] + st["az"] * 0.005
+        st["x"] = st["x"] + st["vx"] * 0.01
+        st["y"] = st["y"] + st["vy"] * 0.01
+        st["z"] = st["z"] + st["vz"] * 0.01
+        a, _ = fmm(st["x"], st["y"], st["z"], p.m, 0.025, 0.6, 16)
+        st["ax"], st["ay"], st["az"] = a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy()
+        st["vx"] = st["vx"] + st["ax"] * 0.005
+        st["vy"] = st["vy"] + st["ay"] * 0.005
+        st["vz"] = st["vz"] + st["az"] * 0.005
+    assert max(np.abs(st[k] - ref[k]).max() for k in ("x", "y", "z")) <= 1e-10
+
+
+def test_fixture_trajectory_20_steps(golden):
+    """fmm_1000_r1 (dt 0.01, 20 steps) from the reference's own step-0 state: the GPU FMM as
+    the force of the reference's KDK reproduces its step-20 snapshot."""
+    g = golden("fmm1000.npz")
+    eps, theta, cap, dt = float(g["softening"]), float(g["theta"]), int(g["leaf_capacity"]), float(g["dt"])
+    s = {k: g[k].copy() for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+    for _ in range(int(g["steps"])):
+        for v, a in (("vx", "ax"), ("vy", "ay"), ("vz", "az")):
+            s[v] = s[v] + s[a] * (0.5 * dt)
+        for x, v in (("x", "vx"), ("y", "vy"), ("z", "vz")):
+            s[x] = s[x] + s[v] * dt
+        a, _ = fmm(s["x"], s["y"], s["z"], g["m"], eps, theta, cap)
+        s["ax"], s["ay"], s["az"] = a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy()
+        for v, a in (("vx", "ax"), ("vy", "ay"), ("vz", "az")):
+            s[v] = s[v] + s[a] * (0.5 * dt)
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.abs(s[k] - g[k + "20"]).max() <= 1e-10, k
