@@ -119,6 +119,7 @@ _SIGNATURES = {
                      S],
     "gx_fmm_moments": [I64, P, P, P, P, Physics, FmmOptionsStruct, I64, P, POINTER(I64)],
     "gx_leaf_lists_build": [I64, P, P, P, P, D, D, I64, c_int, PP],
+    "gx_leaf_lists_build_device": [I64, P, P, P, P, D, D, I64, c_int, S, PP, POINTER(c_int)],
     "gx_leaf_lists_info": [P, POINTER(c_int32), POINTER(I64), POINTER(I64), POINTER(I64), POINTER(I64)],
     "gx_leaf_lists_export": [P, P, P, P, P],
     "gx_leaf_lists_free": [P],

@@ -7,6 +7,7 @@
 
 #include "batch.cuh"
 #include "fmm.cuh"
+#include "fmm_build.cuh"
 #include "fmm_tree.hpp"
 #include "force.cuh"
 #include "integrate.cuh"
@@ -24,6 +25,7 @@
 #include <initializer_list>
 #include <limits>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -1305,58 +1307,84 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
 }
 
 // ======================================================================================
-// FMM: reference octree and lists on the host, moments, far field and near field on the
-// device
+// FMM: the reference octree, its moments, far field and near field
 // ======================================================================================
-extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
-                            gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
-                            double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream) {
-    GX_GUARD_BEGIN
-    const char* fn = "gx_fmm_accel";
-    if (stats) *stats = gx_fmm_stats{0, 0, 0, 0};
-    if (n < 0 || begin < 0 || end < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: negative size or range", fn);
-    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
-    GX_TRY(check_phys(phys, fn));
-    if (!(opt.theta == opt.theta)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: theta is NaN", fn);
-    end = std::min(end, n);  // compute_targets (fmm_solver.cpp:24-33)
-    if (n == 0 || begin >= end) return GX_OK;
-    if (!x || !y || !z || !m || !ax || !ay || !az) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
-    GX_TRY(require_device());
-    bool device;
-    int dev;
-    GX_TRY(classify({x, y, z, m, ax, ay, az}, &device, &dev, fn));
-    DeviceGuard g(dev);
-    cudaStream_t st = (cudaStream_t)stream;
+namespace {
 
-    // The octree is built on the host from host copies of the positions and masses.
-    std::vector<double> hbuf;
-    const double *hx = x, *hy = y, *hz = z, *hm = m;
-    if (device) {
-        hbuf.resize((size_t)n * 4);
-        const double* src[4] = {x, y, z, m};
-        for (int k = 0; k < 4; ++k)
-            GX_CUDA(cudaMemcpyAsync(hbuf.data() + (size_t)k * n, src[k], (size_t)n * sizeof(double),
-                                    cudaMemcpyDeviceToHost, st));
-        GX_CUDA(cudaStreamSynchronize(st));
-        hx = hbuf.data();
-        hy = hx + n;
-        hz = hy + n;
-        hm = hz + n;
-    }
+// Device arrays and sizes of one FMM evaluation's tree, built on the device or the host.
+struct FmmPlan {
+    HostStage hs;
+    explicit FmmPlan(cudaStream_t s) : hs(s) {}
+    bool on_device = false;
+    int32_t n_nodes = 0, n_leaves = 0;
+    std::vector<int32_t> level_off;
+    int64_t n_far = 0, n_near = 0, n_slots = 0;
+    FmmArgs fa{};
+    const int32_t* near_off = nullptr;
+    const int32_t* near_leaf = nullptr;
+};
+
+template <typename T>
+int dev_array(HostStage& hs, int64_t count, T** p) {
+    hs.bufs.emplace_back();
+    GX_TRY(hs.bufs.back().alloc((size_t)std::max<int64_t>(count, 1) * sizeof(T), hs.st));
+    *p = (T*)hs.bufs.back().p;
+    return GX_OK;
+}
+
+template <typename T>
+int dev_copy(HostStage& hs, const std::vector<T>& v, const T** p) {
+    T* d;
+    GX_TRY(hs.in_any(v.data(), (int64_t)v.size(), &d));
+    *p = d;
+    return GX_OK;
+}
+
+void fmm_common_args(FmmArgs& fa, const double* dx, const double* dy, const double* dz, const double* dm,
+                     gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end) {
+    fa.x = dx;
+    fa.y = dy;
+    fa.z = dz;
+    fa.m = dm;
+    fa.t_begin = begin;
+    fa.t_end = end;
+    fa.G = phys.G;
+    fa.eps2 = phys.softening * phys.softening;
+    fa.order = fmm_effective_order(std::min(4, std::max(0, opt.expansion_order)));
+}
+
+// Host builder: the octree and lists on the host, moments on the device.
+int fmm_plan_host(FmmPlan& P, int64_t n, const double* hx, const double* hy, const double* hz, const double* hm,
+                  const double* dx, const double* dy, const double* dz, const double* dm, gx_physics phys,
+                  gx_fmm_options opt, int64_t begin, int64_t end) {
+    HostStage& hs = P.hs;
     FmmTree T;
     GX_TRY(build_fmm_tree(n, hx, hy, hz, hm, phys.softening, opt.theta, opt.leaf_capacity, opt.max_depth, true, &T));
-    const int32_t nl = T.n_leaves(), nn = T.n_nodes();
-    if (stats) {
-        stats->node_count = T.all_nodes;
-        stats->leaf_count = nl;
-        stats->far_interactions = T.n_far;
-        stats->near_interactions = (int64_t)T.near_leaf.size();
-    }
-
+    FmmArgs& fa = P.fa;
+    fmm_common_args(fa, dx, dy, dz, dm, phys, opt, begin, end);
+    P.n_nodes = fa.n_nodes = T.n_nodes();
+    P.n_leaves = fa.n_leaves = T.n_leaves();
+    P.level_off = T.level_off;
+    P.n_far = T.n_far;
+    P.n_near = (int64_t)T.near_leaf.size();
+    GX_TRY(dev_copy(hs, T.node_beg, &fa.node_beg));
+    GX_TRY(dev_copy(hs, T.node_end, &fa.node_end));
+    GX_TRY(dev_copy(hs, T.node_child, &fa.node_child));
+    GX_TRY(dev_copy(hs, T.node_cx, &fa.node_cx));
+    GX_TRY(dev_copy(hs, T.node_cy, &fa.node_cy));
+    GX_TRY(dev_copy(hs, T.node_cz, &fa.node_cz));
+    GX_TRY(dev_copy(hs, T.perm, &fa.perm));
+    GX_TRY(dev_copy(hs, T.leaf_off, &fa.leaf_off));
+    GX_TRY(dev_copy(hs, T.leaf_part, &fa.leaf_part));
+    GX_TRY(dev_copy(hs, T.far_node, &fa.far_node));
+    GX_TRY(dev_copy(hs, T.near_off, &P.near_off));
+    GX_TRY(dev_copy(hs, T.near_leaf, &P.near_leaf));
+    GX_TRY(dev_array(hs, (int64_t)P.n_nodes * kFmmRec, &fa.rec));
+    GX_CUDA(launch_fmm_moments(fa, P.level_off.data(), T.n_levels(), hs.st));
     // far-field work items for the leaves that hold a target in [begin, end)
     std::vector<M2PItem> items;
     int64_t slots = 0;
-    for (int32_t l = 0; l < nl; ++l) {
+    for (int32_t l = 0; l < P.n_leaves; ++l) {
         const int32_t fb = T.far_off[l], fe = T.far_off[l + 1];
         if (fe == fb) continue;
         bool any = false;
@@ -1379,7 +1407,201 @@ extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const d
         }
     }
     if (items.size() > (size_t)std::numeric_limits<int32_t>::max())
-        return fail(GX_ERR_INVALID_ARGUMENT, "%s: too many far-field work items", fn);
+        return fail(GX_ERR_UNSUPPORTED, "FMM: too many far-field work items");
+    fa.n_items = (int32_t)items.size();
+    P.n_slots = slots;
+    if (!items.empty()) GX_TRY(dev_copy(hs, items, &fa.items));
+    return GX_OK;
+}
+
+// Device builder; *deep is set (and nothing else is valid) when the tree needs a split
+// below the key depth, which the host builder handles.
+int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, const double* dz, const double* dm,
+                    gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end, bool* deep) {
+    HostStage& hs = P.hs;
+    cudaStream_t st = hs.st;
+    *deep = false;
+    P.on_device = true;
+    const int64_t cap = std::max<int64_t>(1, opt.leaf_capacity);
+    TreeBuildArgs t{};
+    t.n = (int32_t)n;
+    t.x = dx;
+    t.y = dy;
+    t.z = dz;
+    t.softening = phys.softening;
+    t.cap = cap;
+    t.max_depth = std::max(1, opt.max_depth);
+    GX_TRY(dev_array(hs, 6 * kBboxBlocks, &t.part));
+    GX_TRY(dev_array(hs, 4, &t.root));
+    GX_TRY(dev_array(hs, n, &t.keys));
+    GX_TRY(dev_array(hs, n, &t.keys_alt));
+    GX_TRY(dev_array(hs, n, &t.idx));
+    GX_TRY(dev_array(hs, n, &t.perm));
+    GX_TRY(dev_array(hs, kKeyLevels + 3, &t.level_off));
+    GX_TRY(dev_array(hs, 3, &t.hdr));
+    const size_t sort_bytes = tree_build_temp_bytes(t.n);
+    void* sort_temp;
+    GX_TRY(dev_array(hs, (int64_t)sort_bytes, (char**)&sort_temp));
+    // node slots: 1 + 8 per split node; at most n / (cap + 1) nodes split per level
+    const int64_t per_level = n / (cap + 1) + 1;
+    int32_t hdr[3] = {0, 0, 0};
+    std::vector<int32_t> loff(kKeyLevels + 3);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        const int64_t splits = attempt == 0 ? std::min<int64_t>(3 * per_level + 64, kKeyLevels * per_level)
+                                            : kKeyLevels * per_level;
+        const int64_t capacity = 1 + 8 * splits;
+        if (capacity > std::numeric_limits<int32_t>::max()) return fail(GX_ERR_UNSUPPORTED, "FMM: tree too large");
+        t.capacity = (int32_t)capacity;
+        GX_TRY(dev_array(hs, capacity, &t.beg));
+        GX_TRY(dev_array(hs, capacity, &t.end));
+        GX_TRY(dev_array(hs, capacity, &t.child));
+        GX_TRY(dev_array(hs, capacity, &t.cx));
+        GX_TRY(dev_array(hs, capacity, &t.cy));
+        GX_TRY(dev_array(hs, capacity, &t.cz));
+        GX_TRY(dev_array(hs, capacity, &t.hw));
+        GX_CUDA(launch_tree_build(t, sort_temp, sort_bytes, st));
+        GX_CUDA(cudaMemcpyAsync(hdr, t.hdr, sizeof(hdr), cudaMemcpyDeviceToHost, st));
+        GX_CUDA(cudaMemcpyAsync(loff.data(), t.level_off, loff.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        GX_CUDA(cudaStreamSynchronize(st));
+        if (hdr[2] & 1) {
+            *deep = true;
+            return GX_OK;
+        }
+        if (!(hdr[2] & 2)) break;
+        if (attempt == 1) return fail(GX_ERR_UNSUPPORTED, "FMM: node slots exhausted");
+    }
+    GX_CUDA(launch_tree_leaf_order(t, hdr[0], sort_temp, sort_bytes, st));
+    FmmArgs& fa = P.fa;
+    fmm_common_args(fa, dx, dy, dz, dm, phys, opt, begin, end);
+    P.n_nodes = fa.n_nodes = hdr[0];
+    P.level_off.assign(loff.begin(), loff.begin() + hdr[1] + 1);
+    fa.node_beg = t.beg;
+    fa.node_end = t.end;
+    fa.node_child = t.child;
+    fa.node_cx = t.cx;
+    fa.node_cy = t.cy;
+    fa.node_cz = t.cz;
+    fa.perm = t.perm;
+    GX_TRY(dev_array(hs, (int64_t)P.n_nodes * kFmmRec, &fa.rec));
+    GX_CUDA(launch_fmm_moments(fa, P.level_off.data(), hdr[1], st));
+
+    TreeListArgs la{};
+    la.n = t.n;
+    la.n_nodes = P.n_nodes;
+    la.beg = t.beg;
+    la.end = t.end;
+    la.child = t.child;
+    la.perm = t.perm;
+    la.cx = t.cx;
+    la.cy = t.cy;
+    la.cz = t.cz;
+    la.hw = t.hw;
+    la.rec = fa.rec;
+    la.theta = std::max(1.0e-6, opt.theta);  // FastMultipoleSolver constructor (fmm_solver.cpp:16)
+    la.t_begin = begin;
+    la.t_end = end;
+    const int64_t nb = n + 1, lb = (int64_t)P.n_nodes + 1;
+    GX_TRY(dev_array(hs, nb, &la.start_flag));
+    GX_TRY(dev_array(hs, nb, &la.start_ord));
+    GX_TRY(dev_array(hs, nb, &la.keep));
+    GX_TRY(dev_array(hs, nb, &la.newpos));
+    GX_TRY(dev_array(hs, lb, &la.leaf_off));
+    GX_TRY(dev_array(hs, n, &la.leaf_part));
+    GX_TRY(dev_array(hs, lb, &la.leaf_node));
+    GX_TRY(dev_array(hs, lb, &la.node_leaf));
+    for (int32_t** p : {&la.far_cnt, &la.near_cnt, &la.item_cnt, &la.slot_cnt, &la.far_off, &la.near_off, &la.item_off,
+                        &la.slot_off})
+        GX_TRY(dev_array(hs, lb, p));
+    GX_TRY(dev_array(hs, 4, &la.totals));
+    const size_t list_bytes = tree_list_temp_bytes(la.n, la.n_nodes);
+    void* list_temp;
+    GX_TRY(dev_array(hs, (int64_t)list_bytes, (char**)&list_temp));
+    GX_CUDA(launch_tree_lists_count(la, list_temp, list_bytes, st));
+    int32_t nl = 0;
+    unsigned long long tot[4];
+    GX_CUDA(cudaMemcpyAsync(&nl, la.start_ord + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaMemcpyAsync(tot, la.totals, sizeof(tot), cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    for (unsigned long long v : tot)
+        if (v > (unsigned long long)std::numeric_limits<int32_t>::max())
+            return fail(GX_ERR_UNSUPPORTED, "FMM: interaction lists exceed the int32 range");
+    P.n_leaves = fa.n_leaves = nl;
+    P.n_far = (int64_t)tot[0];
+    P.n_near = (int64_t)tot[1];
+    fa.n_items = (int32_t)tot[2];
+    P.n_slots = (int64_t)tot[3];
+    GX_TRY(dev_array(hs, P.n_far, &la.far_node));
+    GX_TRY(dev_array(hs, P.n_near, &la.near_leaf));
+    M2PItem* items;
+    GX_TRY(dev_array(hs, fa.n_items, &items));
+    la.items = items;
+    GX_CUDA(launch_tree_lists_fill(la, nl, st));
+    fa.leaf_off = la.leaf_off;
+    fa.leaf_part = la.leaf_part;
+    fa.far_node = la.far_node;
+    fa.items = items;
+    P.near_off = la.near_off;
+    P.near_leaf = la.near_leaf;
+    return GX_OK;
+}
+
+// Either builder for device-resident inputs; host copies of the inputs (hx..hm, may be
+// null) spare a download when the host builder has to take over.
+int fmm_plan(std::unique_ptr<FmmPlan>& P, cudaStream_t st, int64_t n, const double* hx, const double* hy,
+             const double* hz, const double* hm, const double* dx, const double* dy, const double* dz, const double* dm,
+             gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end) {
+    P.reset(new FmmPlan(st));
+    bool deep = false;
+    GX_TRY(fmm_plan_device(*P, n, dx, dy, dz, dm, phys, opt, begin, end, &deep));
+    if (!deep) return GX_OK;
+    std::vector<double> hbuf;
+    if (!hx) {
+        hbuf.resize((size_t)n * 4);
+        const double* src[4] = {dx, dy, dz, dm};
+        for (int k = 0; k < 4; ++k)
+            GX_CUDA(cudaMemcpyAsync(hbuf.data() + (size_t)k * n, src[k], (size_t)n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, st));
+        GX_CUDA(cudaStreamSynchronize(st));
+        hx = hbuf.data();
+        hy = hx + n;
+        hz = hy + n;
+        hm = hz + n;
+    }
+    P.reset(new FmmPlan(st));
+    return fmm_plan_host(*P, n, hx, hy, hz, hm, dx, dy, dz, dm, phys, opt, begin, end);
+}
+
+int check_fmm_inputs(int64_t n, const double* m, bool device, const char* fn) {
+    if (n > (int64_t)std::numeric_limits<int32_t>::max() / 2)
+        return fail(GX_ERR_UNSUPPORTED, "%s: n exceeds the int32 index range", fn);
+    if (!device)
+        for (int64_t i = 0; i < n; ++i)
+            if (m[i] < 0.0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: masses must be >= 0", fn);
+    return GX_OK;
+}
+
+}  // namespace
+
+extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                            gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
+                            double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_fmm_accel";
+    if (stats) *stats = gx_fmm_stats{0, 0, 0, 0};
+    if (n < 0 || begin < 0 || end < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: negative size or range", fn);
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
+    GX_TRY(check_phys(phys, fn));
+    if (!(opt.theta == opt.theta)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: theta is NaN", fn);
+    end = std::min(end, n);  // compute_targets (fmm_solver.cpp:24-33)
+    if (n == 0 || begin >= end) return GX_OK;
+    if (!x || !y || !z || !m || !ax || !ay || !az) return fail(GX_ERR_INVALID_ARGUMENT, "%s: null array", fn);
+    GX_TRY(require_device());
+    bool device;
+    int dev;
+    GX_TRY(classify({x, y, z, m, ax, ay, az}, &device, &dev, fn));
+    GX_TRY(check_fmm_inputs(n, m, device, fn));
+    DeviceGuard g(dev);
+    cudaStream_t st = (cudaStream_t)stream;
 
     HostStage hs(st);
     const double *dx = x, *dy = y, *dz = z, *dm = m;
@@ -1395,59 +1617,43 @@ extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const d
         GX_TRY(hs.out(&day, n));
         GX_TRY(hs.out(&daz, n));
     }
+    std::unique_ptr<FmmPlan> P;
+    GX_TRY(fmm_plan(P, st, n, device ? nullptr : x, device ? nullptr : y, device ? nullptr : z, device ? nullptr : m,
+                    dx, dy, dz, dm, phys, opt, begin, end));
+    if (stats) {
+        // node_count counts every node the reference creates, massless ones included
+        stats->node_count = P->n_nodes;
+        stats->leaf_count = P->n_leaves;
+        stats->far_interactions = P->n_far;
+        stats->near_interactions = P->n_near;
+    }
     // reset_accelerations over the target range (fmm_solver.cpp:31); the far and near
     // fields are then added
     for (double* p : {dax, day, daz}) GX_CUDA(cudaMemsetAsync(p + begin, 0, (size_t)(end - begin) * sizeof(double), st));
-
-    if (nl > 0) {
-        int32_t *d_lo, *d_lp, *d_ln, *d_nc, *d_nnc, *d_fn, *d_lv, *d_no, *d_nlf;
-        GX_TRY(hs.in_any(T.leaf_off.data(), (int64_t)T.leaf_off.size(), &d_lo));
-        GX_TRY(hs.in_any(T.leaf_part.data(), (int64_t)T.leaf_part.size(), &d_lp));
-        GX_TRY(hs.in_any(T.leaf_node.data(), (int64_t)T.leaf_node.size(), &d_ln));
-        GX_TRY(hs.in_any(T.node_child.data(), (int64_t)nn, &d_nc));
-        GX_TRY(hs.in_any(T.node_nchild.data(), (int64_t)nn, &d_nnc));
-        GX_TRY(hs.in_any(T.far_node.data(), (int64_t)T.far_node.size(), &d_fn));
-        GX_TRY(hs.in_any(T.level_node.data(), (int64_t)T.level_node.size(), &d_lv));
-        GX_TRY(hs.in_any(T.near_off.data(), (int64_t)T.near_off.size(), &d_no));
-        GX_TRY(hs.in_any(T.near_leaf.data(), (int64_t)T.near_leaf.size(), &d_nlf));
-        M2PItem* d_items = nullptr;
-        if (!items.empty()) GX_TRY(hs.in_any(items.data(), (int64_t)items.size(), &d_items));
-        AsyncBuf rec, part, done, p2p_scratch;
-        GX_TRY(rec.alloc((size_t)nn * kFmmRec * sizeof(double), st));
-        GX_TRY(part.alloc((size_t)std::max<int64_t>(slots, 1) * 3 * sizeof(double), st));
-        GX_TRY(done.alloc((size_t)nl * sizeof(int), st));
-        GX_CUDA(cudaMemsetAsync(done.p, 0, (size_t)nl * sizeof(int), st));
-
-        FmmArgs fa;
-        fa.x = dx; fa.y = dy; fa.z = dz; fa.m = dm;
-        fa.leaf_off = d_lo; fa.leaf_part = d_lp; fa.leaf_node = d_ln;
-        fa.node_child = d_nc; fa.node_nchild = d_nnc; fa.far_node = d_fn;
-        fa.n_leaves = nl;
-        fa.rec = rec.d();
-        fa.items = d_items;
-        fa.n_items = (int32_t)items.size();
+    if (P->n_leaves > 0) {
+        FmmArgs& fa = P->fa;
+        fa.ax = dax;
+        fa.ay = day;
+        fa.az = daz;
+        AsyncBuf part, done, p2p_scratch;
+        GX_TRY(part.alloc((size_t)std::max<int64_t>(P->n_slots, 1) * 3 * sizeof(double), st));
+        GX_TRY(done.alloc((size_t)P->n_leaves * sizeof(int), st));
+        GX_CUDA(cudaMemsetAsync(done.p, 0, (size_t)P->n_leaves * sizeof(int), st));
         fa.scratch = part.d();
         fa.done = (int*)done.p;
-        fa.ax = dax; fa.ay = day; fa.az = daz;
-        fa.t_begin = begin;
-        fa.t_end = end;
-        fa.G = phys.G;
-        fa.eps2 = phys.softening * phys.softening;
-        fa.order = fmm_effective_order(std::min(4, std::max(0, opt.expansion_order)));
-        GX_CUDA(launch_fmm_moments(fa, T.level_off.data(), (int)T.level_off.size() - 1, d_lv, st));
         GX_CUDA(launch_fmm_m2p(fa, st));
 
         P2PArgs pa;
         pa.x = dx; pa.y = dy; pa.z = dz; pa.m = dm;
-        pa.leaf_off = d_lo; pa.leaf_part = d_lp; pa.near_off = d_no; pa.near_leaf = d_nlf;
-        pa.n_leaves = nl;
+        pa.leaf_off = fa.leaf_off; pa.leaf_part = fa.leaf_part; pa.near_off = P->near_off; pa.near_leaf = P->near_leaf;
+        pa.n_leaves = P->n_leaves;
         pa.ax = dax; pa.ay = day; pa.az = daz;
         pa.t_begin = begin;
         pa.t_end = end;
         pa.G = phys.G;
         pa.eps2 = phys.softening * phys.softening;
         pa.eps2f = (float)pa.eps2;
-        GX_TRY(p2p_scratch.alloc(p2p_scratch_bytes(n, nl), st));
+        GX_TRY(p2p_scratch.alloc(p2p_scratch_bytes(n, P->n_leaves), st));
         GX_CUDA(launch_p2p(pa, n, precision, p2p_scratch.p, sm_count(dev), st));
     }
     if (!device) {
@@ -1476,14 +1682,8 @@ extern "C" int gx_fmm_moments(int64_t n, const double* x, const double* y, const
     GX_TRY(require_device());
     GX_TRY(classify({x, y, z, m, records}, &device, &dev, fn));
     if (device) return fail(GX_ERR_INVALID_ARGUMENT, "%s: host arrays only", fn);
+    GX_TRY(check_fmm_inputs(n, m, false, fn));
     DeviceGuard g(dev);
-    FmmTree T;
-    GX_TRY(build_fmm_tree(n, x, y, z, m, phys.softening, opt.theta, opt.leaf_capacity, opt.max_depth, false, &T));
-    const int32_t nn = T.n_nodes(), nl = T.n_leaves();
-    *n_nodes = nn;
-    if (!records || nn == 0) return GX_OK;
-    if (capacity < nn) return fail(GX_ERR_INVALID_ARGUMENT, "%s: records hold %lld nodes, the tree has %d", fn,
-                                   (long long)capacity, nn);
     cudaStream_t st = nullptr;
     HostStage hs(st);
     double *dx, *dy, *dz, *dm;
@@ -1491,26 +1691,76 @@ extern "C" int gx_fmm_moments(int64_t n, const double* x, const double* y, const
     GX_TRY(hs.in(y, n, &dy));
     GX_TRY(hs.in(z, n, &dz));
     GX_TRY(hs.in(m, n, &dm));
-    int32_t *d_lo, *d_lp, *d_ln, *d_nc, *d_nnc, *d_lv;
-    GX_TRY(hs.in_any(T.leaf_off.data(), (int64_t)T.leaf_off.size(), &d_lo));
-    GX_TRY(hs.in_any(T.leaf_part.data(), (int64_t)T.leaf_part.size(), &d_lp));
-    GX_TRY(hs.in_any(T.leaf_node.data(), (int64_t)T.leaf_node.size(), &d_ln));
-    GX_TRY(hs.in_any(T.node_child.data(), (int64_t)nn, &d_nc));
-    GX_TRY(hs.in_any(T.node_nchild.data(), (int64_t)nn, &d_nnc));
-    GX_TRY(hs.in_any(T.level_node.data(), (int64_t)T.level_node.size(), &d_lv));
-    AsyncBuf rec;
-    GX_TRY(rec.alloc((size_t)nn * kFmmRec * sizeof(double), st));
-    FmmArgs fa{};
-    fa.x = dx; fa.y = dy; fa.z = dz; fa.m = dm;
-    fa.leaf_off = d_lo; fa.leaf_part = d_lp; fa.leaf_node = d_ln;
-    fa.node_child = d_nc; fa.node_nchild = d_nnc;
-    fa.n_leaves = nl;
-    fa.rec = rec.d();
-    GX_CUDA(launch_fmm_moments(fa, T.level_off.data(), (int)T.level_off.size() - 1, d_lv, st));
+    std::unique_ptr<FmmPlan> P;
+    GX_TRY(fmm_plan(P, st, n, x, y, z, m, dx, dy, dz, dm, phys, opt, 0, n));
+    const int32_t nn = P->n_nodes;
     std::vector<double> h((size_t)nn * kFmmRec);
-    GX_CUDA(cudaMemcpyAsync(h.data(), rec.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    std::vector<int32_t> child((size_t)nn);
+    GX_CUDA(cudaMemcpyAsync(h.data(), P->fa.rec, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaMemcpyAsync(child.data(), P->fa.node_child, child.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GX_CUDA(cudaStreamSynchronize(st));
-    for (int32_t k = 0; k < nn; ++k) std::copy(&h[(size_t)k * kFmmRec], &h[(size_t)k * kFmmRec] + 35, records + (size_t)k * 35);
+    // nodes with mass > 0, breadth-first from the root, children in octant order
+    std::vector<int32_t> bfs;
+    if (nn > 0 && h[kRecMass] > 0.0) bfs.push_back(0);
+    for (size_t k = 0; k < bfs.size(); ++k) {
+        const int32_t c0 = child[bfs[k]];
+        if (c0 < 0) continue;
+        for (int c = 0; c < 8; ++c)
+            if (h[(size_t)(c0 + c) * kFmmRec + kRecMass] > 0.0) bfs.push_back(c0 + c);
+    }
+    *n_nodes = (int64_t)bfs.size();
+    if (!records) return GX_OK;
+    if (capacity < (int64_t)bfs.size())
+        return fail(GX_ERR_INVALID_ARGUMENT, "%s: records hold %lld nodes, the tree has %zu", fn, (long long)capacity,
+                    bfs.size());
+    for (size_t k = 0; k < bfs.size(); ++k)
+        std::copy(&h[(size_t)bfs[k] * kFmmRec], &h[(size_t)bfs[k] * kFmmRec] + 35, records + k * 35);
+    return GX_OK;
+    GX_GUARD_END
+}
+
+extern "C" int gxi_leaf_lists_from_device(int64_t n, const double* x, const double* y, const double* z,
+                                          const double* m, double softening, double theta, int64_t leaf_capacity,
+                                          int max_depth, void* stream, gx::FmmTree* T, int* on_device) {
+    GX_GUARD_BEGIN
+    const char* fn = "gx_leaf_lists_build_device";
+    GX_TRY(require_device());
+    GX_TRY(check_fmm_inputs(n, m, false, fn));
+    cudaStream_t st = (cudaStream_t)stream;
+    HostStage hs(st);
+    double *dx, *dy, *dz, *dm;
+    GX_TRY(hs.in(x, n, &dx));
+    GX_TRY(hs.in(y, n, &dy));
+    GX_TRY(hs.in(z, n, &dz));
+    GX_TRY(hs.in(m, n, &dm));
+    gx_physics phys{1.0, softening};
+    gx_fmm_options opt{theta, leaf_capacity, max_depth, 4};
+    std::unique_ptr<FmmPlan> P;
+    GX_TRY(fmm_plan(P, st, n, x, y, z, m, dx, dy, dz, dm, phys, opt, 0, n));
+    *on_device = P->on_device ? 1 : 0;
+    const int32_t nl = P->n_leaves;
+    T->leaf_off.resize((size_t)nl + 1);
+    T->near_off.resize((size_t)nl + 1);
+    GX_CUDA(cudaMemcpyAsync(T->leaf_off.data(), P->fa.leaf_off, T->leaf_off.size() * sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaMemcpyAsync(T->near_off.data(), P->near_off, T->near_off.size() * sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    T->leaf_part.resize((size_t)T->leaf_off[nl]);
+    T->near_leaf.resize((size_t)P->n_near);
+    if (!T->leaf_part.empty())
+        GX_CUDA(cudaMemcpyAsync(T->leaf_part.data(), P->fa.leaf_part, T->leaf_part.size() * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, st));
+    if (!T->near_leaf.empty())
+        GX_CUDA(cudaMemcpyAsync(T->near_leaf.data(), P->near_leaf, T->near_leaf.size() * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    T->n_far = P->n_far;
+    T->n_pairs = 0;
+    for (int32_t l = 0; l < nl; ++l)
+        for (int32_t k = T->near_off[l]; k < T->near_off[l + 1]; ++k)
+            T->n_pairs += (int64_t)(T->leaf_off[l + 1] - T->leaf_off[l]) *
+                          (T->leaf_off[T->near_leaf[k] + 1] - T->leaf_off[T->near_leaf[k]]);
     return GX_OK;
     GX_GUARD_END
 }

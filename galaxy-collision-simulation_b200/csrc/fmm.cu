@@ -5,8 +5,9 @@
 // (cpp/fmm/fmm_solver.cpp:157-208) with add_multipole_point / add_multipole_shifted_child
 // (cpp/fmm/multipole.cpp:218-252) are restated with the reference's operations in the
 // reference's order and no contraction (dadd/dmul), so masses, centres of mass and the 31
-// moments of every node are bit-identical to the reference's.  One warp per node; lane k
-// owns moment 4 + k.  Leaves first, then one launch per tree level, deepest first.
+// moments of every node are bit-identical to the reference's (for masses >= 0).  One warp
+// per node; lane k owns moment 4 + k.  Leaves first, then one launch per tree level,
+// deepest first.
 //
 // M2P.  multipole_acceleration (multipole.cpp:254-296) builds the degree-4 Taylor
 // polynomial of (d + u)_c |d + u|_eps^-3 in the source offset u by truncated polynomial
@@ -84,30 +85,33 @@ __device__ __forceinline__ void write_traces(double* r) {
 }
 
 // Leaf moments: p2m_m2m leaf branch (fmm_solver.cpp:162-167, 180-181) and
-// compute_multipole_moments leaf branch (:187-193).
+// compute_multipole_moments leaf branch (:187-193).  One warp per node; internal nodes
+// return.  A massless leaf gets its cell centre as centre of mass, as in the reference.
 __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
     const int w = (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (w >= a.n_leaves) return;
-    const int b = a.leaf_off[w], e = a.leaf_off[w + 1];
-    double* r = a.rec + (size_t)a.leaf_node[w] * kFmmRec;
+    if (w >= a.n_nodes || a.node_child[w] >= 0) return;
+    const int b = a.node_beg[w], e = a.node_end[w];
+    double* r = a.rec + (size_t)w * kFmmRec;
     double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
     for (int k = b; k < e; ++k) {
-        const int i = a.leaf_part[k];
+        const int i = a.perm[k];
         const double mi = a.m[i];
         mass = dadd(mass, mi);
         wx = dadd(wx, dmul(a.x[i], mi));
         wy = dadd(wy, dmul(a.y[i], mi));
         wz = dadd(wz, dmul(a.z[i], mi));
     }
-    // leaves in the list have mass > 0 (collect_leaves, :210-216)
-    const double cx = __ddiv_rn(wx, mass), cy = __ddiv_rn(wy, mass), cz = __ddiv_rn(wz, mass);
+    const bool pos = mass > 0.0;
+    const double cx = pos ? __ddiv_rn(wx, mass) : a.node_cx[w];
+    const double cy = pos ? __ddiv_rn(wy, mass) : a.node_cy[w];
+    const double cz = pos ? __ddiv_rn(wz, mass) : a.node_cz[w];
     if (lane < 31) {
         int ex, ey, ez;
         exponent_of(4 + lane, ex, ey, ez);
         double v = 0.0;
         for (int k = b; k < e; ++k) {
-            const int i = a.leaf_part[k];
+            const int i = a.perm[k];
             const double ox = dsub(a.x[i], cx), oy = dsub(a.y[i], cy), oz = dsub(a.z[i], cz);
             const double mono = dmul(dmul(pow_int(ox, ex), pow_int(oy, ey)), pow_int(oz, ez));
             v = dadd(v, dmul(a.m[i], mono));
@@ -123,26 +127,30 @@ __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
     if (lane == 0) write_traces(r);
 }
 
-// Internal node: p2m_m2m (fmm_solver.cpp:168-181) over the massive children in child
-// order, then add_multipole_shifted_child per child (multipole.cpp:227-252).  Massless
-// children add exact zeros in the reference and are not visited.
-__global__ void __launch_bounds__(kMomBlock) fmm_m2m_kernel(const FmmArgs a, const int32_t* nodes, int count) {
-    const int w = (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
+// Internal node: p2m_m2m (fmm_solver.cpp:168-181) over the children in octant order, then
+// add_multipole_shifted_child per child (multipole.cpp:227-252).  A massless child adds
+// exact zeros to every sum in the reference and is skipped here (masses are >= 0).
+__global__ void __launch_bounds__(kMomBlock) fmm_m2m_kernel(const FmmArgs a, int lb, int le) {
+    const int w = lb + (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (w >= count) return;
-    const int node = nodes[w];
-    const int c0 = a.node_child[node], nc = a.node_nchild[node];
-    double* r = a.rec + (size_t)node * kFmmRec;
+    if (w >= le) return;
+    const int c0 = a.node_child[w];
+    if (c0 < 0) return;
+    double* r = a.rec + (size_t)w * kFmmRec;
     double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-    for (int c = 0; c < nc; ++c) {
+    for (int c = 0; c < 8; ++c) {
         const double* cr = a.rec + (size_t)(c0 + c) * kFmmRec;
         const double cm = cr[kRecMass];
+        if (!(cm > 0.0)) continue;
         mass = dadd(mass, cm);
         wx = dadd(wx, dmul(cr[0], cm));
         wy = dadd(wy, dmul(cr[1], cm));
         wz = dadd(wz, dmul(cr[2], cm));
     }
-    const double cx = __ddiv_rn(wx, mass), cy = __ddiv_rn(wy, mass), cz = __ddiv_rn(wz, mass);
+    const bool pos = mass > 0.0;
+    const double cx = pos ? __ddiv_rn(wx, mass) : a.node_cx[w];
+    const double cy = pos ? __ddiv_rn(wy, mass) : a.node_cy[w];
+    const double cz = pos ? __ddiv_rn(wz, mass) : a.node_cz[w];
     if (lane < 31) {
         const int ka = 4 + lane;
         int ax, ay, az;
@@ -150,10 +158,11 @@ __global__ void __launch_bounds__(kMomBlock) fmm_m2m_kernel(const FmmArgs a, con
         const int da = ax + ay + az;
         const int nbeta = (da + 1) * (da + 2) * (da + 3) / 6;  // slots of degree <= da
         double total = 0.0;
-        for (int c = 0; c < nc; ++c) {
+        for (int c = 0; c < 8; ++c) {
             const double* cr = a.rec + (size_t)(c0 + c) * kFmmRec;
-            const double sx = dsub(cr[0], cx), sy = dsub(cr[1], cy), sz = dsub(cr[2], cz);
             const double cm = cr[kRecMass];
+            if (!(cm > 0.0)) continue;
+            const double sx = dsub(cr[0], cx), sy = dsub(cr[1], cy), sz = dsub(cr[2], cz);
             double value = 0.0;
             for (int kb = 0; kb < nbeta; ++kb) {
                 int bx, by, bz;
@@ -341,19 +350,17 @@ int fmm_effective_order(int expansion_order) {
     return p;
 }
 
-cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels,
-                               const int32_t* level_node_dev, cudaStream_t st) {
+cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st) {
     constexpr int wpb = kMomBlock / 32;
-    if (a.n_leaves > 0) {
-        fmm_leaf_kernel<<<(a.n_leaves + wpb - 1) / wpb, kMomBlock, 0, st>>>(a);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
+    if (a.n_nodes == 0) return cudaSuccess;
+    fmm_leaf_kernel<<<(a.n_nodes + wpb - 1) / wpb, kMomBlock, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     for (int d = n_levels - 1; d >= 0; --d) {
-        const int count = level_off_host[d + 1] - level_off_host[d];
-        if (count == 0) continue;
-        fmm_m2m_kernel<<<(count + wpb - 1) / wpb, kMomBlock, 0, st>>>(a, level_node_dev + level_off_host[d], count);
-        const cudaError_t e = cudaGetLastError();
+        const int lb = level_off_host[d], le = level_off_host[d + 1];
+        if (le <= lb) continue;
+        fmm_m2m_kernel<<<(le - lb + wpb - 1) / wpb, kMomBlock, 0, st>>>(a, lb, le);
+        e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

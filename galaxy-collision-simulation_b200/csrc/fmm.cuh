@@ -34,13 +34,20 @@ struct FmmArgs {
     const double* y;
     const double* z;
     const double* m;
+    // every node, breadth-first (each level contiguous, the 8 children of a node consecutive)
+    int32_t n_nodes;
+    const int32_t* node_beg;  // bodies perm[beg .. end)
+    const int32_t* node_end;
+    const int32_t* node_child;  // first child, -1 for a leaf
+    const double* node_cx;
+    const double* node_cy;
+    const double* node_cz;
+    const int32_t* perm;
+    // leaves with mass > 0, depth-first
+    int32_t n_leaves;
     const int32_t* leaf_off;
     const int32_t* leaf_part;
-    const int32_t* leaf_node;
-    const int32_t* node_child;
-    const int32_t* node_nchild;
     const int32_t* far_node;
-    int32_t n_leaves;
     double* rec;  // n_nodes * kFmmRec
     const M2PItem* items;
     int32_t n_items;
@@ -60,8 +67,7 @@ int fmm_effective_order(int expansion_order);
 constexpr int kM2PChunk = 64;  // far nodes per work item
 
 // Stream-ordered: leaf moments, then one launch per level (deepest first), then M2P.
-cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels,
-                               const int32_t* level_node_dev, cudaStream_t st);
+cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st);
 cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st);
 
 }  // namespace gx

@@ -1,0 +1,93 @@
+// fmm_build.cuh -- the reference octree and its interaction lists built on the device.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gx {
+
+constexpr int kKeyLevels = 21;  // octant levels a 63-bit path key resolves
+constexpr int kBboxBlocks = 296;
+
+// Tree topology from the bodies (layout of fmm_tree.hpp).  Capacity is the number of node
+// slots allocated; hdr receives {n_nodes, n_levels, overflow} where overflow is 1 when a
+// node below kKeyLevels still has to split (the host builder takes such trees) and 2 when
+// the node slots ran out.
+struct TreeBuildArgs {
+    int32_t n;
+    const double* x;
+    const double* y;
+    const double* z;
+    double softening;
+    int64_t cap;
+    int max_depth;
+    int32_t capacity;
+    double* part;     // bbox partials, 6 * kBboxBlocks
+    double* root;     // cx, cy, cz, hw
+    uint64_t* keys;   // n, then sorted in place through keys_alt
+    uint64_t* keys_alt;
+    int32_t* idx;     // n
+    int32_t* perm;    // n: bodies in tree order
+    int32_t* beg;     // capacity each
+    int32_t* end;
+    int32_t* child;
+    double* cx;
+    double* cy;
+    double* cz;
+    double* hw;
+    int32_t* level_off;  // kKeyLevels + 3
+    int32_t* hdr;        // 3
+};
+size_t tree_build_temp_bytes(int32_t n);
+cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st);
+// After a successful build: bodies of every leaf in ascending index order in t.perm.
+cudaError_t launch_tree_leaf_order(const TreeBuildArgs& t, int32_t n_nodes, void* temp, size_t temp_bytes,
+                                   cudaStream_t st);
+
+// Leaves with mass > 0 (depth-first) and their near / far lists, after the node moments.
+struct TreeListArgs {
+    int32_t n;
+    int32_t n_nodes;
+    const int32_t* beg;
+    const int32_t* end;
+    const int32_t* child;
+    const int32_t* perm;
+    const double* cx;
+    const double* cy;
+    const double* cz;
+    const double* hw;
+    const double* rec;  // node records (mass at slot 3)
+    double theta;
+    int64_t t_begin, t_end;
+    // body-position scratch, n + 1 each
+    int32_t* start_flag;
+    int32_t* start_ord;
+    int32_t* keep;
+    int32_t* newpos;
+    // leaves, n_nodes + 1 each
+    int32_t* leaf_off;
+    int32_t* leaf_part;  // n
+    int32_t* leaf_node;
+    int32_t* node_leaf;  // n_nodes
+    // per-leaf counts and their exclusive sums, n_nodes + 1 each
+    int32_t* far_cnt;
+    int32_t* near_cnt;
+    int32_t* item_cnt;
+    int32_t* slot_cnt;
+    int32_t* far_off;
+    int32_t* near_off;
+    int32_t* item_off;
+    int32_t* slot_off;
+    unsigned long long* totals;  // 4: far, near, items, slots as 64-bit sums (overflow check)
+    // outputs of the fill pass
+    int32_t* far_node;
+    int32_t* near_leaf;
+    void* items;  // M2PItem
+};
+size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes);
+// Leaf compaction, the count walk and the offsets (sizes become known on the host after it).
+cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
+// The fill walk and the far-field work items.
+cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st);
+
+}  // namespace gx

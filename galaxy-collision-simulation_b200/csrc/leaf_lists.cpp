@@ -23,6 +23,9 @@
 #include <vector>
 
 extern "C" int gxi_fail(int code, const char* msg);
+extern "C" int gxi_leaf_lists_from_device(int64_t n, const double* x, const double* y, const double* z,
+                                          const double* m, double softening, double theta, int64_t leaf_capacity,
+                                          int max_depth, void* stream, gx::FmmTree* T, int* on_device);
 
 struct gx_leaf_lists {
     gx::FmmTree t;
@@ -37,7 +40,7 @@ struct Node {
     int child0;  // first of 8 consecutive children, -1 for a leaf
     int64_t beg, end;
     int leaf_id;
-    int id;  // breadth-first number among massive nodes, -1 when massless
+    int id;  // breadth-first number
 };
 
 struct Builder {
@@ -188,51 +191,44 @@ int build_fmm_tree(int64_t n, const double* x, const double* y, const double* z,
 
         FmmTree& T = *out;
         T = FmmTree();
-        T.all_nodes = (int64_t)b.nodes.size();
-        // breadth-first numbering of the massive nodes; children of one node stay consecutive
+        // breadth-first numbering of every node; the 8 children of a node stay consecutive
         std::vector<int> bfs, depth;
-        for (Node& nd : b.nodes) nd.id = -1;
-        if (b.nodes[0].mass > 0.0) {
-            bfs.push_back(0);
-            depth.push_back(0);
-            b.nodes[0].id = 0;
-        }
+        bfs.reserve(b.nodes.size());
+        depth.reserve(b.nodes.size());
+        bfs.push_back(0);
+        depth.push_back(0);
+        b.nodes[0].id = 0;
         for (size_t k = 0; k < bfs.size(); ++k) {
             const Node& nd = b.nodes[bfs[k]];
             if (nd.child0 < 0) continue;
             for (int c = 0; c < 8; ++c) {
-                Node& ch = b.nodes[nd.child0 + c];
-                if (ch.mass <= 0.0) continue;
-                ch.id = (int)bfs.size();
+                b.nodes[nd.child0 + c].id = (int)bfs.size();
                 bfs.push_back(nd.child0 + c);
                 depth.push_back(depth[k] + 1);
             }
         }
-        const int nn = (int)bfs.size();
-        T.node_child.assign(nn, -1);
-        T.node_nchild.assign(nn, 0);
-        int max_level = 0;
-        for (int k = 0; k < nn; ++k) {
+        const size_t nn = bfs.size();
+        T.node_beg.resize(nn);
+        T.node_end.resize(nn);
+        T.node_child.resize(nn);
+        T.node_cx.resize(nn);
+        T.node_cy.resize(nn);
+        T.node_cz.resize(nn);
+        T.node_hw.resize(nn);
+        for (size_t k = 0; k < nn; ++k) {
             const Node& nd = b.nodes[bfs[k]];
-            max_level = std::max(max_level, depth[k]);
-            if (nd.child0 < 0) continue;
-            for (int c = 0; c < 8; ++c) {
-                const Node& ch = b.nodes[nd.child0 + c];
-                if (ch.mass <= 0.0) continue;
-                if (T.node_child[k] < 0) T.node_child[k] = ch.id;
-                T.node_nchild[k]++;
-            }
+            T.node_beg[k] = (int32_t)nd.beg;
+            T.node_end[k] = (int32_t)nd.end;
+            T.node_child[k] = nd.child0 < 0 ? -1 : b.nodes[nd.child0].id;
+            T.node_cx[k] = nd.c[0];
+            T.node_cy[k] = nd.c[1];
+            T.node_cz[k] = nd.c[2];
+            T.node_hw[k] = nd.hw;
         }
-        T.level_off.assign(max_level + 2, 0);
-        for (int k = 0; k < nn; ++k)
-            if (T.node_child[k] >= 0) T.level_off[depth[k] + 1]++;
-        for (int d = 0; d <= max_level; ++d) T.level_off[d + 1] += T.level_off[d];
-        T.level_node.resize(T.level_off[max_level + 1]);
-        {
-            std::vector<int32_t> fill(T.level_off.begin(), T.level_off.end() - 1);
-            for (int k = 0; k < nn; ++k)
-                if (T.node_child[k] >= 0) T.level_node[fill[depth[k]]++] = k;
-        }
+        T.level_off.assign(depth.back() + 2, 0);
+        for (size_t k = 0; k < nn; ++k) T.level_off[depth[k] + 1] = (int32_t)(k + 1);
+        T.perm.resize((size_t)n);
+        for (int64_t k = 0; k < n; ++k) T.perm[(size_t)k] = (int32_t)b.perm[(size_t)k];
 
         const size_t nl = leaves.size();
         T.leaf_off.resize(nl + 1);
@@ -288,6 +284,27 @@ extern "C" int gx_leaf_lists_build(int64_t n, const double* x, const double* y, 
         delete L;
         return rc;
     }
+    *out = L;
+    return GX_OK;
+}
+
+extern "C" int gx_leaf_lists_build_device(int64_t n, const double* x, const double* y, const double* z,
+                                          const double* m, double softening, double theta, int64_t leaf_capacity,
+                                          int max_depth, void* stream, gx_leaf_lists** out, int* built_on_device) {
+    if (!out) return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build_device: out is null");
+    *out = nullptr;
+    if (n <= 0 || !x || !y || !z || !m)
+        return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_leaf_lists_build_device: need n > 0 and x, y, z, m");
+    gx_leaf_lists* L = new (std::nothrow) gx_leaf_lists();
+    if (!L) return gxi_fail(GX_ERR_OUT_OF_MEMORY, "gx_leaf_lists_build_device: host allocation failed");
+    int dev = 0;
+    const int rc = gxi_leaf_lists_from_device(n, x, y, z, m, softening, theta, leaf_capacity, max_depth, stream, &L->t,
+                                              &dev);
+    if (rc != GX_OK) {
+        delete L;
+        return rc;
+    }
+    if (built_on_device) *built_on_device = dev;
     *out = L;
     return GX_OK;
 }

@@ -25,6 +25,7 @@ class LeafLists:
     near_leaves: np.ndarray     # int32, leaf ids
     n_far: int = 0
     n_pairs: int = 0
+    built_on_device: bool = False
 
     @property
     def n_leaves(self) -> int:
@@ -32,11 +33,19 @@ class LeafLists:
 
 
 def build_leaf_lists(x, y, z, m, softening: float, theta: float = 0.6, leaf_capacity: int = 16,
-                     max_depth: int = 32) -> LeafLists:
+                     max_depth: int = 32, on_device: bool = False) -> LeafLists:
+    """Leaf lists of the reference octree, built on the host or (on_device) on the GPU;
+    ``on_device`` sets ``LeafLists.built_on_device`` to what actually ran (trees deeper
+    than 21 levels are always built on the host)."""
     xs = [np.ascontiguousarray(a, np.float64) for a in (x, y, z, m)]
     h = ctypes.c_void_p()
-    _ffi.call("gx_leaf_lists_build", len(xs[0]), *(ptr(a) for a in xs), float(softening), float(theta),
-              int(leaf_capacity), int(max_depth), ctypes.byref(h))
+    where = ctypes.c_int(0)
+    if on_device:
+        _ffi.call("gx_leaf_lists_build_device", len(xs[0]), *(ptr(a) for a in xs), float(softening), float(theta),
+                  int(leaf_capacity), int(max_depth), None, ctypes.byref(h), ctypes.byref(where))
+    else:
+        _ffi.call("gx_leaf_lists_build", len(xs[0]), *(ptr(a) for a in xs), float(softening), float(theta),
+                  int(leaf_capacity), int(max_depth), ctypes.byref(h))
     try:
         nl, nlp, nn, nf, npairs = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _ffi.call("gx_leaf_lists_info", h, ctypes.byref(nl), ctypes.byref(nlp), ctypes.byref(nn), ctypes.byref(nf),
@@ -48,7 +57,7 @@ def build_leaf_lists(x, y, z, m, softening: float, theta: float = 0.6, leaf_capa
         _ffi.call("gx_leaf_lists_export", h, ptr(lo), ptr(lp), ptr(no), ptr(nlv))
     finally:
         _ffi.call("gx_leaf_lists_free", h)
-    return LeafLists(lo, lp, no, nlv[: nn.value], nf.value, npairs.value)
+    return LeafLists(lo, lp, no, nlv[: nn.value], nf.value, npairs.value, bool(where.value))
 
 
 def p2p_leaves(x, y, z, m, lists: LeafLists, params: PhysicsParams, ax, ay, az, precision=PRECISION_F64,

@@ -193,11 +193,12 @@ typedef struct gx_fmm_stats {
 } gx_fmm_stats;
 
 /* compute_fmm_accelerations_for_targets (fmm_solver.cpp:324-333); begin = 0, end = n is
- * compute_fmm_accelerations (:315-322).  The reference octree and its interaction lists
- * are built on the host; the node moments (bit-identical to the reference's), the
- * multipole far field (FP64) and the P2P near field (in `precision`) run on the device.
- * Only bodies in [begin, min(end, n)) are written; bodies of massless leaves get zero, as
- * in the reference.  Host or device arrays; `stats` may be NULL. */
+ * compute_fmm_accelerations (:315-322).  The reference octree, its interaction lists,
+ * the node moments (bit-identical to the reference's), the multipole far field (FP64)
+ * and the P2P near field (in `precision`) all run on the device; trees deeper than 21
+ * levels are built on the host.  Only bodies in [begin, min(end, n)) are written; bodies
+ * of massless leaves get zero, as in the reference.  Masses must be >= 0 (host arrays are
+ * checked).  Host or device arrays; `stats` may be NULL. */
 int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
                  gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
                  double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream);
@@ -217,6 +218,14 @@ typedef struct gx_leaf_lists gx_leaf_lists;
 int gx_leaf_lists_build(int64_t n, const double* x, const double* y, const double* z,
                         const double* m, double softening, double theta,
                         int64_t leaf_capacity, int max_depth, gx_leaf_lists** out);
+/* The same lists built on the device (host arrays in, host lists out): the octree from a
+ * stable sort of per-body 63-bit cell paths, the lists by a per-leaf walk.  A tree that
+ * needs a split below depth 21 (more than leaf_capacity nearly coincident bodies) is built
+ * by the host builder instead; *built_on_device (nullable) reports which ran. */
+int gx_leaf_lists_build_device(int64_t n, const double* x, const double* y, const double* z,
+                               const double* m, double softening, double theta,
+                               int64_t leaf_capacity, int max_depth, void* stream,
+                               gx_leaf_lists** out, int* built_on_device);
 int gx_leaf_lists_info(const gx_leaf_lists* l, int32_t* n_leaves, int64_t* n_leaf_particles,
                        int64_t* n_near, int64_t* n_far, int64_t* n_p2p_pairs);
 int gx_leaf_lists_export(const gx_leaf_lists* l, int32_t* leaf_offsets,

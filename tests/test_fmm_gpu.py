@@ -185,3 +185,49 @@ def test_fixture_trajectory_20_steps(golden):
             s[v] = s[v] + s[a] * (0.5 * dt)
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.abs(s[k] - g[k + "20"]).max() <= 1e-10, k
+
+
+@pytest.mark.parametrize("n,cap,theta", [(20000, 64, 0.6), (5000, 16, 0.35), (3000, 1, 0.6), (50000, 16, 0.9),
+                                         (1, 16, 0.6), (9, 8, 0.6)])
+def test_device_built_lists_equal_host_built(n, cap, theta):
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 7 * n + cap, 0.02)
+    h = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, theta, cap)
+    d = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, theta, cap, on_device=True)
+    assert d.built_on_device
+    for f in ("leaf_offsets", "leaf_particles", "near_offsets", "near_leaves"):
+        assert np.array_equal(getattr(h, f), getattr(d, f)), f
+    assert (h.n_far, h.n_pairs) == (d.n_far, d.n_pairs)
+
+
+@need_ref
+def test_device_built_lists_equal_reference():
+    p = gx.ics.two_disk_encounter(6000, 2000, 31, 0.02)
+    ref, _ = oracle.ref_fmm_split(p.x, p.y, p.z, p.m, 1.0, 0.02, 0.6, 16)
+    d = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16, on_device=True)
+    for f in ("leaf_offsets", "leaf_particles", "near_offsets", "near_leaves"):
+        assert np.array_equal(ref[f], getattr(d, f)), f
+
+
+def test_massless_leaves_device_lists():
+    p = gx.ics.two_disk_encounter(3000, 3000, 32, 0.02)
+    p.m[3000:] = 0.0
+    p.m[::5] = 0.0
+    h = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
+    d = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16, on_device=True)
+    assert d.built_on_device
+    for f in ("leaf_offsets", "leaf_particles", "near_offsets", "near_leaves"):
+        assert np.array_equal(getattr(h, f), getattr(d, f)), f
+
+
+@need_ref
+def test_deep_tree_uses_host_builder():
+    """40 coincident bodies with leaf_capacity 16 split down to max_depth 32 in the
+    reference; the device builder hands such trees to the host builder."""
+    p = gx.ics.two_disk_encounter(2000, 2000, 33, 0.02)
+    for k in range(100, 140):
+        p.x[k], p.y[k], p.z[k] = p.x[99], p.y[99], p.z[99]
+    d = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16, on_device=True)
+    assert not d.built_on_device
+    ref = oracle.ref_fmm(p.x, p.y, p.z, p.m, 1.0, 0.02, 0.6, 16)
+    a, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
+    assert rel_err(a, ref).max() <= 1e-12
