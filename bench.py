@@ -194,7 +194,8 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
     ap.add_argument("--workload", default="mixed-n1048576",
-                    choices=["mixed-n1048576", "ensemble", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
+                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "p2p-n65536", "direct-n65536", "direct-n1000",
+                             "fit-n16384"],
                     help="headline (default) or one of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
@@ -658,8 +659,130 @@ def wl_fit(gx, torch, args) -> dict:
     return res
 
 
+FP64_LANES_PER_SM = 64
+# FP64 pipe instructions of one far-field (target, node) evaluation at expansion order 4
+# (m2p_one<4> in csrc/fmm.cu: offsets, softened r^-1 with one refinement step, g1..g5,
+# the quadrupole, octupole and hexadecapole contractions and the accumulation; 171.3
+# measured as DADD + DMUL + DFMA thread instructions per pair), and of one FP64 near-field
+# interaction (offsets, r^2 + eps^2, r^-3 with one refinement step, m r^-3, three
+# accumulations), the count of the direct FP64 kernel.
+FP64_OPS_PER_M2P_PAIR = 171
+FP64_OPS_PER_P2P_PAIR = 17
+
+
+def wl_fmm(gx, torch, args) -> dict:
+    """The reference FMM solver on the N = 65,536 two-disk workload (leaf_capacity 64,
+    theta 0.6, expansion order 4, softening 0.02, dt 0.002): one KDK step = kick-drift,
+    a full FMM force evaluation (octree, lists, moments, far and near field, all on the
+    device), kick.  Device-resident state; the e2e line runs the public API on host
+    arrays.  CPU baseline: the reference's own FastMultipoleSolver (build + evaluate_particle
+    over all host threads), timed on a target sample and extrapolated to one evaluation."""
+    import oracle
+    n, cap, theta, eps, dt = 65536, 64, 0.6, 0.02, 0.002
+    steps = args.steps if args.steps != 10 else 20
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, eps)
+    params, opt = gx.PhysicsParams(1.0, eps), gx.FmmOptions(theta, cap, 32, 4)
+    D = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    A = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(3)]
+    st = torch.cuda.Stream()
+    sp = st.cuda_stream
+    P3 = lambda *ts: [t.data_ptr() for t in ts]
+
+    def step():
+        gx._ffi.call("gx_kick_drift", n, *P3(D["x"], D["y"], D["z"], D["vx"], D["vy"], D["vz"], *A), 0.5 * dt, dt, sp)
+        gx.fmm.fmm_accelerations(D["x"], D["y"], D["z"], D["m"], *A, params, opt, gx.PRECISION_F64, stream=sp)
+        gx._ffi.call("gx_kick", n, *P3(D["vx"], D["vy"], D["vz"], *A), 0.5 * dt, sp)
+
+    with torch.cuda.stream(st):
+        stats = gx.fmm.fmm_accelerations(D["x"], D["y"], D["z"], D["m"], *A, params, opt, gx.PRECISION_F64, stream=sp)
+        a0 = torch.stack(A, 1).cpu().numpy()
+        for _ in range(max(3, args.warmup)):
+            step()
+        st.synchronize()
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        time.sleep(0.3)
+        e0, e1 = _events(torch)
+        e0.record(st)
+        for _ in range(steps):
+            step()
+        e1.record(st)
+        e1.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / steps
+        # phase times of a few evaluations (same state, same stream)
+        phases = []
+        for _ in range(5):
+            _, ph = gx.fmm.fmm_accelerations_timed(D["x"], D["y"], D["z"], D["m"], *A, params, opt, gx.PRECISION_F64,
+                                                   stream=sp)
+            phases.append(ph)
+    ph = {k: float(np.median([q[k] for q in phases])) for k in gx.fmm.PHASES}
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    peaks = json.loads(Path(__file__).with_name("MEASURED_PEAKS.json").read_text()) \
+        if Path(__file__).with_name("MEASURED_PEAKS.json").exists() else {}
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    fp64_peak = sms * FP64_LANES_PER_SM * mhz * 1e6 / 1e12
+    near_int = stats.near_pairs - n  # ordered pairs, self pairs excluded
+    p2p_ach = near_int * FP64_OPS_PER_P2P_PAIR / (ph["near_field"] / 1e3) / 1e12
+    m2p_ach = stats.far_pairs * FP64_OPS_PER_M2P_PAIR / (ph["far_field"] / 1e3) / 1e12
+    dominant = "near_field" if ph["near_field"] >= ph["far_field"] else "far_field"
+    roof = {"bound": "fp64_pipe", "kernel": "p2p_kernel (FP64 near field)" if dominant == "near_field"
+            else "fmm_m2p_kernel<4> (far field)",
+            "achieved": p2p_ach if dominant == "near_field" else m2p_ach, "peak": fp64_peak,
+            "unit": "T FP64-pipe lane-ops/s",
+            "frac": (p2p_ach if dominant == "near_field" else m2p_ach) / fp64_peak,
+            "peak_basis": f"{sms} SMs x {FP64_LANES_PER_SM} FP64 lanes x {mhz:.0f} MHz (sm_max_mhz of "
+                          "MEASURED_PEAKS.json); FP64 arithmetic bounds both kernels, not HBM",
+            "near_field": {"interactions": near_int, "ops_per_interaction": FP64_OPS_PER_P2P_PAIR,
+                           "phase_ms": ph["near_field"], "achieved": p2p_ach, "frac": p2p_ach / fp64_peak,
+                           "note": "phase = plan (count, scan) + kernel"},
+            "far_field": {"pairs": stats.far_pairs, "ops_per_pair": FP64_OPS_PER_M2P_PAIR,
+                          "phase_ms": ph["far_field"], "achieved": m2p_ach, "frac": m2p_ach / fp64_peak},
+            "traffic": None}
+
+    # e2e: the public API on host arrays (H2D of x, y, z, m and D2H of a inside the call)
+    q = p.copy()
+    gx.fmm.compute_fmm_accelerations(q, params, opt)
+    t0 = time.perf_counter()
+    e2e_steps = max(3, steps // 2)
+    for _ in range(e2e_steps):
+        q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
+        q.x += q.vx * dt; q.y += q.vy * dt; q.z += q.vz * dt
+        gx.fmm.compute_fmm_accelerations(q, params, opt)
+        q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
+    e2e = e2e_steps / (time.perf_counter() - t0)
+
+    out = {"metric": "FMM KDK steps/s (N=65536, leaf 64, theta 0.6, p=4, FP64)", "value": 1e3 / ms,
+           "unit": "steps/s", "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "phases_ms_per_eval": ph, "stats": stats.__dict__,
+           "gpu_launches": steps * (19 + stats.tree_levels + 2),
+           "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 3 * n * 8},
+           "roofline": roof, "clocks": clk,
+           "config": {"workload": "fmm-n65536", "n": n, "leaf_capacity": cap, "theta": theta, "expansion_order": 4,
+                      "softening": eps, "dt": dt, "near_field_precision": "f64",
+                      "l2": "inputs (5 MiB) stay L2-resident; not flushed between steps"}}
+    if oracle.ref_available():
+        threads = os.cpu_count() or 1
+        _, b_s, e_s, k = oracle.ref_fmm_timed(p.x, p.y, p.z, p.m, 1.0, eps, theta, cap, 4, 256, threads)
+        per_target = e_s / max(k, 1)
+        stride = max(1, int(np.ceil(n * per_target / max(args.cpu_seconds, 1.0))))
+        acc, b_s, e_s, k = oracle.ref_fmm_timed(p.x, p.y, p.z, p.m, 1.0, eps, theta, cap, 4, stride, threads)
+        eval_s = b_s + e_s * n / k
+        ok = ~np.isnan(acc[:, 0])
+        err = np.linalg.norm(a0[ok] - acc[ok], axis=1) / np.linalg.norm(acc[ok], axis=1)
+        out["cpu_baseline"] = {"value": 1.0 / eval_s, "unit": "steps/s", "cores": threads, "kind": "reference",
+                               "sample": f"FastMultipoleSolver::build once ({b_s:.3f} s) + evaluate_particle on every "
+                                         f"{stride}-th body ({k} bodies, {e_s:.2f} s on {threads} threads), "
+                                         "extrapolated to all bodies; one evaluation per step"}
+        out["parity_vs_reference"] = {"bodies": int(ok.sum()), "rel_err_max": float(err.max()),
+                                      "rel_err_median": float(np.median(err))}
+    return out
+
+
 OTHER_WORKLOADS = {
     "ensemble": wl_ensemble,
+    "fmm-n65536": wl_fmm,
     "p2p-n65536": wl_p2p,
     "direct-n65536": lambda gx, torch, args: wl_direct(gx, torch, args, 65536, 0.02, 0.002, 100),
     "direct-n1000": lambda gx, torch, args: wl_direct(gx, torch, args, 1000, 0.05, 0.005, 20),

@@ -76,7 +76,8 @@ class FmmStatsStruct(ctypes.Structure):
     """gx_fmm_stats: FmmStats of the reference (cpp/fmm/fmm_solver.hpp:22-27)."""
 
     _fields_ = [("node_count", c_int64), ("leaf_count", c_int64), ("far_interactions", c_int64),
-                ("near_interactions", c_int64)]
+                ("near_interactions", c_int64), ("far_pairs", c_int64), ("near_pairs", c_int64),
+                ("tree_levels", c_int64)]
 
 
 P = c_void_p  # any array: numpy .ctypes.data, torch .data_ptr(), or None
@@ -117,6 +118,8 @@ _SIGNATURES = {
     "gx_p2p_leaves": [I64, P, P, P, P, c_int32, P, P, P, P, Physics, c_int, P, P, P, S],
     "gx_fmm_accel": [I64, P, P, P, P, Physics, FmmOptionsStruct, c_int, I64, I64, P, P, P, POINTER(FmmStatsStruct),
                      S],
+    "gx_fmm_accel_timed": [I64, P, P, P, P, Physics, FmmOptionsStruct, c_int, I64, I64, P, P, P,
+                           POINTER(FmmStatsStruct), S, P],
     "gx_fmm_moments": [I64, P, P, P, P, Physics, FmmOptionsStruct, I64, P, POINTER(I64)],
     "gx_leaf_lists_build": [I64, P, P, P, P, D, D, I64, c_int, PP],
     "gx_leaf_lists_build_device": [I64, P, P, P, P, D, D, I64, c_int, S, PP, POINTER(c_int)],

@@ -1311,6 +1311,26 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
 // ======================================================================================
 namespace {
 
+// Optional phase timing of one FMM evaluation: events on the caller's stream at the phase
+// boundaries (tree, moments, lists, far field, near field).
+struct FmmTimer {
+    cudaEvent_t ev[6] = {};
+    double host_tree_ms = -1.0;  // the host builder's own time, when it ran
+    int create() {
+        for (auto& e : ev) GX_CUDA(cudaEventCreate(&e));
+        return GX_OK;
+    }
+    ~FmmTimer() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+int mark(FmmTimer* tm, int k, cudaStream_t st) {
+    if (tm) GX_CUDA(cudaEventRecord(tm->ev[k], st));
+    return GX_OK;
+}
+
 // Device arrays and sizes of one FMM evaluation's tree, built on the device or the host.
 struct FmmPlan {
     HostStage hs;
@@ -1319,6 +1339,7 @@ struct FmmPlan {
     int32_t n_nodes = 0, n_leaves = 0;
     std::vector<int32_t> level_off;
     int64_t n_far = 0, n_near = 0, n_slots = 0;
+    int64_t far_pairs = 0, near_pairs = 0;
     FmmArgs fa{};
     const int32_t* near_off = nullptr;
     const int32_t* near_leaf = nullptr;
@@ -1356,10 +1377,16 @@ void fmm_common_args(FmmArgs& fa, const double* dx, const double* dy, const doub
 // Host builder: the octree and lists on the host, moments on the device.
 int fmm_plan_host(FmmPlan& P, int64_t n, const double* hx, const double* hy, const double* hz, const double* hm,
                   const double* dx, const double* dy, const double* dz, const double* dm, gx_physics phys,
-                  gx_fmm_options opt, int64_t begin, int64_t end) {
+                  gx_fmm_options opt, int64_t begin, int64_t end, FmmTimer* tm) {
     HostStage& hs = P.hs;
     FmmTree T;
+    const auto h0 = std::chrono::steady_clock::now();
     GX_TRY(build_fmm_tree(n, hx, hy, hz, hm, phys.softening, opt.theta, opt.leaf_capacity, opt.max_depth, true, &T));
+    if (tm) tm->host_tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+    GX_TRY(mark(tm, 0, hs.st));
+    P.near_pairs = T.n_pairs;
+    for (int32_t l = 0; l < T.n_leaves(); ++l)
+        P.far_pairs += (int64_t)(T.far_off[l + 1] - T.far_off[l]) * (T.leaf_off[l + 1] - T.leaf_off[l]);
     FmmArgs& fa = P.fa;
     fmm_common_args(fa, dx, dy, dz, dm, phys, opt, begin, end);
     P.n_nodes = fa.n_nodes = T.n_nodes();
@@ -1379,8 +1406,10 @@ int fmm_plan_host(FmmPlan& P, int64_t n, const double* hx, const double* hy, con
     GX_TRY(dev_copy(hs, T.far_node, &fa.far_node));
     GX_TRY(dev_copy(hs, T.near_off, &P.near_off));
     GX_TRY(dev_copy(hs, T.near_leaf, &P.near_leaf));
+    GX_TRY(mark(tm, 1, hs.st));
     GX_TRY(dev_array(hs, (int64_t)P.n_nodes * kFmmRec, &fa.rec));
     GX_CUDA(launch_fmm_moments(fa, P.level_off.data(), T.n_levels(), hs.st));
+    GX_TRY(mark(tm, 2, hs.st));
     // far-field work items for the leaves that hold a target in [begin, end)
     std::vector<M2PItem> items;
     int64_t slots = 0;
@@ -1411,15 +1440,17 @@ int fmm_plan_host(FmmPlan& P, int64_t n, const double* hx, const double* hy, con
     fa.n_items = (int32_t)items.size();
     P.n_slots = slots;
     if (!items.empty()) GX_TRY(dev_copy(hs, items, &fa.items));
+    GX_TRY(mark(tm, 3, hs.st));
     return GX_OK;
 }
 
 // Device builder; *deep is set (and nothing else is valid) when the tree needs a split
 // below the key depth, which the host builder handles.
 int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, const double* dz, const double* dm,
-                    gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end, bool* deep) {
+                    gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end, bool* deep, FmmTimer* tm) {
     HostStage& hs = P.hs;
     cudaStream_t st = hs.st;
+    GX_TRY(mark(tm, 0, st));
     *deep = false;
     P.on_device = true;
     const int64_t cap = std::max<int64_t>(1, opt.leaf_capacity);
@@ -1471,6 +1502,7 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
         if (attempt == 1) return fail(GX_ERR_UNSUPPORTED, "FMM: node slots exhausted");
     }
     GX_CUDA(launch_tree_leaf_order(t, hdr[0], sort_temp, sort_bytes, st));
+    GX_TRY(mark(tm, 1, st));
     FmmArgs& fa = P.fa;
     fmm_common_args(fa, dx, dy, dz, dm, phys, opt, begin, end);
     P.n_nodes = fa.n_nodes = hdr[0];
@@ -1484,6 +1516,7 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
     fa.perm = t.perm;
     GX_TRY(dev_array(hs, (int64_t)P.n_nodes * kFmmRec, &fa.rec));
     GX_CUDA(launch_fmm_moments(fa, P.level_off.data(), hdr[1], st));
+    GX_TRY(mark(tm, 2, st));
 
     TreeListArgs la{};
     la.n = t.n;
@@ -1512,30 +1545,42 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
     for (int32_t** p : {&la.far_cnt, &la.near_cnt, &la.item_cnt, &la.slot_cnt, &la.far_off, &la.near_off, &la.item_off,
                         &la.slot_off})
         GX_TRY(dev_array(hs, lb, p));
-    GX_TRY(dev_array(hs, 4, &la.totals));
+    GX_TRY(dev_array(hs, 6, &la.totals));
+    GX_TRY(dev_array(hs, (int64_t)P.n_nodes, &la.wn));
     const size_t list_bytes = tree_list_temp_bytes(la.n, la.n_nodes);
     void* list_temp;
     GX_TRY(dev_array(hs, (int64_t)list_bytes, (char**)&list_temp));
     GX_CUDA(launch_tree_lists_count(la, list_temp, list_bytes, st));
     int32_t nl = 0;
-    unsigned long long tot[4];
+    unsigned long long tot[6];
     GX_CUDA(cudaMemcpyAsync(&nl, la.start_ord + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GX_CUDA(cudaMemcpyAsync(tot, la.totals, sizeof(tot), cudaMemcpyDeviceToHost, st));
     GX_CUDA(cudaStreamSynchronize(st));
-    for (unsigned long long v : tot)
-        if (v > (unsigned long long)std::numeric_limits<int32_t>::max())
+    for (int k = 0; k < 4; ++k)
+        if (tot[k] > (unsigned long long)std::numeric_limits<int32_t>::max())
             return fail(GX_ERR_UNSUPPORTED, "FMM: interaction lists exceed the int32 range");
+    P.far_pairs = (int64_t)tot[4];
+    P.near_pairs = (int64_t)tot[5];
     P.n_leaves = fa.n_leaves = nl;
     P.n_far = (int64_t)tot[0];
     P.n_near = (int64_t)tot[1];
     fa.n_items = (int32_t)tot[2];
     P.n_slots = (int64_t)tot[3];
     GX_TRY(dev_array(hs, P.n_far, &la.far_node));
+    GX_TRY(dev_array(hs, P.n_far, &la.far_key));
+    GX_TRY(dev_array(hs, P.n_far, &la.far_key_alt));
+    GX_TRY(dev_array(hs, P.n_far, &la.far_tmp));
+    GX_TRY(dev_array(hs, P.n_near, &la.near_key));
+    GX_TRY(dev_array(hs, P.n_near, &la.near_key_alt));
     GX_TRY(dev_array(hs, P.n_near, &la.near_leaf));
     M2PItem* items;
     GX_TRY(dev_array(hs, fa.n_items, &items));
     la.items = items;
-    GX_CUDA(launch_tree_lists_fill(la, nl, st));
+    const size_t sort_list_bytes = tree_list_sort_bytes(P.n_far, P.n_near, nl);
+    void* sort_list_temp;
+    GX_TRY(dev_array(hs, (int64_t)sort_list_bytes, (char**)&sort_list_temp));
+    GX_CUDA(launch_tree_lists_fill(la, nl, P.n_far, P.n_near, sort_list_temp, sort_list_bytes, st));
+    GX_TRY(mark(tm, 3, st));
     fa.leaf_off = la.leaf_off;
     fa.leaf_part = la.leaf_part;
     fa.far_node = la.far_node;
@@ -1549,10 +1594,10 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
 // null) spare a download when the host builder has to take over.
 int fmm_plan(std::unique_ptr<FmmPlan>& P, cudaStream_t st, int64_t n, const double* hx, const double* hy,
              const double* hz, const double* hm, const double* dx, const double* dy, const double* dz, const double* dm,
-             gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end) {
+             gx_physics phys, gx_fmm_options opt, int64_t begin, int64_t end, FmmTimer* tm = nullptr) {
     P.reset(new FmmPlan(st));
     bool deep = false;
-    GX_TRY(fmm_plan_device(*P, n, dx, dy, dz, dm, phys, opt, begin, end, &deep));
+    GX_TRY(fmm_plan_device(*P, n, dx, dy, dz, dm, phys, opt, begin, end, &deep, tm));
     if (!deep) return GX_OK;
     std::vector<double> hbuf;
     if (!hx) {
@@ -1568,7 +1613,7 @@ int fmm_plan(std::unique_ptr<FmmPlan>& P, cudaStream_t st, int64_t n, const doub
         hm = hz + n;
     }
     P.reset(new FmmPlan(st));
-    return fmm_plan_host(*P, n, hx, hy, hz, hm, dx, dy, dz, dm, phys, opt, begin, end);
+    return fmm_plan_host(*P, n, hx, hy, hz, hm, dx, dy, dz, dm, phys, opt, begin, end, tm);
 }
 
 int check_fmm_inputs(int64_t n, const double* m, bool device, const char* fn) {
@@ -1580,14 +1625,13 @@ int check_fmm_inputs(int64_t n, const double* m, bool device, const char* fn) {
     return GX_OK;
 }
 
-}  // namespace
 
-extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
-                            gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
-                            double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream) {
-    GX_GUARD_BEGIN
-    const char* fn = "gx_fmm_accel";
-    if (stats) *stats = gx_fmm_stats{0, 0, 0, 0};
+int fmm_accel(const char* fn, int64_t n, const double* x, const double* y, const double* z, const double* m,
+              gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end, double* ax, double* ay,
+              double* az, gx_fmm_stats* stats, void* stream, double* phase_ms) {
+    if (stats) *stats = gx_fmm_stats{0, 0, 0, 0, 0, 0, 0};
+    if (phase_ms)
+        for (int k = 0; k < GX_FMM_PHASES; ++k) phase_ms[k] = 0.0;
     if (n < 0 || begin < 0 || end < 0) return fail(GX_ERR_INVALID_ARGUMENT, "%s: negative size or range", fn);
     if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: unknown precision", fn);
     GX_TRY(check_phys(phys, fn));
@@ -1617,15 +1661,23 @@ extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const d
         GX_TRY(hs.out(&day, n));
         GX_TRY(hs.out(&daz, n));
     }
+    std::unique_ptr<FmmTimer> tm;
+    if (phase_ms) {
+        tm.reset(new FmmTimer());
+        GX_TRY(tm->create());
+    }
     std::unique_ptr<FmmPlan> P;
     GX_TRY(fmm_plan(P, st, n, device ? nullptr : x, device ? nullptr : y, device ? nullptr : z, device ? nullptr : m,
-                    dx, dy, dz, dm, phys, opt, begin, end));
+                    dx, dy, dz, dm, phys, opt, begin, end, tm.get()));
     if (stats) {
         // node_count counts every node the reference creates, massless ones included
         stats->node_count = P->n_nodes;
         stats->leaf_count = P->n_leaves;
         stats->far_interactions = P->n_far;
         stats->near_interactions = P->n_near;
+        stats->far_pairs = P->far_pairs;
+        stats->near_pairs = P->near_pairs;
+        stats->tree_levels = (int64_t)P->level_off.size() - 1;
     }
     // reset_accelerations over the target range (fmm_solver.cpp:31); the far and near
     // fields are then added
@@ -1642,6 +1694,7 @@ extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const d
         fa.scratch = part.d();
         fa.done = (int*)done.p;
         GX_CUDA(launch_fmm_m2p(fa, st));
+        GX_TRY(mark(tm.get(), 4, st));
 
         P2PArgs pa;
         pa.x = dx; pa.y = dy; pa.z = dz; pa.m = dm;
@@ -1655,14 +1708,47 @@ extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const d
         pa.eps2f = (float)pa.eps2;
         GX_TRY(p2p_scratch.alloc(p2p_scratch_bytes(n, P->n_leaves), st));
         GX_CUDA(launch_p2p(pa, n, precision, p2p_scratch.p, sm_count(dev), st));
+    } else {
+        GX_TRY(mark(tm.get(), 4, st));
     }
+    GX_TRY(mark(tm.get(), 5, st));
     if (!device) {
         GX_TRY(copy_back(ax + begin, dax + begin, end - begin, st));
         GX_TRY(copy_back(ay + begin, day + begin, end - begin, st));
         GX_TRY(copy_back(az + begin, daz + begin, end - begin, st));
         GX_CUDA(cudaStreamSynchronize(st));
     }
+    if (phase_ms) {
+        GX_CUDA(cudaEventSynchronize(tm->ev[5]));
+        for (int k = 0; k < GX_FMM_PHASES; ++k) {
+            float ms = 0.0f;
+            GX_CUDA(cudaEventElapsedTime(&ms, tm->ev[k], tm->ev[k + 1]));
+            phase_ms[k] = ms;
+        }
+        if (tm->host_tree_ms >= 0.0) phase_ms[0] = tm->host_tree_ms;
+    }
     return GX_OK;
+}
+
+}  // namespace
+
+extern "C" int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                            gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
+                            double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream) {
+    GX_GUARD_BEGIN
+    return fmm_accel("gx_fmm_accel", n, x, y, z, m, phys, opt, precision, begin, end, ax, ay, az, stats, stream,
+                     nullptr);
+    GX_GUARD_END
+}
+
+extern "C" int gx_fmm_accel_timed(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                                  gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
+                                  double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream,
+                                  double* phase_ms) {
+    GX_GUARD_BEGIN
+    if (!phase_ms) return fail(GX_ERR_INVALID_ARGUMENT, "gx_fmm_accel_timed: phase_ms is null");
+    return fmm_accel("gx_fmm_accel_timed", n, x, y, z, m, phys, opt, precision, begin, end, ax, ay, az, stats, stream,
+                     phase_ms);
     GX_GUARD_END
 }
 

@@ -37,36 +37,58 @@ namespace {
 constexpr int kMomBlock = 256;  // 8 warps, one node each
 constexpr int kM2PBlock = 128;
 
-// Multi-index of moment slot k (0..34) in the reference's exponent order: degree
-// ascending, then the x exponent descending, then the y exponent descending.
-__device__ __forceinline__ void exponent_of(int k, int& ex, int& ey, int& ez) {
-    int d = 0;
-    while ((d + 1) * (d + 2) * (d + 3) / 6 <= k) ++d;
-    int r = k - d * (d + 1) * (d + 2) / 6;
-    ex = d;
-    while (r > d - ex) {
-        r -= d - ex + 1;
-        --ex;
-    }
-    ey = d - ex - r;
-    ez = d - ex - ey;
-}
-
-// pow_int (multipole.cpp:43-49): 1.0 multiplied by v, e times.
-__device__ __forceinline__ double pow_int(double v, int e) {
-    double r = 1.0;
-    for (int i = 0; i < e; ++i) r = dmul(r, v);
-    return r;
-}
-
 // binomial (multipole.cpp:57-76) for n <= 4.
-__device__ __forceinline__ int binom4(int n, int k) {
-    if (k < 0 || k > n) return 0;
-    if (k == 0 || k == n) return 1;
-    if (n == 2) return 2;
-    if (n == 3) return 3;
-    return k == 2 ? 6 : 4;
+constexpr int binom4(int n, int k) {
+    return (k < 0 || k > n) ? 0 : (k == 0 || k == n) ? 1 : n == 2 ? 2 : n == 3 ? 3 : (k == 2 ? 6 : 4);
 }
+
+constexpr int kMaxShiftTerms = 12;  // (2+1)(1+1)(1+1): the most multi-indices below a degree-4 one
+
+// Index tables, evaluated at compile time.  Moment slot k (0..34) is the reference's
+// exponent order (multipole.cpp:16-26): degree ascending, then the x exponent descending,
+// then the y exponent descending.  For every moment alpha of degree 2..4 (slot 4 + a) the
+// terms of add_multipole_shifted_child (multipole.cpp:227-252) in the reference's beta
+// order: beta <= alpha componentwise, degree-1 betas left out (their moment is 0 about the
+// child's centre of mass, and adding the zero product never changes a sum that starts at
+// +0), each with the binomial product and the exponents of the shift.
+struct MomentTables {
+    int ex[35] = {}, ey[35] = {}, ez[35] = {};
+    int nterm[31] = {};
+    double bin[31][kMaxShiftTerms] = {};
+    int kb[31][kMaxShiftTerms] = {}, dx[31][kMaxShiftTerms] = {}, dy[31][kMaxShiftTerms] = {},
+        dz[31][kMaxShiftTerms] = {};
+};
+
+constexpr MomentTables make_moment_tables() {
+    MomentTables t;
+    int k = 0;
+    for (int d = 0; d <= 4; ++d)
+        for (int x = d; x >= 0; --x)
+            for (int y = d - x; y >= 0; --y) {
+                t.ex[k] = x;
+                t.ey[k] = y;
+                t.ez[k] = d - x - y;
+                ++k;
+            }
+    for (int a = 0; a < 31; ++a) {
+        const int ka = 4 + a, ax = t.ex[ka], ay = t.ey[ka], az = t.ez[ka];
+        int n = 0;
+        for (int b = 0; b < 35; ++b) {
+            const int bx = t.ex[b], by = t.ey[b], bz = t.ez[b];
+            if (bx > ax || by > ay || bz > az || bx + by + bz == 1) continue;
+            t.bin[a][n] = (double)(binom4(ax, bx) * binom4(ay, by) * binom4(az, bz));
+            t.kb[a][n] = b;
+            t.dx[a][n] = ax - bx;
+            t.dy[a][n] = ay - by;
+            t.dz[a][n] = az - bz;
+            ++n;
+        }
+        t.nterm[a] = n;
+    }
+    return t;
+}
+
+__device__ const MomentTables kTab = make_moment_tables();
 
 // Traces of the moments (record slots 35..45) from slots 4..34.
 __device__ __forceinline__ void write_traces(double* r) {
@@ -84,38 +106,69 @@ __device__ __forceinline__ void write_traces(double* r) {
     r[kRecTr2] = txx + tyy + tzz;
 }
 
+// v^e for e in 0..4 as pow_int (multipole.cpp:43-49) computes it: 1.0 times v, e times
+// (the first product is exact).
+struct Pow4 {
+    double p1, p2, p3, p4;
+    __device__ __forceinline__ explicit Pow4(double v) : p1(v), p2(dmul(v, v)), p3(dmul(p2, v)), p4(dmul(p3, v)) {}
+    __device__ __forceinline__ double operator()(int e) const {
+        return e == 0 ? 1.0 : (e == 1 ? p1 : (e == 2 ? p2 : (e == 3 ? p3 : p4)));
+    }
+};
+
 // Leaf moments: p2m_m2m leaf branch (fmm_solver.cpp:162-167, 180-181) and
 // compute_multipole_moments leaf branch (:187-193).  One warp per node; internal nodes
-// return.  A massless leaf gets its cell centre as centre of mass, as in the reference.
+// return.  The leaf's bodies are staged 32 at a time in shared memory; every lane then
+// runs the reference's sequential sums over them (lane k for moment 4 + k).  A massless
+// leaf gets its cell centre as centre of mass, as in the reference.
 __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
+    __shared__ double s_b[kMomBlock / 32][4][32];
+    const int wl = threadIdx.x >> 5;
     const int w = (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (w >= a.n_nodes || a.node_child[w] >= 0) return;
     const int b = a.node_beg[w], e = a.node_end[w];
     double* r = a.rec + (size_t)w * kFmmRec;
+    double(*sb)[32] = s_b[wl];
+    auto stage = [&](int k0) {
+        __syncwarp();
+        if (k0 + lane < e) {
+            const int i = a.perm[k0 + lane];
+            sb[0][lane] = a.x[i];
+            sb[1][lane] = a.y[i];
+            sb[2][lane] = a.z[i];
+            sb[3][lane] = a.m[i];
+        }
+        __syncwarp();
+        return min(32, e - k0);
+    };
     double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-    for (int k = b; k < e; ++k) {
-        const int i = a.perm[k];
-        const double mi = a.m[i];
-        mass = dadd(mass, mi);
-        wx = dadd(wx, dmul(a.x[i], mi));
-        wy = dadd(wy, dmul(a.y[i], mi));
-        wz = dadd(wz, dmul(a.z[i], mi));
+    for (int k0 = b; k0 < e; k0 += 32) {
+        const int cnt = stage(k0);
+        for (int q = 0; q < cnt; ++q) {
+            const double mi = sb[3][q];
+            mass = dadd(mass, mi);
+            wx = dadd(wx, dmul(sb[0][q], mi));
+            wy = dadd(wy, dmul(sb[1][q], mi));
+            wz = dadd(wz, dmul(sb[2][q], mi));
+        }
     }
     const bool pos = mass > 0.0;
     const double cx = pos ? __ddiv_rn(wx, mass) : a.node_cx[w];
     const double cy = pos ? __ddiv_rn(wy, mass) : a.node_cy[w];
     const double cz = pos ? __ddiv_rn(wz, mass) : a.node_cz[w];
-    if (lane < 31) {
-        int ex, ey, ez;
-        exponent_of(4 + lane, ex, ey, ez);
-        double v = 0.0;
-        for (int k = b; k < e; ++k) {
-            const int i = a.perm[k];
-            const double ox = dsub(a.x[i], cx), oy = dsub(a.y[i], cy), oz = dsub(a.z[i], cz);
-            const double mono = dmul(dmul(pow_int(ox, ex), pow_int(oy, ey)), pow_int(oz, ez));
-            v = dadd(v, dmul(a.m[i], mono));
+    const int ks = lane < 31 ? 4 + lane : 0;
+    const int ex = kTab.ex[ks], ey = kTab.ey[ks], ez = kTab.ez[ks];
+    double v = 0.0;
+    for (int k0 = b; k0 < e; k0 += 32) {
+        const int cnt = stage(k0);
+        for (int q = 0; q < cnt; ++q) {
+            const Pow4 px(dsub(sb[0][q], cx)), py(dsub(sb[1][q], cy)), pz(dsub(sb[2][q], cz));
+            const double mono = dmul(dmul(px(ex), py(ey)), pz(ez));
+            v = dadd(v, dmul(sb[3][q], mono));
         }
+    }
+    if (lane < 31) {
         r[4 + lane] = v;
     } else {
         r[0] = cx;
@@ -128,56 +181,56 @@ __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
 }
 
 // Internal node: p2m_m2m (fmm_solver.cpp:168-181) over the children in octant order, then
-// add_multipole_shifted_child per child (multipole.cpp:227-252).  A massless child adds
-// exact zeros to every sum in the reference and is skipped here (masses are >= 0).
-__global__ void __launch_bounds__(kMomBlock) fmm_m2m_kernel(const FmmArgs a, int lb, int le) {
-    const int w = lb + (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (w >= le) return;
+// add_multipole_shifted_child per child (multipole.cpp:227-252).  One CTA per node: the 8
+// children's records are staged in shared memory, warp c computes child c's shifted
+// contribution to every moment (lane a for moment 4 + a), and warp 0 adds the 8
+// contributions in child order, as the reference does.  A massless child adds exact zeros
+// to every sum in the reference and is skipped here (masses are >= 0).
+__global__ void __launch_bounds__(256) fmm_m2m_kernel(const FmmArgs a, int lb) {
+    __shared__ double s_child[8][kRecTrQ];
+    __shared__ double s_val[8][32];
+    const int w = lb + blockIdx.x;
     const int c0 = a.node_child[w];
     if (c0 < 0) return;
-    double* r = a.rec + (size_t)w * kFmmRec;
+    const int tid = threadIdx.x, c = tid >> 5, lane = tid & 31;
+    for (int k = tid; k < 8 * kRecTrQ; k += 256) s_child[k / kRecTrQ][k % kRecTrQ] = a.rec[(size_t)(c0 + k / kRecTrQ) * kFmmRec + k % kRecTrQ];
+    __syncthreads();
     double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-    for (int c = 0; c < 8; ++c) {
-        const double* cr = a.rec + (size_t)(c0 + c) * kFmmRec;
-        const double cm = cr[kRecMass];
+    for (int q = 0; q < 8; ++q) {
+        const double cm = s_child[q][kRecMass];
         if (!(cm > 0.0)) continue;
         mass = dadd(mass, cm);
-        wx = dadd(wx, dmul(cr[0], cm));
-        wy = dadd(wy, dmul(cr[1], cm));
-        wz = dadd(wz, dmul(cr[2], cm));
+        wx = dadd(wx, dmul(s_child[q][0], cm));
+        wy = dadd(wy, dmul(s_child[q][1], cm));
+        wz = dadd(wz, dmul(s_child[q][2], cm));
     }
     const bool pos = mass > 0.0;
     const double cx = pos ? __ddiv_rn(wx, mass) : a.node_cx[w];
     const double cy = pos ? __ddiv_rn(wy, mass) : a.node_cy[w];
     const double cz = pos ? __ddiv_rn(wz, mass) : a.node_cz[w];
-    if (lane < 31) {
-        const int ka = 4 + lane;
-        int ax, ay, az;
-        exponent_of(ka, ax, ay, az);
-        const int da = ax + ay + az;
-        const int nbeta = (da + 1) * (da + 2) * (da + 3) / 6;  // slots of degree <= da
-        double total = 0.0;
-        for (int c = 0; c < 8; ++c) {
-            const double* cr = a.rec + (size_t)(c0 + c) * kFmmRec;
-            const double cm = cr[kRecMass];
-            if (!(cm > 0.0)) continue;
-            const double sx = dsub(cr[0], cx), sy = dsub(cr[1], cy), sz = dsub(cr[2], cz);
-            double value = 0.0;
-            for (int kb = 0; kb < nbeta; ++kb) {
-                int bx, by, bz;
-                exponent_of(kb, bx, by, bz);
-                if (bx > ax || by > ay || bz > az) continue;  // multinomial_shift == 0
-                const double bin = (double)(binom4(ax, bx) * binom4(ay, by) * binom4(az, bz));
-                const double sf = dmul(dmul(dmul(bin, pow_int(sx, ax - bx)), pow_int(sy, ay - by)), pow_int(sz, az - bz));
-                if (sf == 0.0) continue;
-                const int db = bx + by + bz;
-                const double mv = db == 0 ? cm : (db == 1 ? 0.0 : cr[kb]);
-                value = dadd(value, dmul(sf, mv));
-            }
-            total = dadd(total, value);
+    const double* cr = s_child[c];
+    const double cm = cr[kRecMass];
+    if (lane < 31 && cm > 0.0) {
+        const Pow4 px(dsub(cr[0], cx)), py(dsub(cr[1], cy)), pz(dsub(cr[2], cz));
+        const int nt = kTab.nterm[lane];
+        double value = 0.0;
+        for (int q = 0; q < nt; ++q) {
+            const double sf = dmul(dmul(dmul(kTab.bin[lane][q], px(kTab.dx[lane][q])), py(kTab.dy[lane][q])),
+                                   pz(kTab.dz[lane][q]));
+            if (sf == 0.0) continue;
+            const int kb = kTab.kb[lane][q];
+            value = dadd(value, dmul(sf, kb == 0 ? cm : cr[kb]));
         }
-        r[ka] = total;
+        s_val[c][lane] = value;
+    }
+    __syncthreads();
+    if (c != 0) return;
+    double* r = a.rec + (size_t)w * kFmmRec;
+    if (lane < 31) {
+        double total = 0.0;
+        for (int q = 0; q < 8; ++q)
+            if (s_child[q][kRecMass] > 0.0) total = dadd(total, s_val[q][lane]);
+        r[4 + lane] = total;
     } else {
         r[0] = cx;
         r[1] = cy;
@@ -359,7 +412,7 @@ cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, 
     for (int d = n_levels - 1; d >= 0; --d) {
         const int lb = level_off_host[d], le = level_off_host[d + 1];
         if (le <= lb) continue;
-        fmm_m2m_kernel<<<(le - lb + wpb - 1) / wpb, kMomBlock, 0, st>>>(a, lb, le);
+        fmm_m2m_kernel<<<le - lb, 256, 0, st>>>(a, lb);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -12,14 +12,14 @@
 //   3. a stable radix sort of (key, body): depth-first tree order;
 //   4. one CTA walks the levels: a node with more than leaf_capacity bodies splits into 8
 //      children whose body ranges are found by binary search on the sorted keys;
-//   5. a second stable sort on (leaf rank, body) puts the bodies of every leaf in
-//      ascending index order, the order the reference's sums run in.
+//   5. one warp per leaf sorts the leaf's bodies into ascending index order, the order
+//      the reference's sums run in.
 // Nodes are numbered breadth-first.  Trees that need a split below level 21 (more than
 // leaf_capacity nearly coincident bodies) are reported back for the host builder.
 //
-// Lists: a leaf with mass > 0 walks the tree depth-first from the root with the
-// reference's tests (mass > 0, well_separated, leaf) in the reference's child order.
-// One thread per leaf; a count pass, exclusive sums, a fill pass.
+// Lists: every leaf with mass > 0 is walked with the reference's tests (mass > 0,
+// well_separated, leaf) by one warp over a shared-memory stack; a count pass, exclusive
+// sums, a fill pass and one radix sort into the reference's depth-first order.
 #include "fmm_build.cuh"
 #include "fmm.cuh"
 #include "gx_device.cuh"
@@ -35,7 +35,8 @@ namespace {
 
 constexpr int kBboxThreads = 256;
 constexpr int kBuildThreads = 1024;
-constexpr int kWalkThreads = 128;
+constexpr int kWalkThreads = 128;  // 4 warps, one leaf each
+constexpr int kWalkStack = 2048;   // shared stack slots per warp
 constexpr int kStack = 7 * (kKeyLevels + 1) + 8;
 
 __global__ void __launch_bounds__(kBboxThreads) bbox_partial_kernel(const TreeBuildArgs t) {
@@ -68,16 +69,34 @@ __global__ void __launch_bounds__(kBboxThreads) bbox_partial_kernel(const TreeBu
     }
 }
 
-// Root cell (fmm_solver.cpp:62-85), one thread.
-__global__ void bbox_final_kernel(const TreeBuildArgs t, int blocks) {
+// Root cell (fmm_solver.cpp:62-85): one block reduces the partial extrema.
+__global__ void __launch_bounds__(kBboxThreads) bbox_final_kernel(const TreeBuildArgs t, int blocks) {
     double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-    for (int b = 0; b < blocks; ++b)
+    for (int b = threadIdx.x; b < blocks; b += kBboxThreads)
         for (int c = 0; c < 3; ++c) {
             lo[c] = fmin(lo[c], t.part[b * 6 + c]);
             hi[c] = fmax(hi[c], t.part[b * 6 + 3 + c]);
         }
-    for (int c = 0; c < 3; ++c) t.root[c] = dmul(dadd(lo[c], hi[c]), 0.5);
-    double hw = dmul(0.5, fmax(fmax(dsub(hi[0], lo[0]), dsub(hi[1], lo[1])), dsub(hi[2], lo[2])));
+    __shared__ double s[6][kBboxThreads / 32];
+    for (int c = 0; c < 3; ++c) {
+        lo[c] = warp_min(lo[c]);
+        hi[c] = warp_max(hi[c]);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int c = 0; c < 3; ++c) {
+            s[c][w] = lo[c];
+            s[3 + c][w] = hi[c];
+        }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int c = 0; c < 3; ++c)
+        for (int k = 1; k < kBboxThreads / 32; ++k) {
+            s[c][0] = fmin(s[c][0], s[c][k]);
+            s[3 + c][0] = fmax(s[3 + c][0], s[3 + c][k]);
+        }
+    for (int c = 0; c < 3; ++c) t.root[c] = dmul(dadd(s[c][0], s[3 + c][0]), 0.5);
+    double hw = dmul(0.5, fmax(fmax(dsub(s[3][0], s[0][0]), dsub(s[4][0], s[1][0])), dsub(s[5][0], s[2][0])));
     hw = fmax(hw, dadd(t.softening, 1.0e-6));
     t.root[3] = dmul(hw, 1.0001);
 }
@@ -119,11 +138,15 @@ __device__ __forceinline__ int lower_octant(const uint64_t* keys, int b, int e, 
     return b;
 }
 
-// One CTA builds the whole topology level by level.
+// One CTA builds the whole topology level by level; 8 threads per node, thread c finds
+// where octant c starts in the node's sorted range.
 __global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBuildArgs t, const uint64_t* keys) {
+    constexpr int kNodesPerPass = kBuildThreads / 8;
     __shared__ int s_warp[kBuildThreads / 32];
+    __shared__ int s_bound[kNodesPerPass][9];
     __shared__ int s_over;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int j = tid >> 3, c = tid & 7;
     if (tid == 0) {
         t.beg[0] = 0;
         t.end[0] = t.n;
@@ -139,15 +162,23 @@ __global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBui
     int lb = 0, le = 1, L = 0;
     while (lb < le) {
         int next = le;
-        for (int k0 = lb; k0 < le; k0 += kBuildThreads) {
-            const int k = k0 + tid;
-            int split = 0;
-            if (k < le && t.end[k] - t.beg[k] > t.cap && L < t.max_depth) {
-                if (L >= kKeyLevels) atomicOr(&s_over, 1);
-                else split = 1;
+        for (int k0 = lb; k0 < le; k0 += kNodesPerPass) {
+            const int k = k0 + j;
+            int split = 0, b = 0, e = 0;
+            if (k < le) {
+                b = t.beg[k];
+                e = t.end[k];
+                if (e - b > t.cap && L < t.max_depth) {
+                    if (L >= kKeyLevels) {
+                        if (c == 0) atomicOr(&s_over, 1);
+                    } else {
+                        split = 1;
+                    }
+                }
             }
-            // block-wide exclusive scan of the split flags
-            int v = split;
+            // exclusive scan over the nodes of this pass (thread c == 0 carries the flag)
+            const int flag = c == 0 ? split : 0;
+            int v = flag;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int u = __shfl_up_sync(0xffffffffu, v, o);
@@ -165,31 +196,31 @@ __global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBui
                 s_warp[lane] = w;
             }
             __syncthreads();
-            const int rank = v - split + (wid > 0 ? s_warp[wid - 1] : 0);
+            const int incl = v + (wid > 0 ? s_warp[wid - 1] : 0);
+            const int rank = incl - split;  // nodes of this pass before node j that split
             const int total = s_warp[kBuildThreads / 32 - 1];
             const bool room = (int64_t)next + 8 * (int64_t)total <= (int64_t)t.capacity;
             if (!room && tid == 0) atomicOr(&s_over, 2);
+            const bool go = split && room;
+            if (go) {
+                const int sh = 3 * (kKeyLevels - 1 - L);
+                s_bound[j][c] = c == 0 ? b : lower_octant(keys, b, e, sh, c);
+                if (c == 0) s_bound[j][8] = e;
+            }
+            __syncthreads();
             if (k < le) {
-                if (split && room) {
+                if (go) {
                     const int c0 = next + 8 * rank;
-                    t.child[k] = c0;
-                    const int b = t.beg[k], e = t.end[k];
-                    const int sh = 3 * (kKeyLevels - 1 - L);
+                    if (c == 0) t.child[k] = c0;
                     const double chw = dmul(t.hw[k], 0.5);
-                    const double pcx = t.cx[k], pcy = t.cy[k], pcz = t.cz[k];
-                    int lo = b;
-                    for (int c = 0; c < 8; ++c) {
-                        const int hi = c == 7 ? e : lower_octant(keys, lo, e, sh, c + 1);
-                        t.beg[c0 + c] = lo;
-                        t.end[c0 + c] = hi;
-                        t.child[c0 + c] = -1;
-                        t.cx[c0 + c] = child_centre(pcx, chw, c & 1);
-                        t.cy[c0 + c] = child_centre(pcy, chw, c & 2);
-                        t.cz[c0 + c] = child_centre(pcz, chw, c & 4);
-                        t.hw[c0 + c] = chw;
-                        lo = hi;
-                    }
-                } else {
+                    t.beg[c0 + c] = s_bound[j][c];
+                    t.end[c0 + c] = s_bound[j][c + 1];
+                    t.child[c0 + c] = -1;
+                    t.cx[c0 + c] = child_centre(t.cx[k], chw, c & 1);
+                    t.cy[c0 + c] = child_centre(t.cy[k], chw, c & 2);
+                    t.cz[c0 + c] = child_centre(t.cz[k], chw, c & 4);
+                    t.hw[c0 + c] = chw;
+                } else if (c == 0) {
                     t.child[k] = -1;
                 }
             }
@@ -215,23 +246,22 @@ __global__ void __launch_bounds__(256) gather_perm_kernel(const int32_t* idx_sor
     if (i < n) perm[i] = idx_sorted[i];
 }
 
-// Leaf order: the first body position of every non-empty leaf.
-__global__ void __launch_bounds__(256) leaf_start_kernel(const TreeBuildArgs t, int n_nodes, int32_t* flag) {
-    const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k < n_nodes && t.child[k] < 0 && t.end[k] > t.beg[k]) flag[t.beg[k]] = 1;
-}
-
-// (rank of the body's leaf, body index): sorting these puts each leaf's bodies in
-// ascending index order (the reference's particle_indices order) and moves nothing
-// across leaves.
-__global__ void __launch_bounds__(256) leaf_key_kernel(const TreeBuildArgs t, const int32_t* rank) {
-    const int p = blockIdx.x * 256 + threadIdx.x;
-    if (p < t.n) t.keys[p] = ((uint64_t)(rank[p] - 1) << 31) | (uint64_t)t.perm[p];
-}
-
-__global__ void __launch_bounds__(256) leaf_unpack_kernel(const uint64_t* keys, int32_t* perm, int n) {
-    const int p = blockIdx.x * 256 + threadIdx.x;
-    if (p < n) perm[p] = (int32_t)(keys[p] & 0x7fffffffull);
+// Leaf order: one warp per leaf puts the leaf's bodies in ascending index order (the
+// reference's particle_indices order): each body's new place is the number of smaller
+// indices in the leaf, written to t.idx and copied back.
+__global__ void __launch_bounds__(256) leaf_sort_kernel(const TreeBuildArgs t, int n_nodes) {
+    const int w = (int)((blockIdx.x * 256u + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= n_nodes || t.child[w] >= 0) return;
+    const int b = t.beg[w], e = t.end[w];
+    if (e - b < 2) return;
+    for (int i = b + lane; i < e; i += 32) {
+        const int v = t.perm[i];
+        int r = 0;
+        for (int q = b; q < e; ++q) r += t.perm[q] < v;
+        t.idx[b + r] = v;
+    }
+    __syncwarp();
+    for (int i = b + lane; i < e; i += 32) t.perm[i] = t.idx[i];
 }
 
 __device__ __forceinline__ double node_mass(const double* rec, int k) { return rec[(size_t)k * kFmmRec + kRecMass]; }
@@ -257,58 +287,168 @@ __global__ void __launch_bounds__(256) leaf_emit_kernel(const TreeListArgs a) {
     for (int p = b; p < e; ++p) a.leaf_part[a.newpos[p]] = a.perm[p];
 }
 
-// well_separated (fmm_solver.cpp:228-241) for a source with mass > 0.
-__device__ __forceinline__ bool well_separated(const TreeListArgs& a, int t, int s) {
-    const double dx = dsub(a.cx[s], a.cx[t]), dy = dsub(a.cy[s], a.cy[t]), dz = dsub(a.cz[s], a.cz[t]);
-    const double dist = __dsqrt_rn(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
-    if (dist == 0.0) return false;
-    const double comb = dmul(2.0, dadd(a.hw[t], a.hw[s]));
-    return __ddiv_rn(comb, dist) < a.theta;
+__global__ void __launch_bounds__(256) walk_pack_kernel(const TreeListArgs a) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k >= a.n_nodes) return;
+    WalkNode w;
+    w.cx = a.cx[k];
+    w.cy = a.cy[k];
+    w.cz = a.cz[k];
+    w.hw = a.hw[k];
+    w.mass = node_mass(a.rec, k);
+    w.child = a.child[k];
+    w.beg = a.beg[k];
+    w.end = a.end[k];
+    a.wn[k] = w;
 }
 
-// build_leaf_interactions (fmm_solver.cpp:254-277) for every leaf with mass > 0.
+// One node of the walk (build_leaf_interactions, fmm_solver.cpp:254-277): 1 far, 2 near,
+// 3 expand, 0 massless; well_separated (:228-241) with the reference's operations.
+__device__ __forceinline__ int classify(const WalkNode& T, int t, const WalkNode& S, int s, double theta) {
+    if (!(S.mass > 0.0)) return 0;
+    if (s != t) {
+        const double dx = dsub(S.cx, T.cx), dy = dsub(S.cy, T.cy), dz = dsub(S.cz, T.cz);
+        const double dist = __dsqrt_rn(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
+        if (dist != 0.0 && __ddiv_rn(dmul(2.0, dadd(T.hw, S.hw)), dist) < theta) return 1;
+    }
+    return S.child < 0 ? 2 : 3;
+}
+
+// Every leaf with mass > 0, one warp each: the walk of build_leaf_interactions from the
+// root, with a shared-memory stack the warp pops 32 nodes at a time (each lane classifies
+// one node; expanded nodes push their 8 children).  The fill pass appends each far node as
+// key (leaf << 32 | first body) with the node id, and each near leaf as key
+// (leaf << 32 | leaf ordinal); one radix sort of all keys then yields every leaf's lists
+// in the reference's depth-first order (far nodes of one leaf are disjoint subtrees, so
+// depth-first order is the order of their first bodies, and leaf ordinals are
+// depth-first numbers).  When the stack would overflow, every lane finishes its share of
+// the pending nodes depth first with a private stack.
 template <bool FILL>
 __global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a) {
-    const int l = blockIdx.x * kWalkThreads + threadIdx.x;
+    constexpr int W = kWalkThreads / 32;
+    __shared__ int s_stk[W][kWalkStack];
+    __shared__ int s_pos[W][2];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int l = blockIdx.x * W + wid;
     const int n_leaves = a.start_ord[a.n];
     if (l >= n_leaves) return;
     const int t = a.leaf_node[l];
-    int stack[kStack];
-    int sp = 0;
-    stack[sp++] = 0;
-    int nf = 0, nn = 0;
+    const WalkNode T = a.wn[t];
     const int fo = FILL ? a.far_off[l] : 0, no = FILL ? a.near_off[l] : 0;
-    while (sp > 0) {
-        const int s = stack[--sp];
-        if (!(node_mass(a.rec, s) > 0.0)) continue;
-        if (s != t && well_separated(a, t, s)) {
-            if (FILL) a.far_node[fo + nf] = s;
-            ++nf;
-            continue;
+    const uint64_t lk = (uint64_t)l << 32;
+    const unsigned lt = (1u << lane) - 1u;
+    int* stk = s_stk[wid];
+    int nf = 0, nn = 0, top = 1, pend = -1;
+    long long nsrc = 0;  // count pass: bodies of the near leaves found by this lane
+    if (lane == 0) stk[0] = 0;
+    __syncwarp();
+    while (top > 0) {
+        const int take = min(32, top), base = top - take;
+        int s = -1, cls = 0;
+        WalkNode S;
+        if (lane < take) {
+            s = stk[base + lane];
+            S = a.wn[s];
+            cls = classify(T, t, S, s, a.theta);
         }
-        const int c0 = a.child[s];
-        if (c0 < 0) {
-            if (FILL) a.near_leaf[no + nn] = a.node_leaf[s];
-            ++nn;
-            continue;
+        __syncwarp();
+        top = base;
+        const unsigned mf = __ballot_sync(0xffffffffu, cls == 1);
+        const unsigned mn = __ballot_sync(0xffffffffu, cls == 2);
+        const unsigned me = __ballot_sync(0xffffffffu, cls == 3);
+        if (FILL) {
+            if (cls == 1) {
+                const int pos = fo + nf + __popc(mf & lt);
+                a.far_key[pos] = lk | (uint32_t)S.beg;
+                a.far_tmp[pos] = s;
+            }
+            if (cls == 2) a.near_key[no + nn + __popc(mn & lt)] = lk | (uint32_t)a.node_leaf[s];
+        } else if (cls == 2) {
+            nsrc += S.end - S.beg;
         }
-        for (int c = 7; c >= 0; --c) stack[sp++] = c0 + c;
+        nf += __popc(mf);
+        nn += __popc(mn);
+        const int add = 8 * __popc(me);
+        if (top + add > kWalkStack) {
+            pend = cls == 3 ? S.child : -1;
+            break;
+        }
+        if (cls == 3) {
+            const int at = top + 8 * __popc(me & lt);
+            for (int c = 0; c < 8; ++c) stk[at + c] = S.child + 7 - c;
+        }
+        top += add;
+        __syncwarp();
     }
-    if (FILL) return;
-    a.far_cnt[l] = nf;
-    a.near_cnt[l] = nn;
-    // far-field work items: only leaves with a target in range
-    const int tb = a.leaf_off[l], te = a.leaf_off[l + 1];
-    bool any = false;
-    for (int k = tb; k < te && !any; ++k) any = a.leaf_part[k] >= a.t_begin && a.leaf_part[k] < a.t_end;
-    const int nch = (any && nf > 0) ? (nf + kM2PChunk - 1) / kM2PChunk : 0;
-    const int slots = nch > 1 ? nch * (te - tb) : 0;
-    a.item_cnt[l] = nch;
-    a.slot_cnt[l] = slots;
-    atomicAdd(&a.totals[0], (unsigned long long)nf);
-    atomicAdd(&a.totals[1], (unsigned long long)nn);
-    atomicAdd(&a.totals[2], (unsigned long long)nch);
-    atomicAdd(&a.totals[3], (unsigned long long)slots);
+    if (top > 0 || __any_sync(0xffffffffu, pend >= 0)) {
+        // overflow: each lane walks its pending children and its share of the stack
+        if (lane == 0) {
+            s_pos[wid][0] = nf;
+            s_pos[wid][1] = nn;
+        }
+        __syncwarp();
+        int lf = 0, ln = 0;
+        int st[kStack];
+        for (int i = lane - 32; i < top; i += 32) {
+            int sp = 0;
+            if (i < 0) {
+                if (pend < 0) continue;
+                for (int c = 7; c >= 0; --c) st[sp++] = pend + c;
+            } else {
+                st[sp++] = stk[i];
+            }
+            while (sp > 0) {
+                const int s = st[--sp];
+                const WalkNode S = a.wn[s];
+                const int cls = classify(T, t, S, s, a.theta);
+                if (cls == 1) {
+                    if (FILL) {
+                        const int pos = fo + atomicAdd(&s_pos[wid][0], 1);
+                        a.far_key[pos] = lk | (uint32_t)S.beg;
+                        a.far_tmp[pos] = s;
+                    }
+                    ++lf;
+                } else if (cls == 2) {
+                    if (FILL) a.near_key[no + atomicAdd(&s_pos[wid][1], 1)] = lk | (uint32_t)a.node_leaf[s];
+                    else nsrc += S.end - S.beg;
+                    ++ln;
+                } else if (cls == 3) {
+                    for (int c = 7; c >= 0; --c) st[sp++] = S.child + c;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lf += __shfl_xor_sync(0xffffffffu, lf, o);
+            ln += __shfl_xor_sync(0xffffffffu, ln, o);
+        }
+        nf += lf;
+        nn += ln;
+    }
+    if constexpr (!FILL) {
+        for (int o = 16; o > 0; o >>= 1) nsrc += __shfl_xor_sync(0xffffffffu, nsrc, o);
+        if (lane != 0) return;
+        a.far_cnt[l] = nf;
+        a.near_cnt[l] = nn;
+        // far-field work items: only leaves with a target in range
+        const int tb = a.leaf_off[l], te = a.leaf_off[l + 1];
+        bool any = false;
+        for (int k = tb; k < te && !any; ++k) any = a.leaf_part[k] >= a.t_begin && a.leaf_part[k] < a.t_end;
+        const int nch = (any && nf > 0) ? (nf + kM2PChunk - 1) / kM2PChunk : 0;
+        const int slots = nch > 1 ? nch * (te - tb) : 0;
+        a.item_cnt[l] = nch;
+        a.slot_cnt[l] = slots;
+        atomicAdd(&a.totals[0], (unsigned long long)nf);
+        atomicAdd(&a.totals[1], (unsigned long long)nn);
+        atomicAdd(&a.totals[2], (unsigned long long)nch);
+        atomicAdd(&a.totals[3], (unsigned long long)slots);
+        atomicAdd(&a.totals[4], (unsigned long long)nf * (unsigned long long)(te - tb));
+        atomicAdd(&a.totals[5], (unsigned long long)nsrc * (unsigned long long)(te - tb));
+    }
+}
+
+__global__ void __launch_bounds__(256) near_unpack_kernel(const uint64_t* keys, int32_t* out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i < n) out[i] = (int32_t)(keys[i] & 0xffffffffull);
 }
 
 __global__ void __launch_bounds__(256) items_kernel(const TreeListArgs a, int n_leaves) {
@@ -338,25 +478,17 @@ size_t scan_bytes(int count) {
 
 }  // namespace
 
-int leaf_key_bits(int32_t n) {
-    int b = 1;
-    while (b < 31 && (1ll << b) <= (long long)n) ++b;
-    return 31 + b;
-}
-
 size_t tree_build_temp_bytes(int32_t n) {
-    size_t b = 0, c = 0, d = 0;
+    size_t b = 0;
     cub::DoubleBuffer<uint64_t> k(nullptr, nullptr);
     cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
     cub::DeviceRadixSort::SortPairs(nullptr, b, k, v, n, 0, 3 * kKeyLevels);
-    cub::DeviceRadixSort::SortKeys(nullptr, c, k, n, 0, leaf_key_bits(n));
-    cub::DeviceScan::InclusiveSum(nullptr, d, (const int32_t*)nullptr, (int32_t*)nullptr, n);
-    return std::max(b, std::max(c, d));
+    return b;
 }
 
 cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st) {
     bbox_partial_kernel<<<kBboxBlocks, kBboxThreads, 0, st>>>(t);
-    bbox_final_kernel<<<1, 1, 0, st>>>(t, kBboxBlocks);
+    bbox_final_kernel<<<1, kBboxThreads, 0, st>>>(t, kBboxBlocks);
     keys_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -371,19 +503,9 @@ cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_by
 
 cudaError_t launch_tree_leaf_order(const TreeBuildArgs& t, int32_t n_nodes, void* temp, size_t temp_bytes,
                                    cudaStream_t st) {
-    cudaError_t e;
-    // t.idx is free after the first sort: leaf-start flags, then their inclusive sum in place
-    if ((e = cudaMemsetAsync(t.idx, 0, (size_t)t.n * sizeof(int32_t), st)) != cudaSuccess) return e;
-    leaf_start_kernel<<<(n_nodes + 255) / 256, 256, 0, st>>>(t, n_nodes, t.idx);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    size_t tb = temp_bytes;
-    if ((e = cub::DeviceScan::InclusiveSum(temp, tb, t.idx, t.idx, t.n, st)) != cudaSuccess) return e;
-    leaf_key_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, t.idx);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    cub::DoubleBuffer<uint64_t> k(t.keys, t.keys_alt);
-    tb = temp_bytes;
-    if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, k, t.n, 0, leaf_key_bits(t.n), st)) != cudaSuccess) return e;
-    leaf_unpack_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(k.Current(), t.perm, t.n);
+    (void)temp;
+    (void)temp_bytes;
+    leaf_sort_kernel<<<(n_nodes + 7) / 8, 256, 0, st>>>(t, n_nodes);
     return cudaGetLastError();
 }
 
@@ -398,7 +520,7 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     if ((e = cudaMemsetAsync(a.keep, 0, nb, st)) != cudaSuccess) return e;
     for (int32_t* p : {a.far_cnt, a.near_cnt, a.item_cnt, a.slot_cnt})
         if ((e = cudaMemsetAsync(p, 0, lb, st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(a.totals, 0, 4 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.totals, 0, 6 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
     const int gn = (a.n_nodes + 255) / 256;
     leaf_mark_kernel<<<gn, 256, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -407,7 +529,8 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     tb = temp_bytes;
     if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.keep, a.newpos, a.n + 1, st)) != cudaSuccess) return e;
     leaf_emit_kernel<<<gn, 256, 0, st>>>(a);
-    walk_kernel<false><<<(a.n_nodes + kWalkThreads - 1) / kWalkThreads, kWalkThreads, 0, st>>>(a);
+    walk_pack_kernel<<<gn, 256, 0, st>>>(a);
+    walk_kernel<false><<<(a.n_nodes + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int32_t* cnt[4] = {a.far_cnt, a.near_cnt, a.item_cnt, a.slot_cnt};
     int32_t* off[4] = {a.far_off, a.near_off, a.item_off, a.slot_off};
@@ -418,9 +541,44 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     return cudaSuccess;
 }
 
-cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st) {
+int list_key_bits(int32_t n_leaves) {
+    int b = 1;
+    while (b < 31 && (1ll << b) <= (long long)n_leaves) ++b;
+    return 32 + b;
+}
+
+size_t tree_list_sort_bytes(int64_t n_far, int64_t n_near, int32_t n_leaves) {
+    size_t b = 0, c = 0;
+    cub::DoubleBuffer<uint64_t> k(nullptr, nullptr);
+    cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
+    cub::DeviceRadixSort::SortPairs(nullptr, b, k, v, (int)n_far, 0, list_key_bits(n_leaves));
+    cub::DeviceRadixSort::SortKeys(nullptr, c, k, (int)n_near, 0, list_key_bits(n_leaves));
+    return std::max(b, c);
+}
+
+cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, int64_t n_far, int64_t n_near, void* temp,
+                                   size_t temp_bytes, cudaStream_t st) {
     if (n_leaves == 0) return cudaSuccess;
-    walk_kernel<true><<<(n_leaves + kWalkThreads - 1) / kWalkThreads, kWalkThreads, 0, st>>>(a);
+    walk_kernel<true><<<(n_leaves + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int bits = list_key_bits(n_leaves);
+    if (n_far > 0) {
+        cub::DoubleBuffer<uint64_t> k(a.far_key, a.far_key_alt);
+        cub::DoubleBuffer<int32_t> v(a.far_tmp, a.far_node);
+        size_t tb = temp_bytes;
+        if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, k, v, (int)n_far, 0, bits, st)) != cudaSuccess) return e;
+        if (v.Current() != a.far_node &&
+            (e = cudaMemcpyAsync(a.far_node, v.Current(), (size_t)n_far * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                 st)) != cudaSuccess)
+            return e;
+    }
+    if (n_near > 0) {
+        cub::DoubleBuffer<uint64_t> k(a.near_key, a.near_key_alt);
+        size_t tb = temp_bytes;
+        if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, k, (int)n_near, 0, bits, st)) != cudaSuccess) return e;
+        near_unpack_kernel<<<(unsigned)((n_near + 255) / 256), 256, 0, st>>>(k.Current(), a.near_leaf, n_near);
+    }
     items_kernel<<<(n_leaves + 255) / 256, 256, 0, st>>>(a, n_leaves);
     return cudaGetLastError();
 }

@@ -40,9 +40,18 @@ struct TreeBuildArgs {
 };
 size_t tree_build_temp_bytes(int32_t n);
 cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st);
-// After a successful build: bodies of every leaf in ascending index order in t.perm.
+// After a successful build: bodies of every leaf in ascending index order in t.perm
+// (uses t.idx as scratch).
 cudaError_t launch_tree_leaf_order(const TreeBuildArgs& t, int32_t n_nodes, void* temp, size_t temp_bytes,
                                    cudaStream_t st);
+
+// What the list walk reads of a node, packed (56 B).
+struct WalkNode {
+    double cx, cy, cz, hw;
+    double mass;
+    int32_t child;
+    int32_t beg, end;
+};
 
 // Leaves with mass > 0 (depth-first) and their near / far lists, after the node moments.
 struct TreeListArgs {
@@ -57,6 +66,7 @@ struct TreeListArgs {
     const double* cz;
     const double* hw;
     const double* rec;  // node records (mass at slot 3)
+    WalkNode* wn;       // n_nodes, filled before the walk
     double theta;
     int64_t t_begin, t_end;
     // body-position scratch, n + 1 each
@@ -78,8 +88,13 @@ struct TreeListArgs {
     int32_t* near_off;
     int32_t* item_off;
     int32_t* slot_off;
-    unsigned long long* totals;  // 4: far, near, items, slots as 64-bit sums (overflow check)
-    // outputs of the fill pass
+    unsigned long long* totals;  // 6: far, near, items, slots (overflow check), far and near body pairs
+    // fill pass: unsorted lists as sort keys (leaf << 32 | order key), then the sorted lists
+    uint64_t* far_key;  // order key: first body of the far node
+    uint64_t* far_key_alt;
+    int32_t* far_tmp;   // node ids beside far_key
+    uint64_t* near_key;  // order key: leaf ordinal of the near leaf
+    uint64_t* near_key_alt;
     int32_t* far_node;
     int32_t* near_leaf;
     void* items;  // M2PItem
@@ -87,7 +102,9 @@ struct TreeListArgs {
 size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes);
 // Leaf compaction, the count walk and the offsets (sizes become known on the host after it).
 cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
-// The fill walk and the far-field work items.
-cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st);
+// The fill walk, the sort of every leaf's lists into depth-first order, the far-field work items.
+size_t tree_list_sort_bytes(int64_t n_far, int64_t n_near, int32_t n_leaves);
+cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, int64_t n_far, int64_t n_near, void* temp,
+                                   size_t temp_bytes, cudaStream_t st);
 
 }  // namespace gx

@@ -32,10 +32,18 @@ class FmmOptions:
 
 @dataclass
 class FmmStats:
+    """FmmStats of the reference, plus the body-pair counts of the far and near fields and
+    the number of tree levels."""
     node_count: int = 0
     leaf_count: int = 0
     far_interactions: int = 0
     near_interactions: int = 0
+    far_pairs: int = 0
+    near_pairs: int = 0
+    tree_levels: int = 0
+
+
+PHASES = ("tree", "moments", "lists", "far_field", "near_field")
 
 
 def fmm_accelerations(x, y, z, m, ax, ay, az, params: PhysicsParams, options: FmmOptions | None = None,
@@ -47,7 +55,25 @@ def fmm_accelerations(x, y, z, m, ax, ay, az, params: PhysicsParams, options: Fm
     _ffi.call("gx_fmm_accel", n, ptr(x), ptr(y), ptr(z), ptr(m), params.ffi(), options.ffi(),
               _ffi.precision_code(precision), int(begin), int(n if end is None else end), ptr(ax), ptr(ay), ptr(az),
               ctypes.byref(st), _ffi.stream_ptr(stream))
-    return FmmStats(st.node_count, st.leaf_count, st.far_interactions, st.near_interactions)
+    return _stats(st)
+
+
+def _stats(st) -> FmmStats:
+    return FmmStats(st.node_count, st.leaf_count, st.far_interactions, st.near_interactions, st.far_pairs,
+                    st.near_pairs, st.tree_levels)
+
+
+def fmm_accelerations_timed(x, y, z, m, ax, ay, az, params: PhysicsParams, options: FmmOptions | None = None,
+                            precision=PRECISION_F64, begin: int = 0, end: int | None = None, stream=None):
+    """fmm_accelerations plus {phase: device milliseconds} for PHASES (synchronizes)."""
+    options = options or FmmOptions()
+    n = len(x)
+    st = _ffi.FmmStatsStruct()
+    ms = (ctypes.c_double * len(PHASES))()
+    _ffi.call("gx_fmm_accel_timed", n, ptr(x), ptr(y), ptr(z), ptr(m), params.ffi(), options.ffi(),
+              _ffi.precision_code(precision), int(begin), int(n if end is None else end), ptr(ax), ptr(ay), ptr(az),
+              ctypes.byref(st), _ffi.stream_ptr(stream), ctypes.addressof(ms))
+    return _stats(st), dict(zip(PHASES, list(ms)))
 
 
 class FastMultipoleSolver:

@@ -184,12 +184,17 @@ typedef struct gx_fmm_options {
     int32_t expansion_order;
 } gx_fmm_options;
 
-/* FmmStats (fmm_solver.hpp:22-27). */
+/* FmmStats (fmm_solver.hpp:22-27), then three counts of this engine: far_pairs = sum over
+ * leaves of (bodies x far nodes), near_pairs = sum over leaves of (bodies x bodies of
+ * its near leaves, itself included), tree_levels = depth of the octree + 1. */
 typedef struct gx_fmm_stats {
     int64_t node_count;
     int64_t leaf_count;
     int64_t far_interactions;
     int64_t near_interactions;
+    int64_t far_pairs;
+    int64_t near_pairs;
+    int64_t tree_levels;
 } gx_fmm_stats;
 
 /* compute_fmm_accelerations_for_targets (fmm_solver.cpp:324-333); begin = 0, end = n is
@@ -202,6 +207,16 @@ typedef struct gx_fmm_stats {
 int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,
                  gx_physics phys, gx_fmm_options opt, int precision, int64_t begin, int64_t end,
                  double* ax, double* ay, double* az, gx_fmm_stats* stats, void* stream);
+
+/* gx_fmm_accel that also reports where the device time went: phase_ms[GX_FMM_PHASES]
+ * receives, from CUDA events on `stream`, the octree build (host clock when the host
+ * builder ran), the node moments, the interaction lists, the far field and the near
+ * field, in milliseconds.  Synchronizes the stream.  No reference counterpart. */
+#define GX_FMM_PHASES 5
+int gx_fmm_accel_timed(int64_t n, const double* x, const double* y, const double* z,
+                       const double* m, gx_physics phys, gx_fmm_options opt, int precision,
+                       int64_t begin, int64_t end, double* ax, double* ay, double* az,
+                       gx_fmm_stats* stats, void* stream, double* phase_ms);
 
 /* Node data of the reference octree (p2m_m2m / compute_multipole_moments,
  * fmm_solver.cpp:157-208), computed on the device: for every node with mass > 0, numbered

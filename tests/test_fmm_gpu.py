@@ -231,3 +231,30 @@ def test_deep_tree_uses_host_builder():
     ref = oracle.ref_fmm(p.x, p.y, p.z, p.m, 1.0, 0.02, 0.6, 16)
     a, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
     assert rel_err(a, ref).max() <= 1e-12
+
+
+@pytest.mark.parametrize("n,cap", [(20000, 64), (8000, 16)])
+def test_pair_counts_and_phase_timing(n, cap):
+    """far_pairs / near_pairs match sums over the host-built lists; the timed entry point
+    returns the same accelerations with positive phase times."""
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 41 + cap, 0.02)
+    L = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, cap)
+    a, st = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, cap)
+    assert st.near_pairs == L.n_pairs and st.far_pairs > 0 and st.tree_levels >= 2
+    assert st.near_interactions == len(L.near_leaves) and st.far_interactions == L.n_far
+    b = [np.zeros(n) for _ in range(3)]
+    st2, ms = gx.fmm.fmm_accelerations_timed(p.x, p.y, p.z, p.m, *b, gx.PhysicsParams(1.0, 0.02), gx.FmmOptions(0.6, cap))
+    assert np.array_equal(np.stack(b, 1), a) and st2 == st
+    assert set(ms) == set(gx.fmm.PHASES) and all(v > 0.0 for v in ms.values())
+
+
+@need_ref
+def test_pair_counts_host_builder():
+    """The host builder (taken for trees deeper than 21 levels) reports the same counts as
+    sums over its lists."""
+    p = gx.ics.two_disk_encounter(2000, 2000, 43, 0.02)
+    for k in range(100, 140):
+        p.x[k], p.y[k], p.z[k] = p.x[99], p.y[99], p.z[99]
+    L = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
+    _, st = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
+    assert st.near_pairs == L.n_pairs and st.far_interactions == L.n_far and st.tree_levels > 22
