@@ -17,8 +17,10 @@
 //
 // Inside an item: a warp scan of the near leaves' sizes lets every thread gather its own
 // slots of the chunk (by index, from the SoA state) into shared memory JT at a time.  In the
-// fast forms each target is served by L adjacent lanes (L = 8, 4, 2, 1 for leaves of <= 16,
-// 32, 64, more bodies) that split the staged sources and are combined with warp shuffles.
+// fast forms every thread serves two targets (halving the shared-memory reads per
+// interaction): a leaf's targets form H rows of two, each row gets L = block / H threads
+// that split the staged sources (any L, so a 22-body leaf keeps 121 of 128 threads busy),
+// and a row's L partial sums are added in lane order.
 // The exact form uses one chunk per leaf and one lane per target and walks the sources in
 // the reference's order starting from the incoming acceleration (the far field), which
 // makes it bit-identical to the reference's evaluate_particle.
@@ -34,10 +36,6 @@ constexpr int kNearBatch = 256;  // near leaves whose (start, length) sit in sha
 constexpr int kMaxChunks = 8;    // a leaf's source sequence is split into at most this many items
 constexpr int kMinChunk = 2048;  // ... of at least this many sources
 constexpr int kScanBlock = 1024;
-
-__device__ __forceinline__ int lanes_for(int nt) {
-    return nt <= 16 ? 8 : nt <= 32 ? 4 : nt <= 64 ? 2 : 1;
-}
 
 // Per leaf: number of sources, number of chunks, scratch demand (split leaves only).
 __global__ void p2p_count_kernel(const P2PArgs a, int exact) {
@@ -127,6 +125,7 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
     __shared__ int sidx[kP2PJT];
     __shared__ int s_beg[kNearBatch];
     __shared__ int s_pre[kNearBatch + 1];
+    __shared__ double s_red[6][kP2PBlock];
     __shared__ int s_item, s_last;
 
     const int tid = threadIdx.x;
@@ -155,108 +154,32 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
         const int tb = a.leaf_off[leaf];
         const int nt = a.leaf_off[leaf + 1] - tb;
         const int nb = a.near_off[leaf], ne = a.near_off[leaf + 1];
-        const int L = (MODE == kF64Exact) ? 1 : lanes_for(nt);
-        const int slots = kP2PBlock / L;
-        const int slot = tid / L, lane = tid % L;
         // Origin of the mixed form: the leaf's first body (near sources are close to it).
         const int first = a.leaf_part[tb];
         const double ox = a.x[first], oy = a.y[first], oz = a.z[first];
 
-        for (int pass = 0; pass * slots < nt; ++pass) {
-            const int t = pass * slots + slot;
-            const int i = t < nt ? a.leaf_part[tb + t] : first;
-            const bool ok = t < nt && i >= a.t_begin && i < a.t_end;
-            const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
-            const float xf = __double2float_rn(xi - ox), yf = __double2float_rn(yi - oy),
-                        zf = __double2float_rn(zi - oz);
-            double fx = 0.0, fy = 0.0, fz = 0.0;
-            if (MODE == kF64Exact && ok) {
-                fx = a.ax[i];
-                fy = a.ay[i];
-                fz = a.az[i];
+        auto stage = [&](int c, int j) {
+            sidx[c] = j;
+            if (MODE == kMixed) {
+                float* sxf = reinterpret_cast<float*>(sxd);
+                float* syf = reinterpret_cast<float*>(syd);
+                float* szf = reinterpret_cast<float*>(szd);
+                float* smf = reinterpret_cast<float*>(smd);
+                sxf[c] = __double2float_rn(a.x[j] - ox);
+                syf[c] = __double2float_rn(a.y[j] - oy);
+                szf[c] = __double2float_rn(a.z[j] - oz);
+                smf[c] = __double2float_rn(a.m[j]);
+            } else {
+                sxd[c] = a.x[j];
+                syd[c] = a.y[j];
+                szd[c] = a.z[j];
+                smd[c] = a.m[j];
             }
-            CompF cx, cy, cz;
-            cx.init();
-            cy.init();
-            cz.init();
-
-            auto compute = [&](int cnt) {
-                if (MODE == kF64Exact) {
-                    for (int jj = 0; jj < cnt; ++jj) {
-                        if (sidx[jj] == i) continue;
-                        const double rx = dsub(sxd[jj], xi), ry = dsub(syd[jj], yi), rz = dsub(szd[jj], zi);
-                        const double s2 = dadd(dadd(dadd(dmul(rx, rx), dmul(ry, ry)), dmul(rz, rz)), a.eps2);
-                        if (s2 == 0.0) {
-                            fx = dadd(fx, 0.0);
-                            fy = dadd(fy, 0.0);
-                            fz = dadd(fz, 0.0);
-                            continue;
-                        }
-                        const double inv = __ddiv_rn(1.0, __dsqrt_rn(s2));
-                        const double inv3 = dmul(dmul(inv, inv), inv);
-                        const double scale = dmul(dmul(a.G, smd[jj]), inv3);
-                        fx = dadd(fx, dmul(rx, scale));
-                        fy = dadd(fy, dmul(ry, scale));
-                        fz = dadd(fz, dmul(rz, scale));
-                    }
-                } else if (MODE == kF64) {
-#pragma unroll 4
-                    for (int jj = lane; jj < cnt; jj += L) {
-                        const double dx = sxd[jj] - xi, dy = syd[jj] - yi, dz = szd[jj] - zi;
-                        double r = fma(dx, dx, a.eps2);
-                        r = fma(dy, dy, r);
-                        r = fma(dz, dz, r);
-                        double y = rsqrt_f64(r);
-                        if (EPS0) y = (r == 0.0 || sidx[jj] == i) ? 0.0 : y;
-                        const double w = smd[jj] * (y * y * y);
-                        fx = fma(dx, w, fx);
-                        fy = fma(dy, w, fy);
-                        fz = fma(dz, w, fz);
-                    }
-                } else {
-                    float px = 0.f, py = 0.f, pz = 0.f;
-                    const float* sxf = reinterpret_cast<const float*>(sxd);
-                    const float* syf = reinterpret_cast<const float*>(syd);
-                    const float* szf = reinterpret_cast<const float*>(szd);
-                    const float* smf = reinterpret_cast<const float*>(smd);
-#pragma unroll 4
-                    for (int jj = lane; jj < cnt; jj += L) {
-                        const float dx = sxf[jj] - xf, dy = syf[jj] - yf, dz = szf[jj] - zf;
-                        float r = fmaf(dx, dx, a.eps2f);
-                        r = fmaf(dy, dy, r);
-                        r = fmaf(dz, dz, r);
-                        float iv = rsqrt_f32(r);
-                        if (EPS0) iv = (r == 0.f || sidx[jj] == i) ? 0.f : iv;
-                        const float w = smf[jj] * (iv * iv * iv);
-                        px = fmaf(dx, w, px);
-                        py = fmaf(dy, w, py);
-                        pz = fmaf(dz, w, pz);
-                    }
-                    cx.add(px);
-                    cy.add(py);
-                    cz.add(pz);
-                }
-            };
-            auto stage = [&](int c, int j) {
-                sidx[c] = j;
-                if (MODE == kMixed) {
-                    float* sxf = reinterpret_cast<float*>(sxd);
-                    float* syf = reinterpret_cast<float*>(syd);
-                    float* szf = reinterpret_cast<float*>(szd);
-                    float* smf = reinterpret_cast<float*>(smd);
-                    sxf[c] = __double2float_rn(a.x[j] - ox);
-                    syf[c] = __double2float_rn(a.y[j] - oy);
-                    szf[c] = __double2float_rn(a.z[j] - oz);
-                    smf[c] = __double2float_rn(a.m[j]);
-                } else {
-                    sxd[c] = a.x[j];
-                    syd[c] = a.y[j];
-                    szd[c] = a.z[j];
-                    smd[c] = a.m[j];
-                }
-            };
-
-            // Walk the near list in batches; stage only the slots of this item's chunk.
+        };
+        // Every source slot [c_lo, c_hi) of this item staged kP2PJT at a time, compute(take)
+        // after each: the near list is walked in batches, a warp scan of the near leaves'
+        // sizes lets every thread gather its own slots by index.
+        auto sweep = [&](auto&& compute) {
             int64_t base = 0;  // slots before the current near batch
             for (int qb = nb; qb < ne && base < c_hi; qb += kNearBatch) {
                 const int cnt = min(kNearBatch, ne - qb);
@@ -305,40 +228,159 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
                 base += total;
                 __syncthreads();  // s_beg / s_pre are rewritten by the next batch
             }
+        };
 
-            if (MODE == kF64Exact) {
+        if constexpr (MODE == kF64Exact) {
+            // One target per thread, sources in the reference's order, starting from the
+            // incoming acceleration (the far field).
+            for (int t0 = 0; t0 < nt; t0 += kP2PBlock) {
+                const int t = t0 + tid;
+                const int i = t < nt ? a.leaf_part[tb + t] : first;
+                const bool ok = t < nt && i >= a.t_begin && i < a.t_end;
+                const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
+                double fx = 0.0, fy = 0.0, fz = 0.0;
+                if (ok) {
+                    fx = a.ax[i];
+                    fy = a.ay[i];
+                    fz = a.az[i];
+                }
+                sweep([&](int cnt) {
+                    for (int jj = 0; jj < cnt; ++jj) {
+                        if (sidx[jj] == i) continue;
+                        const double rx = dsub(sxd[jj], xi), ry = dsub(syd[jj], yi), rz = dsub(szd[jj], zi);
+                        const double s2 = dadd(dadd(dadd(dmul(rx, rx), dmul(ry, ry)), dmul(rz, rz)), a.eps2);
+                        if (s2 == 0.0) {
+                            fx = dadd(fx, 0.0);
+                            fy = dadd(fy, 0.0);
+                            fz = dadd(fz, 0.0);
+                            continue;
+                        }
+                        const double inv = __ddiv_rn(1.0, __dsqrt_rn(s2));
+                        const double inv3 = dmul(dmul(inv, inv), inv);
+                        const double scale = dmul(dmul(a.G, smd[jj]), inv3);
+                        fx = dadd(fx, dmul(rx, scale));
+                        fy = dadd(fy, dmul(ry, scale));
+                        fz = dadd(fz, dmul(rz, scale));
+                    }
+                });
                 if (ok) {
                     a.ax[i] = fx;
                     a.ay[i] = fy;
                     a.az[i] = fz;
                 }
-                continue;
             }
-            if (MODE == kMixed) {
-                fx = cx.value();
-                fy = cy.value();
-                fz = cz.value();
-            }
-            // Combine the L lanes of this target (adjacent lanes of one warp).
-            for (int o = L >> 1; o > 0; o >>= 1) {
-                fx += __shfl_xor_sync(0xffffffffu, fx, o);
-                fy += __shfl_xor_sync(0xffffffffu, fy, o);
-                fz += __shfl_xor_sync(0xffffffffu, fz, o);
-            }
-            if (ok && lane == 0) {
-                if (chunks == 1) {
-                    a.ax[i] = a.ax[i] + a.G * fx;
-                    a.ay[i] = a.ay[i] + a.G * fy;
-                    a.az[i] = a.az[i] + a.G * fz;
+            continue;
+        } else {
+            // Two targets per thread: the leaf's targets (up to 2 x kP2PBlock per pass) form
+            // H rows of two (row r holds targets r and r + H); every row gets L = block / H
+            // lanes that split the staged sources, and a row's L partial sums are added in
+            // lane order in shared memory.
+            for (int t0 = 0; t0 < nt; t0 += 2 * kP2PBlock) {
+                const int ntp = min(2 * kP2PBlock, nt - t0);
+                const int H = (ntp + 1) >> 1;
+                const int L = max(1, kP2PBlock / H);
+                const bool act = tid < H * L;
+                const int row = act ? tid / L : 0, lane = act ? tid - row * L : 0;
+                const bool has_b = act && row + H < ntp;
+                const int ia = a.leaf_part[tb + t0 + row];
+                const int ib = has_b ? a.leaf_part[tb + t0 + row + H] : ia;
+                const double xa = a.x[ia], ya = a.y[ia], za = a.z[ia];
+                const double xb = a.x[ib], yb = a.y[ib], zb = a.z[ib];
+                double f[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if constexpr (MODE == kF64) {
+                    sweep([&](int cnt) {
+                        if (!act) return;
+#pragma unroll 2
+                        for (int jj = lane; jj < cnt; jj += L) {
+                            const double qx = sxd[jj], qy = syd[jj], qz = szd[jj], qm = smd[jj];
+                            const double dxa = qx - xa, dya = qy - ya, dza = qz - za;
+                            const double dxb = qx - xb, dyb = qy - yb, dzb = qz - zb;
+                            const double ra = fma(dza, dza, fma(dya, dya, fma(dxa, dxa, a.eps2)));
+                            const double rb = fma(dzb, dzb, fma(dyb, dyb, fma(dxb, dxb, a.eps2)));
+                            double ya3 = rsqrt_f64(ra), yb3 = rsqrt_f64(rb);
+                            if (EPS0) {
+                                ya3 = (ra == 0.0 || sidx[jj] == ia) ? 0.0 : ya3;
+                                yb3 = (rb == 0.0 || sidx[jj] == ib) ? 0.0 : yb3;
+                            }
+                            const double wa = qm * (ya3 * ya3 * ya3), wb = qm * (yb3 * yb3 * yb3);
+                            f[0] = fma(dxa, wa, f[0]);
+                            f[1] = fma(dya, wa, f[1]);
+                            f[2] = fma(dza, wa, f[2]);
+                            f[3] = fma(dxb, wb, f[3]);
+                            f[4] = fma(dyb, wb, f[4]);
+                            f[5] = fma(dzb, wb, f[5]);
+                        }
+                    });
                 } else {
-                    const size_t k = (size_t)(a.plan_scratch[leaf] + (int64_t)chunk * nt + t) * 3;
-                    a.scratch[k] = fx;
-                    a.scratch[k + 1] = fy;
-                    a.scratch[k + 2] = fz;
+                    const float xfa = __double2float_rn(xa - ox), yfa = __double2float_rn(ya - oy),
+                                zfa = __double2float_rn(za - oz);
+                    const float xfb = __double2float_rn(xb - ox), yfb = __double2float_rn(yb - oy),
+                                zfb = __double2float_rn(zb - oz);
+                    CompF c[6];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) c[k].init();
+                    sweep([&](int cnt) {
+                        if (!act) return;
+                        const float* sxf = reinterpret_cast<const float*>(sxd);
+                        const float* syf = reinterpret_cast<const float*>(syd);
+                        const float* szf = reinterpret_cast<const float*>(szd);
+                        const float* smf = reinterpret_cast<const float*>(smd);
+                        float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+                        for (int jj = lane; jj < cnt; jj += L) {
+                            const float qx = sxf[jj], qy = syf[jj], qz = szf[jj], qm = smf[jj];
+                            const float dxa = qx - xfa, dya = qy - yfa, dza = qz - zfa;
+                            const float dxb = qx - xfb, dyb = qy - yfb, dzb = qz - zfb;
+                            const float ra = fmaf(dza, dza, fmaf(dya, dya, fmaf(dxa, dxa, a.eps2f)));
+                            const float rb = fmaf(dzb, dzb, fmaf(dyb, dyb, fmaf(dxb, dxb, a.eps2f)));
+                            float ia3 = rsqrt_f32(ra), ib3 = rsqrt_f32(rb);
+                            if (EPS0) {
+                                ia3 = (ra == 0.f || sidx[jj] == ia) ? 0.f : ia3;
+                                ib3 = (rb == 0.f || sidx[jj] == ib) ? 0.f : ib3;
+                            }
+                            const float wa = qm * (ia3 * ia3 * ia3), wb = qm * (ib3 * ib3 * ib3);
+                            p[0] = fmaf(dxa, wa, p[0]);
+                            p[1] = fmaf(dya, wa, p[1]);
+                            p[2] = fmaf(dza, wa, p[2]);
+                            p[3] = fmaf(dxb, wb, p[3]);
+                            p[4] = fmaf(dyb, wb, p[4]);
+                            p[5] = fmaf(dzb, wb, p[5]);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) c[k].add(p[k]);
+                    });
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) f[k] = c[k].value();
                 }
+                if (act)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) s_red[k][tid] = f[k];
+                __syncthreads();
+                if (act && lane == 0) {
+                    double S[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                    for (int q = 0; q < L; ++q)
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) S[k] += s_red[k][tid + q];
+                    for (int h = 0; h < (has_b ? 2 : 1); ++h) {
+                        const int t = t0 + row + h * H;
+                        const int i = h ? ib : ia;
+                        if (i < a.t_begin || i >= a.t_end) continue;
+                        if (chunks == 1) {
+                            a.ax[i] = a.ax[i] + a.G * S[3 * h];
+                            a.ay[i] = a.ay[i] + a.G * S[3 * h + 1];
+                            a.az[i] = a.az[i] + a.G * S[3 * h + 2];
+                        } else {
+                            const size_t k = (size_t)(a.plan_scratch[leaf] + (int64_t)chunk * nt + t) * 3;
+                            a.scratch[k] = S[3 * h];
+                            a.scratch[k + 1] = S[3 * h + 1];
+                            a.scratch[k + 2] = S[3 * h + 2];
+                        }
+                    }
+                }
+                __syncthreads();
             }
         }
-        if (MODE == kF64Exact || chunks == 1) continue;
+        if (chunks == 1) continue;
         // Split leaf: the CTA that completes its last chunk adds the partials in chunk order.
         __threadfence();
         __syncthreads();
