@@ -1567,19 +1567,14 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
     fa.n_items = (int32_t)tot[2];
     P.n_slots = (int64_t)tot[3];
     GX_TRY(dev_array(hs, P.n_far, &la.far_node));
-    GX_TRY(dev_array(hs, P.n_far, &la.far_key));
-    GX_TRY(dev_array(hs, P.n_far, &la.far_key_alt));
-    GX_TRY(dev_array(hs, P.n_far, &la.far_tmp));
     GX_TRY(dev_array(hs, P.n_near, &la.near_key));
-    GX_TRY(dev_array(hs, P.n_near, &la.near_key_alt));
+    GX_TRY(dev_array(hs, (int64_t)nl, &la.long_leaf));
+    GX_TRY(dev_array(hs, 1, &la.long_count));
     GX_TRY(dev_array(hs, P.n_near, &la.near_leaf));
     M2PItem* items;
     GX_TRY(dev_array(hs, fa.n_items, &items));
     la.items = items;
-    const size_t sort_list_bytes = tree_list_sort_bytes(P.n_far, P.n_near, nl);
-    void* sort_list_temp;
-    GX_TRY(dev_array(hs, (int64_t)sort_list_bytes, (char**)&sort_list_temp));
-    GX_CUDA(launch_tree_lists_fill(la, nl, P.n_far, P.n_near, sort_list_temp, sort_list_bytes, st));
+    GX_CUDA(launch_tree_lists_fill(la, nl, st));
     GX_TRY(mark(tm, 3, st));
     fa.leaf_off = la.leaf_off;
     fa.leaf_part = la.leaf_part;

@@ -30,6 +30,7 @@
 #include "gx_device.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace gx {
 namespace {
@@ -305,42 +306,79 @@ __device__ __forceinline__ void m2p_one(const double* __restrict__ r, double tx,
     fz += cd * dz + vz;
 }
 
-// Work item = (target leaf, up to kM2PChunk far nodes).  The item's node records are
-// staged in shared memory; thread t evaluates target t % W against nodes t / W,
-// t / W + S, ... (W = targets rounded up to a power of two, S = block / W); the S partial
-// sums of a target are added in slot order, so results do not depend on scheduling.
+// Shared-memory stride of a staged node record: slots 0..45 (16-byte multiple).
+constexpr int kStageStride = 46;
+constexpr int kM2PSub = 64;  // node records per shared-memory buffer
+constexpr size_t kM2PDynSmem = 2 * kM2PSub * kStageStride * sizeof(double);
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Work item = (target leaf, up to kM2PChunk far nodes).  The item's node records stream
+// through two shared-memory buffers of kM2PSub records: while the block evaluates one
+// buffer, cp.async fills the other.  Thread t evaluates target t % W against nodes t / W,
+// t / W + S, ... of each buffer (W = the leaf's targets, at most one block; S = block / W
+// node slots, so at most W - 1 threads idle); the S partial sums of a target are added in
+// slot order, so results do not depend on scheduling.
 template <int P>
 __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
-    constexpr int NEED = P == 0 ? 4 : (P == 2 ? kRecTrQ + 1 : kRecTr2 + 1);
-    __shared__ __align__(16) double s_rec[kM2PChunk * kFmmRec];
+    constexpr int PIECES = P == 0 ? 2 : (P == 2 ? (kRecTrQ + 2) / 2 : kStageStride / 2);  // 16-byte pieces
+    extern __shared__ __align__(16) double s_dyn[];
     __shared__ double s_red[kM2PBlock * 3];
     __shared__ int s_last;
     const int tid = threadIdx.x;
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
         const M2PItem w = a.items[it];
         const int cnt = w.fe - w.fb;
-        for (int k = tid; k < cnt * NEED; k += kM2PBlock) {
-            const int j = k / NEED, c = k - j * NEED;
-            s_rec[j * kFmmRec + c] = a.rec[(size_t)a.far_node[w.fb + j] * kFmmRec + c];
-        }
-        __syncthreads();
+        const int nsub = (cnt + kM2PSub - 1) / kM2PSub;
+        auto stage = [&](int sc) {
+            double* buf = s_dyn + (sc & 1) * (kM2PSub * kStageStride);
+            const int j0 = sc * kM2PSub, m = min(kM2PSub, cnt - j0);
+            for (int k = tid; k < m * PIECES; k += kM2PBlock) {
+                const int j = k / PIECES, pc = k - j * PIECES;
+                const double* src = a.rec + (size_t)a.far_node[w.fb + j0 + j] * kFmmRec + 2 * pc;
+                cp_async16(buf + j * kStageStride + 2 * pc, src);
+            }
+            cp_async_commit();
+        };
         const int tb = a.leaf_off[w.leaf], nt = a.leaf_off[w.leaf + 1] - tb;
-        int W = 1;
-        while (W < nt && W < kM2PBlock) W <<= 1;
+        const int W = min(nt, kM2PBlock);
         const int S = kM2PBlock / W;
-        const int q = tid / W, tl = tid % W;
+        const int q = tid / W, tl = tid - q * W;
         for (int t0 = 0; t0 < nt; t0 += W) {
             const int t = t0 + tl;
             double fx = 0.0, fy = 0.0, fz = 0.0;
             int i = -1;
-            if (t < nt) {
+            double tx = 0.0, ty = 0.0, tz = 0.0;
+            if (q < S && t < nt) {
                 i = a.leaf_part[tb + t];
                 if (i >= a.t_begin && i < a.t_end) {
-                    const double tx = a.x[i], ty = a.y[i], tz = a.z[i];
-                    for (int j = q; j < cnt; j += S) m2p_one<P>(s_rec + j * kFmmRec, tx, ty, tz, a.eps2, fx, fy, fz);
+                    tx = a.x[i];
+                    ty = a.y[i];
+                    tz = a.z[i];
                 } else {
                     i = -1;
                 }
+            }
+            stage(0);
+            for (int sc = 0; sc < nsub; ++sc) {
+                if (sc + 1 < nsub) {
+                    stage(sc + 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncthreads();
+                const double* buf = s_dyn + (sc & 1) * (kM2PSub * kStageStride);
+                const int m = min(kM2PSub, cnt - sc * kM2PSub);
+                if (i >= 0)
+                    for (int j = q; j < m; j += S) m2p_one<P>(buf + j * kStageStride, tx, ty, tz, a.eps2, fx, fy, fz);
+                __syncthreads();  // the next stage() overwrites this buffer
             }
             s_red[tid * 3 + 0] = fx;
             s_red[tid * 3 + 1] = fy;
@@ -395,6 +433,23 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
     }
 }
 
+template <int P>
+cudaError_t launch_m2p_order(const FmmArgs& a, cudaStream_t st) {
+    // the shared-memory opt-in is a per-device setting of the kernel
+    static std::atomic<unsigned long long> set_on{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(set_on.load() & bit)) {
+        e = cudaFuncSetAttribute(fmm_m2p_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kM2PDynSmem);
+        if (e != cudaSuccess) return e;
+        set_on.fetch_or(bit);
+    }
+    fmm_m2p_kernel<P><<<std::min(a.n_items, 1 << 20), kM2PBlock, kM2PDynSmem, st>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int fmm_effective_order(int expansion_order) {
@@ -421,13 +476,11 @@ cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, 
 
 cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st) {
     if (a.n_items == 0) return cudaSuccess;
-    const int grid = std::min(a.n_items, 1 << 20);
     switch (a.order) {
-        case 0: fmm_m2p_kernel<0><<<grid, kM2PBlock, 0, st>>>(a); break;
-        case 2: fmm_m2p_kernel<2><<<grid, kM2PBlock, 0, st>>>(a); break;
-        default: fmm_m2p_kernel<4><<<grid, kM2PBlock, 0, st>>>(a); break;
+        case 0: return launch_m2p_order<0>(a, st);
+        case 2: return launch_m2p_order<2>(a, st);
+        default: return launch_m2p_order<4>(a, st);
     }
-    return cudaGetLastError();
 }
 
 }  // namespace gx

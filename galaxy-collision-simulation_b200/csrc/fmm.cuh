@@ -64,7 +64,7 @@ struct FmmArgs {
 
 // Effective expansion order of multipole_acceleration (multipole.cpp:261-265).
 int fmm_effective_order(int expansion_order);
-constexpr int kM2PChunk = 64;  // far nodes per work item
+constexpr int kM2PChunk = 512;  // far nodes per work item
 
 // Stream-ordered: leaf moments, then one launch per level (deepest first), then M2P.
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st);

@@ -19,7 +19,7 @@
 //
 // Lists: every leaf with mass > 0 is walked with the reference's tests (mass > 0,
 // well_separated, leaf) by one warp over a shared-memory stack; a count pass, exclusive
-// sums, a fill pass and one radix sort into the reference's depth-first order.
+// sums, and a fill pass (near lists sorted into the reference's depth-first order).
 #include "fmm_build.cuh"
 #include "fmm.cuh"
 #include "gx_device.cuh"
@@ -138,12 +138,14 @@ __device__ __forceinline__ int lower_octant(const uint64_t* keys, int b, int e, 
     return b;
 }
 
-// One CTA builds the whole topology level by level; 8 threads per node, thread c finds
-// where octant c starts in the node's sorted range.
+// One CTA builds the whole topology level by level.  Per pass it classifies up to 1024 nodes
+// of the level (one per thread), compacts the ones that split, and gives each splitting node
+// 8 threads: thread c finds where octant c starts in the node's sorted range.
 __global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBuildArgs t, const uint64_t* keys) {
-    constexpr int kNodesPerPass = kBuildThreads / 8;
+    constexpr int kSplitPerSub = kBuildThreads / 8;
     __shared__ int s_warp[kBuildThreads / 32];
-    __shared__ int s_bound[kNodesPerPass][9];
+    __shared__ int s_split[kBuildThreads];
+    __shared__ int s_bound[kSplitPerSub][9];
     __shared__ int s_over;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int j = tid >> 3, c = tid & 7;
@@ -162,23 +164,16 @@ __global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBui
     int lb = 0, le = 1, L = 0;
     while (lb < le) {
         int next = le;
-        for (int k0 = lb; k0 < le; k0 += kNodesPerPass) {
-            const int k = k0 + j;
-            int split = 0, b = 0, e = 0;
-            if (k < le) {
-                b = t.beg[k];
-                e = t.end[k];
-                if (e - b > t.cap && L < t.max_depth) {
-                    if (L >= kKeyLevels) {
-                        if (c == 0) atomicOr(&s_over, 1);
-                    } else {
-                        split = 1;
-                    }
-                }
+        const int sh = 3 * (kKeyLevels - 1 - L);
+        for (int k0 = lb; k0 < le; k0 += kBuildThreads) {
+            const int k = k0 + tid;
+            int split = 0;
+            if (k < le && t.end[k] - t.beg[k] > t.cap && L < t.max_depth) {
+                if (L >= kKeyLevels) atomicOr(&s_over, 1);
+                else split = 1;
             }
-            // exclusive scan over the nodes of this pass (thread c == 0 carries the flag)
-            const int flag = c == 0 ? split : 0;
-            int v = flag;
+            // block-wide exclusive scan of the split flags
+            int v = split;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int u = __shfl_up_sync(0xffffffffu, v, o);
@@ -196,32 +191,38 @@ __global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBui
                 s_warp[lane] = w;
             }
             __syncthreads();
-            const int incl = v + (wid > 0 ? s_warp[wid - 1] : 0);
-            const int rank = incl - split;  // nodes of this pass before node j that split
+            const int rank = v - split + (wid > 0 ? s_warp[wid - 1] : 0);
             const int total = s_warp[kBuildThreads / 32 - 1];
             const bool room = (int64_t)next + 8 * (int64_t)total <= (int64_t)t.capacity;
+            if (k < le && !(split && room)) t.child[k] = -1;
+            if (split && room) s_split[rank] = k;
             if (!room && tid == 0) atomicOr(&s_over, 2);
-            const bool go = split && room;
-            if (go) {
-                const int sh = 3 * (kKeyLevels - 1 - L);
-                s_bound[j][c] = c == 0 ? b : lower_octant(keys, b, e, sh, c);
-                if (c == 0) s_bound[j][8] = e;
-            }
             __syncthreads();
-            if (k < le) {
-                if (go) {
-                    const int c0 = next + 8 * rank;
-                    if (c == 0) t.child[k] = c0;
-                    const double chw = dmul(t.hw[k], 0.5);
-                    t.beg[c0 + c] = s_bound[j][c];
-                    t.end[c0 + c] = s_bound[j][c + 1];
-                    t.child[c0 + c] = -1;
-                    t.cx[c0 + c] = child_centre(t.cx[k], chw, c & 1);
-                    t.cy[c0 + c] = child_centre(t.cy[k], chw, c & 2);
-                    t.cz[c0 + c] = child_centre(t.cz[k], chw, c & 4);
-                    t.hw[c0 + c] = chw;
-                } else if (c == 0) {
-                    t.child[k] = -1;
+            if (room) {
+                for (int q0 = 0; q0 < total; q0 += kSplitPerSub) {
+                    const int q = q0 + j;
+                    int node = -1, b = 0, e = 0;
+                    if (q < total) {
+                        node = s_split[q];
+                        b = t.beg[node];
+                        e = t.end[node];
+                        s_bound[j][c] = c == 0 ? b : lower_octant(keys, b, e, sh, c);
+                        if (c == 0) s_bound[j][8] = e;
+                    }
+                    __syncthreads();
+                    if (q < total) {
+                        const int c0 = next + 8 * q;
+                        if (c == 0) t.child[node] = c0;
+                        const double chw = dmul(t.hw[node], 0.5);
+                        t.beg[c0 + c] = s_bound[j][c];
+                        t.end[c0 + c] = s_bound[j][c + 1];
+                        t.child[c0 + c] = -1;
+                        t.cx[c0 + c] = child_centre(t.cx[node], chw, c & 1);
+                        t.cy[c0 + c] = child_centre(t.cy[node], chw, c & 2);
+                        t.cz[c0 + c] = child_centre(t.cz[node], chw, c & 4);
+                        t.hw[c0 + c] = chw;
+                    }
+                    __syncthreads();
                 }
             }
             next += 8 * total;
@@ -299,6 +300,9 @@ __global__ void __launch_bounds__(256) walk_pack_kernel(const TreeListArgs a) {
     w.child = a.child[k];
     w.beg = a.beg[k];
     w.end = a.end[k];
+    w.mask = 0;
+    if (w.child >= 0)
+        for (int c = 0; c < 8; ++c) w.mask |= (node_mass(a.rec, w.child + c) > 0.0 ? 1 : 0) << c;
     a.wn[k] = w;
 }
 
@@ -314,20 +318,54 @@ __device__ __forceinline__ int classify(const WalkNode& T, int t, const WalkNode
     return S.child < 0 ? 2 : 3;
 }
 
+// One warp sorts the distinct keys v[0 .. n) ascending and writes the low 32 bits of each to
+// out in that order: a bitonic sort in the shared buffer buf (kWalkStack / 2 slots) when the
+// list fits, else every key's rank (the number of smaller keys) computed from global memory.
+__device__ void sort_into(const uint64_t* v, int n, uint64_t* buf, int lane, int32_t* out) {
+    constexpr int kCap = kWalkStack / 2;
+    if (n <= kCap) {
+        int P = 1;
+        while (P < n) P <<= 1;
+        for (int i = lane; i < P; i += 32) buf[i] = i < n ? v[i] : ~0ull;
+        __syncwarp();
+        for (int k = 2; k <= P; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < P; i += 32) {
+                    const int m = i ^ j;
+                    if (m > i) {
+                        const uint64_t x = buf[i], y = buf[m];
+                        if ((x > y) == ((i & k) == 0)) {
+                            buf[i] = y;
+                            buf[m] = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        for (int i = lane; i < n; i += 32) out[i] = (int32_t)(uint32_t)buf[i];
+        __syncwarp();
+        return;
+    }
+    for (int i = lane; i < n; i += 32) {
+        const uint64_t key = v[i];
+        int r = 0;
+        for (int q = 0; q < n; ++q) r += v[q] < key;
+        out[r] = (int32_t)(uint32_t)key;
+    }
+}
+
 // Every leaf with mass > 0, one warp each: the walk of build_leaf_interactions from the
 // root, with a shared-memory stack the warp pops 32 nodes at a time (each lane classifies
-// one node; expanded nodes push their 8 children).  The fill pass appends each far node as
-// key (leaf << 32 | first body) with the node id, and each near leaf as key
-// (leaf << 32 | leaf ordinal); one radix sort of all keys then yields every leaf's lists
-// in the reference's depth-first order (far nodes of one leaf are disjoint subtrees, so
-// depth-first order is the order of their first bodies, and leaf ordinals are
-// depth-first numbers).  When the stack would overflow, every lane finishes its share of
+// one node; expanded nodes push their children with mass > 0).  The fill pass writes each far node
+// where the walk meets it (the far list holds the reference's nodes in the walk's own,
+// deterministic order; only the summation order of the far field depends on it) and each
+// near leaf as its ordinal, then sorts the near list into the reference's depth-first order
+// (leaf ordinals are depth-first numbers), which the near field's exact form relies on.  When the stack would overflow, every lane finishes its share of
 // the pending nodes depth first with a private stack.
 template <bool FILL>
 __global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a) {
     constexpr int W = kWalkThreads / 32;
-    __shared__ int s_stk[W][kWalkStack];
-    __shared__ int s_pos[W][2];
+    __shared__ __align__(16) int s_stk[W][kWalkStack];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int l = blockIdx.x * W + wid;
     const int n_leaves = a.start_ord[a.n];
@@ -335,10 +373,9 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a
     const int t = a.leaf_node[l];
     const WalkNode T = a.wn[t];
     const int fo = FILL ? a.far_off[l] : 0, no = FILL ? a.near_off[l] : 0;
-    const uint64_t lk = (uint64_t)l << 32;
     const unsigned lt = (1u << lane) - 1u;
     int* stk = s_stk[wid];
-    int nf = 0, nn = 0, top = 1, pend = -1;
+    int nf = 0, nn = 0, top = 1, pend = -1, pmask = 0, pchild = 0;
     long long nsrc = 0;  // count pass: bodies of the near leaves found by this lane
     if (lane == 0) stk[0] = 0;
     __syncwarp();
@@ -359,72 +396,98 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a
         if (FILL) {
             if (cls == 1) {
                 const int pos = fo + nf + __popc(mf & lt);
-                a.far_key[pos] = lk | (uint32_t)S.beg;
-                a.far_tmp[pos] = s;
+                a.far_node[pos] = s;
             }
-            if (cls == 2) a.near_key[no + nn + __popc(mn & lt)] = lk | (uint32_t)a.node_leaf[s];
+            if (cls == 2) a.near_key[no + nn + __popc(mn & lt)] = (uint32_t)a.node_leaf[s];
         } else if (cls == 2) {
             nsrc += S.end - S.beg;
         }
         nf += __popc(mf);
         nn += __popc(mn);
-        const int add = 8 * __popc(me);
+        // expanded nodes push their massive children (massless ones would be skipped anyway)
+        const int mine = cls == 3 ? __popc(S.mask) : 0;
+        int at = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, at, o);
+            if (lane >= o) at += u;
+        }
+        const int add = __shfl_sync(0xffffffffu, at, 31);
         if (top + add > kWalkStack) {
-            pend = cls == 3 ? S.child : -1;
+            pend = cls == 3 ? s : -1;
+            pmask = cls == 3 ? S.mask : 0;
+            pchild = cls == 3 ? S.child : 0;
             break;
         }
         if (cls == 3) {
-            const int at = top + 8 * __popc(me & lt);
-            for (int c = 0; c < 8; ++c) stk[at + c] = S.child + 7 - c;
+            at = top + at - mine;
+            for (int c = 7; c >= 0; --c)
+                if (S.mask >> c & 1) stk[at++] = S.child + c;
         }
         top += add;
         __syncwarp();
     }
     if (top > 0 || __any_sync(0xffffffffu, pend >= 0)) {
-        // overflow: each lane walks its pending children and its share of the stack
-        if (lane == 0) {
-            s_pos[wid][0] = nf;
-            s_pos[wid][1] = nn;
-        }
-        __syncwarp();
-        int lf = 0, ln = 0;
+        // overflow: each lane walks its pending children and its share of the stack depth
+        // first with a private stack -- once to count, and in the fill pass once more to
+        // write at the lane's place (lanes in order), so the list order is deterministic
         int st[kStack];
-        for (int i = lane - 32; i < top; i += 32) {
-            int sp = 0;
-            if (i < 0) {
-                if (pend < 0) continue;
-                for (int c = 7; c >= 0; --c) st[sp++] = pend + c;
-            } else {
-                st[sp++] = stk[i];
-            }
-            while (sp > 0) {
-                const int s = st[--sp];
-                const WalkNode S = a.wn[s];
-                const int cls = classify(T, t, S, s, a.theta);
-                if (cls == 1) {
-                    if (FILL) {
-                        const int pos = fo + atomicAdd(&s_pos[wid][0], 1);
-                        a.far_key[pos] = lk | (uint32_t)S.beg;
-                        a.far_tmp[pos] = s;
+        auto lane_walk = [&](bool write, int fpos, int npos, int& lf, int& ln) {
+            lf = ln = 0;
+            for (int i = lane - 32; i < top; i += 32) {
+                int sp = 0;
+                if (i < 0) {
+                    if (pend < 0) continue;
+                    for (int c = 7; c >= 0; --c)
+                        if (pmask >> c & 1) st[sp++] = pchild + c;
+                } else {
+                    st[sp++] = stk[i];
+                }
+                while (sp > 0) {
+                    const int s = st[--sp];
+                    const WalkNode S = a.wn[s];
+                    const int cls = classify(T, t, S, s, a.theta);
+                    if (cls == 1) {
+                        if (write) a.far_node[fpos + lf] = s;
+                        ++lf;
+                    } else if (cls == 2) {
+                        if (write) a.near_key[npos + ln] = (uint32_t)a.node_leaf[s];
+                        else nsrc += S.end - S.beg;
+                        ++ln;
+                    } else if (cls == 3) {
+                        for (int c = 7; c >= 0; --c)
+                            if (S.mask >> c & 1) st[sp++] = S.child + c;
                     }
-                    ++lf;
-                } else if (cls == 2) {
-                    if (FILL) a.near_key[no + atomicAdd(&s_pos[wid][1], 1)] = lk | (uint32_t)a.node_leaf[s];
-                    else nsrc += S.end - S.beg;
-                    ++ln;
-                } else if (cls == 3) {
-                    for (int c = 7; c >= 0; --c) st[sp++] = S.child + c;
                 }
             }
+        };
+        int lf, ln;
+        lane_walk(false, 0, 0, lf, ln);
+        int ef = lf, en = ln;  // inclusive prefix sums over the lanes
+        for (int o = 1; o < 32; o <<= 1) {
+            const int uf = __shfl_up_sync(0xffffffffu, ef, o), un = __shfl_up_sync(0xffffffffu, en, o);
+            if (lane >= o) {
+                ef += uf;
+                en += un;
+            }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            lf += __shfl_xor_sync(0xffffffffu, lf, o);
-            ln += __shfl_xor_sync(0xffffffffu, ln, o);
+        if (FILL) {
+            int lf2, ln2;
+            nsrc = 0;
+            lane_walk(true, fo + nf + ef - lf, no + nn + en - ln, lf2, ln2);
         }
-        nf += lf;
-        nn += ln;
+        nf += __shfl_sync(0xffffffffu, ef, 31);
+        nn += __shfl_sync(0xffffffffu, en, 31);
     }
-    if constexpr (!FILL) {
+    if constexpr (FILL) {
+        // the near list into the reference's depth-first order (leaf ordinals are depth-first
+        // numbers)
+        __syncwarp();
+        if (nn <= kWalkStack / 2) {
+            sort_into(a.near_key + no, nn, reinterpret_cast<uint64_t*>(stk), lane, a.near_leaf + no);
+        } else if (lane == 0) {
+            a.long_leaf[atomicAdd(a.long_count, 1)] = l;  // sorted by long_sort_kernel
+        }
+    } else {
         for (int o = 16; o > 0; o >>= 1) nsrc += __shfl_xor_sync(0xffffffffu, nsrc, o);
         if (lane != 0) return;
         a.far_cnt[l] = nf;
@@ -446,9 +509,66 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a
     }
 }
 
-__global__ void __launch_bounds__(256) near_unpack_kernel(const uint64_t* keys, int32_t* out, int64_t n) {
-    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
-    if (i < n) out[i] = (int32_t)(keys[i] & 0xffffffffull);
+// Near lists longer than a warp's buffer: one CTA per list.  Runs of kLongSort ordinals
+// are sorted by a bitonic network in shared memory and written back in place; each ordinal's
+// final place is then the sum over the runs of the number of smaller ordinals in the run
+// (binary searches; the ordinals are distinct).
+constexpr int kLongSort = 8192;
+__global__ void __launch_bounds__(1024) long_sort_kernel(const TreeListArgs a) {
+    __shared__ uint32_t s_key[kLongSort];
+    const int n_long = *a.long_count;
+    for (int q = blockIdx.x; q < n_long; q += gridDim.x) {
+        const int l = a.long_leaf[q];
+        const int no = a.near_off[l], n = a.near_off[l + 1] - no;
+        uint64_t* v = a.near_key + no;
+        const int runs = (n + kLongSort - 1) / kLongSort;
+        for (int r = 0; r < runs; ++r) {
+            const int b = r * kLongSort, m = min(kLongSort, n - b);
+            int P = 1;
+            while (P < m) P <<= 1;
+            for (int i = threadIdx.x; i < P; i += 1024) s_key[i] = i < m ? (uint32_t)v[b + i] : 0xffffffffu;
+            __syncthreads();
+            for (int k = 2; k <= P; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = threadIdx.x; i < P; i += 1024) {
+                        const int mm = i ^ j;
+                        if (mm > i) {
+                            const uint32_t x = s_key[i], y = s_key[mm];
+                            if ((x > y) == ((i & k) == 0)) {
+                                s_key[i] = y;
+                                s_key[mm] = x;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            if (runs == 1) {
+                for (int i = threadIdx.x; i < m; i += 1024) a.near_leaf[no + i] = (int32_t)s_key[i];
+            } else {
+                for (int i = threadIdx.x; i < m; i += 1024) v[b + i] = s_key[i];
+            }
+            __syncthreads();
+        }
+        if (runs == 1) continue;
+        __threadfence_block();
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += 1024) {
+            const uint64_t key = v[i];
+            int pos = 0;
+            for (int r = 0; r < runs; ++r) {
+                int lo = r * kLongSort, hi = min(n, lo + kLongSort);
+                const int base = lo;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (v[mid] < key) lo = mid + 1;
+                    else hi = mid;
+                }
+                pos += lo - base;
+            }
+            a.near_leaf[no + pos] = (int32_t)(uint32_t)key;
+        }
+        __syncthreads();
+    }
 }
 
 __global__ void __launch_bounds__(256) items_kernel(const TreeListArgs a, int n_leaves) {
@@ -541,44 +661,12 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     return cudaSuccess;
 }
 
-int list_key_bits(int32_t n_leaves) {
-    int b = 1;
-    while (b < 31 && (1ll << b) <= (long long)n_leaves) ++b;
-    return 32 + b;
-}
-
-size_t tree_list_sort_bytes(int64_t n_far, int64_t n_near, int32_t n_leaves) {
-    size_t b = 0, c = 0;
-    cub::DoubleBuffer<uint64_t> k(nullptr, nullptr);
-    cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
-    cub::DeviceRadixSort::SortPairs(nullptr, b, k, v, (int)n_far, 0, list_key_bits(n_leaves));
-    cub::DeviceRadixSort::SortKeys(nullptr, c, k, (int)n_near, 0, list_key_bits(n_leaves));
-    return std::max(b, c);
-}
-
-cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, int64_t n_far, int64_t n_near, void* temp,
-                                   size_t temp_bytes, cudaStream_t st) {
+cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st) {
     if (n_leaves == 0) return cudaSuccess;
-    walk_kernel<true><<<(n_leaves + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(a.long_count, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    const int bits = list_key_bits(n_leaves);
-    if (n_far > 0) {
-        cub::DoubleBuffer<uint64_t> k(a.far_key, a.far_key_alt);
-        cub::DoubleBuffer<int32_t> v(a.far_tmp, a.far_node);
-        size_t tb = temp_bytes;
-        if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, k, v, (int)n_far, 0, bits, st)) != cudaSuccess) return e;
-        if (v.Current() != a.far_node &&
-            (e = cudaMemcpyAsync(a.far_node, v.Current(), (size_t)n_far * sizeof(int32_t), cudaMemcpyDeviceToDevice,
-                                 st)) != cudaSuccess)
-            return e;
-    }
-    if (n_near > 0) {
-        cub::DoubleBuffer<uint64_t> k(a.near_key, a.near_key_alt);
-        size_t tb = temp_bytes;
-        if ((e = cub::DeviceRadixSort::SortKeys(temp, tb, k, (int)n_near, 0, bits, st)) != cudaSuccess) return e;
-        near_unpack_kernel<<<(unsigned)((n_near + 255) / 256), 256, 0, st>>>(k.Current(), a.near_leaf, n_near);
-    }
+    walk_kernel<true><<<(n_leaves + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
+    long_sort_kernel<<<296, 1024, 0, st>>>(a);
     items_kernel<<<(n_leaves + 255) / 256, 256, 0, st>>>(a, n_leaves);
     return cudaGetLastError();
 }

@@ -45,12 +45,14 @@ cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_by
 cudaError_t launch_tree_leaf_order(const TreeBuildArgs& t, int32_t n_nodes, void* temp, size_t temp_bytes,
                                    cudaStream_t st);
 
-// What the list walk reads of a node, packed (56 B).
+// What the list walk reads of a node, packed (56 B); mask has bit c set when child c has
+// mass > 0.
 struct WalkNode {
     double cx, cy, cz, hw;
     double mass;
     int32_t child;
     int32_t beg, end;
+    int32_t mask;
 };
 
 // Leaves with mass > 0 (depth-first) and their near / far lists, after the node moments.
@@ -89,12 +91,10 @@ struct TreeListArgs {
     int32_t* item_off;
     int32_t* slot_off;
     unsigned long long* totals;  // 6: far, near, items, slots (overflow check), far and near body pairs
-    // fill pass: unsorted lists as sort keys (leaf << 32 | order key), then the sorted lists
-    uint64_t* far_key;  // order key: first body of the far node
-    uint64_t* far_key_alt;
-    int32_t* far_tmp;   // node ids beside far_key
-    uint64_t* near_key;  // order key: leaf ordinal of the near leaf
-    uint64_t* near_key_alt;
+    // fill pass: the near lists unsorted (leaf ordinals), then sorted into near_leaf
+    uint64_t* near_key;
+    int32_t* long_leaf;   // leaves whose near lists are sorted by a separate kernel
+    int32_t* long_count;
     int32_t* far_node;
     int32_t* near_leaf;
     void* items;  // M2PItem
@@ -102,9 +102,7 @@ struct TreeListArgs {
 size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes);
 // Leaf compaction, the count walk and the offsets (sizes become known on the host after it).
 cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
-// The fill walk, the sort of every leaf's lists into depth-first order, the far-field work items.
-size_t tree_list_sort_bytes(int64_t n_far, int64_t n_near, int32_t n_leaves);
-cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, int64_t n_far, int64_t n_near, void* temp,
-                                   size_t temp_bytes, cudaStream_t st);
+// The fill walk (each leaf's lists sorted into depth-first order) and the far-field work items.
+cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st);
 
 }  // namespace gx

@@ -37,15 +37,18 @@ constexpr int kMaxChunks = 8;    // a leaf's source sequence is split into at mo
 constexpr int kMinChunk = 2048;  // ... of at least this many sources
 constexpr int kScanBlock = 1024;
 
-// Per leaf: number of sources, number of chunks, scratch demand (split leaves only).
-__global__ void p2p_count_kernel(const P2PArgs a, int exact) {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+// Per leaf (one warp each): number of sources, number of chunks, scratch demand (split
+// leaves only).
+__global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exact) {
+    const int l = (int)((blockIdx.x * 256u + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (l >= a.n_leaves) return;
     int64_t src = 0;
-    for (int q = a.near_off[l]; q < a.near_off[l + 1]; ++q) {
+    for (int q = a.near_off[l] + lane; q < a.near_off[l + 1]; q += 32) {
         const int s = a.near_leaf[q];
         src += a.leaf_off[s + 1] - a.leaf_off[s];
     }
+    for (int o = 16; o > 0; o >>= 1) src += __shfl_xor_sync(0xffffffffu, src, o);
+    if (lane != 0) return;
     const int nt = a.leaf_off[l + 1] - a.leaf_off[l];
     int chunks = 0;
     if (nt > 0 && src > 0) {
@@ -459,7 +462,7 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     cudaError_t e = cudaMemsetAsync(a.plan_done, 0, nl * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    p2p_count_kernel<<<(a.n_leaves + 255) / 256, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0);
+    p2p_count_kernel<<<(a.n_leaves + 7) / 8, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0);
     p2p_scan_kernel<<<1, kScanBlock, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (precision == kF64Exact) return launch_main<kF64Exact, false>(a, sms, st);

@@ -258,3 +258,18 @@ def test_pair_counts_host_builder():
     L = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
     _, st = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
     assert st.near_pairs == L.n_pairs and st.far_interactions == L.n_far and st.tree_levels > 22
+
+
+def test_long_near_lists_device_equal_host():
+    """A dense cube beside a sparse halo: big halo leaves border thousands of small ones, so
+    near lists run past the warp's sort buffer (1024) and past the CTA's (8192)."""
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.random((20000, 3)), rng.random((300, 3)) * 3 + 1.0])
+    m = np.full(len(x), 1.0 / len(x))
+    cols = [np.ascontiguousarray(x[:, k]) for k in range(3)]
+    h = gx.build_leaf_lists(*cols, m, 0.001, 0.6, 4)
+    d = gx.build_leaf_lists(*cols, m, 0.001, 0.6, 4, on_device=True)
+    nl = np.diff(h.near_offsets)
+    assert d.built_on_device and ((nl > 1024) & (nl <= 8192)).any() and (nl > 8192).any()
+    for f in ("leaf_offsets", "leaf_particles", "near_offsets", "near_leaves"):
+        assert np.array_equal(getattr(h, f), getattr(d, f)), f
