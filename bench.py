@@ -194,8 +194,8 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
     ap.add_argument("--workload", default="mixed-n1048576",
-                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "p2p-n65536", "direct-n65536", "direct-n1000",
-                             "fit-n16384"],
+                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "snapshots-n1048576", "p2p-n65536",
+                             "direct-n65536", "direct-n1000", "fit-n16384"],
                     help="headline (default) or one of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
@@ -780,9 +780,67 @@ def wl_fmm(gx, torch, args) -> dict:
     return out
 
 
+def wl_snapshots(gx, torch, args) -> dict:
+    """Snapshot output from the resident N = 2^20 session (mixed precision): 20 KDK steps with
+    a snapshot (reference CSV + binary) every 5 steps vs the same steps without; the stepping
+    stream pays only the device-to-device copy, the writer thread does the rest."""
+    import shutil
+    import tempfile
+    n, eps, dt, steps, every = 1 << 20, 0.01, 0.001, 20, 5
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps, mass1=1.0, mass2=1.0 / 3.0)
+    out = tempfile.mkdtemp(prefix="gx_snap_")
+    try:
+        with gx.Session(n, gx.PhysicsParams(1.0, eps)) as s, gx.SnapshotWriter(out, n, binary=True, slots=2) as w:
+            s.set_particles(p)
+            s.compute_accelerations(gx.PRECISION_MIXED)
+            st = torch.cuda.Stream()
+            s.set_stream(st)
+            s.step(3, dt, gx.PRECISION_MIXED)
+            s.synchronize()
+            res = {}
+            for label, snap in (("without", False), ("with", True)):
+                a, e = _events(torch)
+                t0 = time.perf_counter()
+                a.record(st)
+                for k in range(steps // every):
+                    s.step(every, dt, gx.PRECISION_MIXED)
+                    if snap:
+                        s.snapshot(w, k, k * every * dt)
+                e.record(st)
+                e.synchronize()
+                res[label] = {"device_ms": a.elapsed_time(e), "wall_ms_to_last_step": (time.perf_counter() - t0) * 1e3}
+            t1 = time.perf_counter()
+            w.flush()
+            drain = time.perf_counter() - t1
+            # the stream's own cost of one snapshot: events around the call on an idle stream
+            copies = []
+            for k in range(3):
+                a, e = _events(torch)
+                a.record(st)
+                s.snapshot(w, 100 + k, 0.0)
+                e.record(st)
+                e.synchronize()
+                copies.append(a.elapsed_time(e))
+                w.flush()
+        snaps = steps // every
+        csv_bytes = sum(os.path.getsize(os.path.join(out, f)) for f in os.listdir(out)
+                        if f.endswith(".csv") and f.startswith("snapshot_0000")) / snaps * snaps
+    finally:
+        shutil.rmtree(out, ignore_errors=True)
+    over = (res["with"]["device_ms"] - res["without"]["device_ms"]) / snaps
+    return {"metric": "stream time per snapshot (N=2^20, device copy)", "value": float(np.median(copies)),
+            "unit": "ms", "step_overhead_ms_per_snapshot": over,
+            "higher_is_better": False, "steps": steps, "snapshot_every": every, "snapshots": snaps,
+            "step_ms_without": res["without"]["device_ms"] / steps, "step_ms_with": res["with"]["device_ms"] / steps,
+            "writer_drain_s_after_last_step": drain, "csv_bytes_per_snapshot": csv_bytes / snaps,
+            "config": {"workload": "snapshots-n1048576", "n": n, "formats": "reference CSV + binary SoA",
+                       "precision": "mixed"}}
+
+
 OTHER_WORKLOADS = {
     "ensemble": wl_ensemble,
     "fmm-n65536": wl_fmm,
+    "snapshots-n1048576": wl_snapshots,
     "p2p-n65536": wl_p2p,
     "direct-n65536": lambda gx, torch, args: wl_direct(gx, torch, args, 65536, 0.02, 0.002, 100),
     "direct-n1000": lambda gx, torch, args: wl_direct(gx, torch, args, 1000, 0.05, 0.005, 20),

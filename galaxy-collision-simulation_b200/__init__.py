@@ -11,6 +11,7 @@ of its FMM.  Compute runs in hand-written sm_100a CUDA kernels behind the C ABI 
 * ``fmm``      -- the reference FMM solver (moments, far field and near field on the GPU)
 * ``adjoint``  -- autograd Function over the leapfrog with the adjoint kernel (needs torch)
 * ``ics``      -- seeded two-disk initial conditions
+* ``snapshots`` -- the reference's CSV snapshot / diagnostics output (+ a binary form), async
 """
 from ._ffi import (GX_ERR_CUDA, GX_ERR_INVALID_ARGUMENT, GX_ERR_NO_DEVICE, GX_ERR_OUT_OF_MEMORY, GX_ERR_TIMEOUT,
                    GX_ERR_UNSUPPORTED, GX_OK, LIB_PATH, PRECISION_F64, PRECISION_F64_EXACT, PRECISION_MIXED, GxError,
@@ -22,6 +23,7 @@ from .fmm import (FastMultipoleSolver, FmmOptions, FmmStats, compute_fmm_acceler
                   compute_fmm_accelerations_for_targets)
 from .fmm_p2p import LeafLists, build_leaf_lists, p2p_leaves
 from .session import Batch, Session, batch_accelerations, describe_variant
+from .snapshots import SnapshotWriter, read_binary
 from . import ics
 
 __all__ = [
@@ -30,6 +32,6 @@ __all__ = [
     "cuda_direct_leapfrog_step", "compute_diagnostics", "indexed_accelerations", "build_leaf_lists", "p2p_leaves",
     "batch_accelerations", "describe_variant", "device_available", "load", "ics",
     "FastMultipoleSolver", "FmmOptions", "FmmStats", "compute_fmm_accelerations",
-    "compute_fmm_accelerations_for_targets",
+    "compute_fmm_accelerations_for_targets", "SnapshotWriter", "read_binary",
     "PRECISION_F64", "PRECISION_MIXED", "PRECISION_F64_EXACT",
 ]

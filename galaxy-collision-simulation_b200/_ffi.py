@@ -25,6 +25,8 @@ GX_ERR_UNSUPPORTED = 6
 PRECISION_F64 = 0
 PRECISION_MIXED = 1
 PRECISION_F64_EXACT = 2
+SNAPSHOT_CSV = 1
+SNAPSHOT_BINARY = 2
 PRECISIONS = {"f64": PRECISION_F64, "mixed": PRECISION_MIXED, "f64-exact": PRECISION_F64_EXACT}
 
 _STATUS_NAMES = {
@@ -116,6 +118,12 @@ _SIGNATURES = {
     "gx_session_set_config": [P, c_int, c_int, c_int],
     "gx_session_autotune": [P, c_int, POINTER(D)],
     "gx_p2p_leaves": [I64, P, P, P, P, c_int32, P, P, P, P, Physics, c_int, P, P, P, S],
+    "gx_snapshot_writer_create": [c_char_p, I64, P, c_int, c_int, PP],
+    "gx_snapshot_writer_flush": [P],
+    "gx_snapshot_writer_destroy": [P],
+    "gx_snapshot_write": [P, c_int, D, P, P, P, P, P, P, P, P, P, P, S],
+    "gx_snapshot_write_diagnostics": [P, c_int, D, POINTER(DiagnosticsStruct)],
+    "gx_session_snapshot": [P, P, c_int, D],
     "gx_fmm_accel": [I64, P, P, P, P, Physics, FmmOptionsStruct, c_int, I64, I64, P, P, P, POINTER(FmmStatsStruct),
                      S],
     "gx_fmm_accel_timed": [I64, P, P, P, P, Physics, FmmOptionsStruct, c_int, I64, I64, P, P, P,

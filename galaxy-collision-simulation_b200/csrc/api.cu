@@ -984,6 +984,15 @@ extern "C" int gx_session_get_state(gx_session* s, double* x, double* y, double*
     GX_GUARD_END
 }
 
+extern "C" int gx_session_snapshot(gx_session* s, gx_snapshot_writer* w, int step, double time) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_session(s, "gx_session_snapshot"));
+    DeviceGuard g(s->device);
+    return gx_snapshot_write(w, step, time, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m,
+                             s->stream);
+    GX_GUARD_END
+}
+
 extern "C" int gx_session_device_arrays(gx_session* s, double** p) {
     GX_TRY(check_session(s, "gx_session_device_arrays"));
     if (!p) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_device_arrays: null");

@@ -87,6 +87,10 @@ class Session:
         _ffi.call("gx_session_diagnostics", self._h, ctypes.byref(d))
         return Diagnostics.from_struct(d)
 
+    def snapshot(self, writer, step: int, time: float) -> None:
+        """Hands the current state to a SnapshotWriter without stalling the session's stream."""
+        _ffi.call("gx_session_snapshot", self._h, writer.handle, int(step), float(time))
+
     def synchronize(self, timeout_ms: float | None = None):
         if timeout_ms is None:
             _ffi.call("gx_session_synchronize", self._h)

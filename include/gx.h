@@ -149,6 +149,9 @@ int gx_session_compute_accelerations(gx_session* s, int precision);
 /* n_steps KDK steps (kick dt/2, drift dt, force, kick dt/2 per step). */
 int gx_session_step(gx_session* s, int64_t n_steps, double dt, int precision);
 int gx_session_diagnostics(gx_session* s, gx_diagnostics* out);
+/* gx_snapshot_write of the session's state on the session's stream (declared below). */
+struct gx_snapshot_writer;
+int gx_session_snapshot(gx_session* s, struct gx_snapshot_writer* w, int step, double time);
 int gx_session_synchronize(gx_session* s);
 /* Bounded host wait: GX_ERR_TIMEOUT if the stream is still busy after timeout_ms. */
 int gx_session_synchronize_timeout(gx_session* s, double timeout_ms);
@@ -173,6 +176,36 @@ int gx_p2p_leaves(int64_t n, const double* x, const double* y, const double* z,
                   const int32_t* leaf_particles, const int32_t* near_offsets,
                   const int32_t* near_leaves, gx_physics phys, int precision, double* ax,
                   double* ay, double* az, void* stream);
+
+/* ---- snapshot output (cpp/io/snapshot_writer.cpp:38-128) ------------------------- */
+/* SnapshotWriter with output that does not stall the stepping stream.  CSV files are the
+ * reference's byte for byte (snapshot_%06d.csv, diagnostics.csv); the binary form
+ * snapshot_%06d.bin holds the same state as SoA doubles ("GXSNAP01", int64 n, int32 step,
+ * int32 fields = 10, double time, x y z vx vy vz ax ay az m, uint32 group ids). */
+#define GX_SNAPSHOT_CSV 1
+#define GX_SNAPSHOT_BINARY 2
+typedef struct gx_snapshot_writer gx_snapshot_writer;
+/* SnapshotWriter constructor (snapshot_writer.cpp:38-57): creates `directory` and, with
+ * GX_SNAPSHOT_CSV, starts diagnostics.csv with the reference's header.  n and the group ids
+ * (NULL: all 0) are fixed for the writer's life; `slots` snapshots may be in flight. */
+int gx_snapshot_writer_create(const char* directory, int64_t n, const uint32_t* group_id,
+                              int formats, int slots, gx_snapshot_writer** out);
+/* Waits until every snapshot handed over so far is written; the first write error. */
+int gx_snapshot_writer_flush(gx_snapshot_writer* w);
+/* Flushes, then frees the writer; returns the flush status. */
+int gx_snapshot_writer_destroy(gx_snapshot_writer* w);
+/* write_snapshot (snapshot_writer.cpp:72-96) of arrays x..az, m -- all host or all device
+ * memory.  Device arrays are copied device-to-device on `stream` (later work on `stream`
+ * may overwrite them at once), then to pinned host memory on the writer's own stream; a
+ * writer thread formats and writes.  Host arrays are copied during the call.  Blocks only
+ * while all slots are in flight. */
+int gx_snapshot_write(gx_snapshot_writer* w, int step, double time, const double* x,
+                      const double* y, const double* z, const double* vx, const double* vy,
+                      const double* vz, const double* ax, const double* ay, const double* az,
+                      const double* m, void* stream);
+/* write_diagnostics (snapshot_writer.cpp:99-128): one row of diagnostics.csv. */
+int gx_snapshot_write_diagnostics(gx_snapshot_writer* w, int step, double time,
+                                  const gx_diagnostics* d);
 
 /* ---- FMM (cpp/fmm/fmm_solver.hpp:15-20, fmm_solver.cpp:315-333) --------------------- */
 /* FmmOptions with the reference's defaults: theta 0.6, leaf_capacity 16, max_depth 32,

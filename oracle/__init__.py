@@ -74,6 +74,8 @@ def ref():
         lib.ref_fmm_split.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int,
                                       POINTER(c_int32), POINTER(c_int64), P, P, P, P, P, P, P]
         lib.ref_smoke80_inputs.argtypes = [P, P, P, P]
+        lib.ref_write_outputs.argtypes = [ctypes.c_char_p, c_int64, P, P, P, P, P, P, P, P, P, P, P, c_int, c_double,
+                                          P]
         lib.ref_fmm_moments.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, c_int64, P,
                                         POINTER(c_int64), P]
         lib.ref_fmm_timed.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, c_int64, c_int,
@@ -258,6 +260,15 @@ def ref_fmm_timed(x, y, z, m, G, eps, theta, leaf_capacity, order, stride, threa
     ref().ref_fmm_timed(n, _p(x), _p(y), _p(z), _p(m), G, eps, theta, leaf_capacity, order, stride, threads,
                         *map(_p, out), ctypes.byref(b), ctypes.byref(e), ctypes.byref(k))
     return np.stack(out, 1), b.value, e.value, k.value
+
+
+def ref_write_outputs(directory, state: dict, m, group, step, time, diag13):
+    """The reference SnapshotWriter writes diagnostics.csv (header + one row) and one snapshot."""
+    arrs = [_f(state[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")] + [_f(m)]
+    g = None if group is None else np.ascontiguousarray(group, np.uint32)
+    d = _f(diag13)
+    ref().ref_write_outputs(str(directory).encode(), len(arrs[0]), *map(_p, arrs), None if g is None else _p(g),
+                            int(step), float(time), _p(d))
 
 
 def ref_smoke80_inputs():

@@ -25,6 +25,7 @@
 #include "core/initial_conditions.hpp"
 #include "core/integrator.hpp"
 #include "direct/direct_solver.hpp"
+#include "io/snapshot_writer.hpp"
 #include "fmm/multipole.hpp"
 #include "mpi/distributed_solver.hpp"
 
@@ -285,6 +286,31 @@ void ref_fmm_timed(int64_t n, const double* x, const double* y, const double* z,
     *build_s = std::chrono::duration<double>(t1 - t0).count();
     *eval_s = std::chrono::duration<double>(t3 - t2).count();
     *n_eval = static_cast<int64_t>(work.size());
+}
+
+// SnapshotWriter (snapshot_writer.cpp:38-128) on one state: diagnostics.csv header, one
+// snapshot file and one diagnostics row (diag: 13 doubles in the row's column order).
+int ref_write_outputs(const char* directory, int64_t n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz, const double* ax, const double* ay,
+                      const double* az, const double* m, const uint32_t* group, int step, double time,
+                      const double* diag) {
+    auto p = to_particles(n, x, y, z, m, vx, vy, vz, ax, ay, az);
+    for (int64_t i = 0; i < n; ++i) p[i].group_id = group ? group[i] : 0u;
+    fmmgalaxy::SimulationConfig cfg;
+    cfg.output.directory = directory;
+    cfg.output.format = "csv";
+    fmmgalaxy::SnapshotWriter w(cfg);
+    w.write_snapshot(step, time, p);
+    fmmgalaxy::Diagnostics d;
+    d.total_mass = diag[0];
+    d.kinetic_energy = diag[1];
+    d.potential_energy = diag[2];
+    d.total_energy = diag[3];
+    d.momentum = {diag[4], diag[5], diag[6]};
+    d.center_of_mass = {diag[7], diag[8], diag[9]};
+    d.angular_momentum = {diag[10], diag[11], diag[12]};
+    w.write_diagnostics(step, time, d, static_cast<std::size_t>(n));
+    return 0;
 }
 
 // The inputs of the reference smoke test's solver-agreement case (smoke_tests.cpp:83-89):
