@@ -194,7 +194,7 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
     ap.add_argument("--workload", default="mixed-n1048576",
-                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "snapshots-n1048576", "p2p-n65536",
+                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "snapshots-n1048576", "ics-ensemble512", "p2p-n65536",
                              "direct-n65536", "direct-n1000", "fit-n16384"],
                     help="headline (default) or one of the other configurations")
     args = ap.parse_args()
@@ -837,10 +837,60 @@ def wl_snapshots(gx, torch, args) -> dict:
                        "precision": "mixed"}}
 
 
+def wl_ics(gx, torch, args) -> dict:
+    """Initial conditions of the 512-encounter ensemble generated on the device: 1024 disks
+    (N_b ~ U[1024, 16384] per encounter, two disks each, mass ratio ~ U[1, 10], impact
+    parameter ~ U[0.5, 4], inclination ~ U[0, 90] deg) with the reference's disk model.
+    CPU baseline: the reference's generate_galaxies (one mt19937_64 stream) on a sample."""
+    import oracle
+    rng = np.random.Generator(np.random.PCG64(7))
+    sizes = 2 * rng.integers(512, 8193, 512)
+    ratio, impact, incl = rng.uniform(1, 10, 512), rng.uniform(0.5, 4.0, 512), rng.uniform(0, np.pi / 2, 512)
+    gals = []
+    for b in range(512):
+        h = int(sizes[b]) // 2
+        gals.append(dict(n_particles=h, mass=1.0, radius=1.0, thickness=0.05, group_id=2 * b))
+        gals.append(dict(n_particles=h, mass=1.0 / ratio[b], radius=1.0, thickness=0.05, group_id=2 * b + 1,
+                         position=(10.0, impact[b], 0.0), velocity=(-0.5, 0.0, 0.0), inclination=incl[b]))
+    params = gx.PhysicsParams(1.0, 0.05)
+    n = int(sum(g["n_particles"] for g in gals))
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            out = gx.ics.generate_galaxies(gals, params, 11, device="cuda", stream=st.cuda_stream)
+        a, e = _events(torch)
+        a.record(st)
+        reps = 10
+        for _ in range(reps):
+            out = gx.ics.generate_galaxies(gals, params, 11, device="cuda", stream=st.cuda_stream)
+        e.record(st)
+        e.synchronize()
+    ms = a.elapsed_time(e) / reps
+    t0 = time.perf_counter()
+    host = gx.ics.generate_galaxies(gals, params, 11)
+    e2e_s = time.perf_counter() - t0
+    res = {"metric": "bodies generated per second (512-encounter ensemble ICs)", "value": n / (ms / 1e3),
+           "unit": "bodies/s", "bodies": n, "galaxies": len(gals), "ms_per_generation": ms,
+           "e2e": {"value": n / e2e_s, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 7 * 8 * n + 4 * n},
+           "config": {"workload": "ics-ensemble512", "model": "reference disk (initial_conditions.cpp:37-89)",
+                      "random_numbers": "Philox4x32-10, counter (galaxy, body, block)"}}
+    if oracle.ref_available():
+        sample = gals[: max(2, len(gals) // 16)]
+        ns = int(sum(g["n_particles"] for g in sample))
+        t0 = time.perf_counter()
+        oracle.ref_generate_galaxies(sample, 1.0, 0.05, 11)
+        cs = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": ns / cs, "unit": "bodies/s", "cores": 1, "kind": "reference",
+                               "sample": f"generate_galaxies on the first {len(sample)} disks ({ns} bodies, {cs:.2f} s)"}
+    del host, out
+    return res
+
+
 OTHER_WORKLOADS = {
     "ensemble": wl_ensemble,
     "fmm-n65536": wl_fmm,
     "snapshots-n1048576": wl_snapshots,
+    "ics-ensemble512": wl_ics,
     "p2p-n65536": wl_p2p,
     "direct-n65536": lambda gx, torch, args: wl_direct(gx, torch, args, 65536, 0.02, 0.002, 100),
     "direct-n1000": lambda gx, torch, args: wl_direct(gx, torch, args, 1000, 0.05, 0.005, 20),

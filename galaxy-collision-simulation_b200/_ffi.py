@@ -82,6 +82,14 @@ class FmmStatsStruct(ctypes.Structure):
                 ("tree_levels", c_int64)]
 
 
+class GalaxyStruct(ctypes.Structure):
+    """gx_galaxy: GalaxyConfig of the reference (cpp/core/initial_conditions.hpp:14-24)."""
+
+    _fields_ = [("n_particles", c_int64), ("mass", c_double), ("radius", c_double), ("position", c_double * 3),
+                ("velocity", c_double * 3), ("orientation", c_double), ("group_id", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("thickness", c_double), ("inclination", c_double)]
+
+
 P = c_void_p  # any array: numpy .ctypes.data, torch .data_ptr(), or None
 PP = POINTER(c_void_p)
 I64 = c_int64
@@ -118,6 +126,8 @@ _SIGNATURES = {
     "gx_session_set_config": [P, c_int, c_int, c_int],
     "gx_session_autotune": [P, c_int, POINTER(D)],
     "gx_p2p_leaves": [I64, P, P, P, P, c_int32, P, P, P, P, Physics, c_int, P, P, P, S],
+    "gx_galaxies_body_count": [c_int32, P],
+    "gx_generate_galaxies": [c_int32, P, Physics, ctypes.c_uint64, P, P, P, P, P, P, P, P, S],
     "gx_snapshot_writer_create": [c_char_p, I64, P, c_int, c_int, PP],
     "gx_snapshot_writer_flush": [P],
     "gx_snapshot_writer_destroy": [P],
@@ -156,7 +166,7 @@ _SIGNATURES = {
     "gx_variant_describe": [c_int, c_int, c_char_p, c_int],
     "gx_debug_fail_allocations": [c_int],
 }
-_RESTYPES = {"gx_last_error": c_char_p}
+_RESTYPES = {"gx_last_error": c_char_p, "gx_galaxies_body_count": c_int64}
 
 _lib = None
 

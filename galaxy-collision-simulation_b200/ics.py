@@ -112,3 +112,50 @@ def ensemble(n_instances: int = 512, seed: int = 7, n_min: int = 1024, n_max: in
     ps = ParticleSet(cat("x"), cat("y"), cat("z"), cat("vx"), cat("vy"), cat("vz"), cat("m"),
                      group_id=cat("group_id"))
     return offsets, ps, dict(sizes=sizes, mass_ratio=ratio, impact=impact, inclination_deg=incl)
+
+
+def _galaxy_struct(g: dict):
+    from . import _ffi
+    gs = _ffi.GalaxyStruct()
+    gs.n_particles = int(g["n_particles"])
+    gs.mass = float(g["mass"])
+    gs.radius = float(g["radius"])
+    gs.position[:] = [float(v) for v in g.get("position", (0.0, 0.0, 0.0))]
+    gs.velocity[:] = [float(v) for v in g.get("velocity", (0.0, 0.0, 0.0))]
+    gs.orientation = float(g.get("orientation", 0.0))
+    gs.group_id = int(g.get("group_id", 0))
+    gs.thickness = float(g.get("thickness", 0.0))
+    gs.inclination = float(g.get("inclination", 0.0))
+    return gs
+
+
+def generate_galaxies(galaxies, params, seed: int, device=None, stream=None):
+    """The reference's generate_galaxies (cpp/core/initial_conditions.cpp:92-114) computed on
+    the GPU: each galaxy is a dict of GalaxyConfig fields (n_particles, mass, radius,
+    position, velocity, orientation, group_id, thickness, inclination).  Returns a
+    ParticleSet (host) or, with device="cuda", a dict of CUDA tensors.  Same disk model as
+    the reference; the random numbers come from a counter-based generator, so the bodies
+    differ from the reference's mt19937_64 draws but follow the same distributions."""
+    import ctypes
+    from . import _ffi
+    from .engine import ParticleSet
+    arr = (_ffi.GalaxyStruct * max(1, len(galaxies)))(*[_galaxy_struct(g) for g in galaxies])
+    n = int(_ffi.load().gx_galaxies_body_count(len(galaxies), ctypes.addressof(arr)))
+    fields = ("x", "y", "z", "vx", "vy", "vz", "m")
+    if device is not None:
+        import torch
+        out = {f: torch.empty(n, dtype=torch.float64, device=device) for f in fields}
+        grp = torch.empty(n, dtype=torch.int32, device=device)
+        _ffi.call("gx_generate_galaxies", len(galaxies), ctypes.addressof(arr), params.ffi(), int(seed),
+                  *(out[f].data_ptr() for f in fields), grp.data_ptr(), _ffi.stream_ptr(stream))
+        out["group_id"] = grp
+        return out
+    out = {f: np.zeros(n) for f in fields}
+    grp = np.zeros(n, np.uint32)
+    if n:
+        _ffi.call("gx_generate_galaxies", len(galaxies), ctypes.addressof(arr), params.ffi(), int(seed),
+                  *(out[f].ctypes.data for f in fields), grp.ctypes.data, _ffi.stream_ptr(stream))
+    p = ParticleSet(x=out["x"], y=out["y"], z=out["z"], vx=out["vx"], vy=out["vy"], vz=out["vz"], m=out["m"])
+    p.group_id = grp
+    return p
+

@@ -177,6 +177,33 @@ int gx_p2p_leaves(int64_t n, const double* x, const double* y, const double* z,
                   const int32_t* near_leaves, gx_physics phys, int precision, double* ax,
                   double* ay, double* az, void* stream);
 
+/* ---- initial conditions (cpp/core/initial_conditions.cpp:37-114) ------------------ */
+/* GalaxyConfig (cpp/core/initial_conditions.hpp:14-24). */
+typedef struct gx_galaxy {
+    int64_t n_particles;
+    double mass;
+    double radius;
+    double position[3];
+    double velocity[3];
+    double orientation;
+    uint32_t group_id;
+    uint32_t reserved;
+    double thickness;
+    double inclination;
+} gx_galaxy;
+/* Bodies generate_galaxies makes for the list: galaxies with n_particles == 0, mass <= 0 or
+ * radius <= 0 make none (initial_conditions.cpp:46-48). */
+int64_t gx_galaxies_body_count(int32_t n_galaxies, const gx_galaxy* galaxies);
+/* generate_galaxies (initial_conditions.cpp:92-114) on the device: the reference's disk
+ * model, bodies concatenated in galaxy order, written to host or device arrays of
+ * gx_galaxies_body_count entries (group_id may be NULL).  The random numbers come from a
+ * counter-based generator (Philox4x32-10 keyed by the seed, counter = galaxy, body, block),
+ * not from the reference's mt19937_64 stream: same distributions, different draws; a
+ * galaxy's bodies do not depend on the other galaxies. */
+int gx_generate_galaxies(int32_t n_galaxies, const gx_galaxy* galaxies, gx_physics phys,
+                         uint64_t seed, double* x, double* y, double* z, double* vx, double* vy,
+                         double* vz, double* m, uint32_t* group_id, void* stream);
+
 /* ---- snapshot output (cpp/io/snapshot_writer.cpp:38-128) ------------------------- */
 /* SnapshotWriter with output that does not stall the stepping stream.  CSV files are the
  * reference's byte for byte (snapshot_%06d.csv, diagnostics.csv); the binary form

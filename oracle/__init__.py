@@ -52,6 +52,8 @@ def port():
         lib.oracle_p2p_near.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_int32, P, P, P, P, P, P, P]
         lib.oracle_direct_vjp.argtypes = [c_int64, P, P, P, P, P, P, P, c_double, c_double, P, P, P, P]
         lib.oracle_ownership.argtypes = [c_int64, c_int, c_int, POINTER(c_int64), POINTER(c_int64)]
+        lib.oracle_generate_disk.argtypes = [c_int64, c_double, c_double, c_double, ctypes.c_double, c_double, P, P,
+                                             ctypes.c_uint32, c_double, c_double, ctypes.c_uint64, P, P, P, P, P, P, P]
         _port = lib
     return _port
 
@@ -74,6 +76,8 @@ def ref():
         lib.ref_fmm_split.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int,
                                       POINTER(c_int32), POINTER(c_int64), P, P, P, P, P, P, P]
         lib.ref_smoke80_inputs.argtypes = [P, P, P, P]
+        lib.ref_generate_galaxies.argtypes = [c_int, P, c_double, c_double, ctypes.c_uint64, P, P, P, P, P, P, P, P]
+        lib.ref_generate_galaxies.restype = c_int64
         lib.ref_write_outputs.argtypes = [ctypes.c_char_p, c_int64, P, P, P, P, P, P, P, P, P, P, P, c_int, c_double,
                                           P]
         lib.ref_fmm_moments.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, c_int64, P,
@@ -269,6 +273,48 @@ def ref_write_outputs(directory, state: dict, m, group, step, time, diag13):
     d = _f(diag13)
     ref().ref_write_outputs(str(directory).encode(), len(arrs[0]), *map(_p, arrs), None if g is None else _p(g),
                             int(step), float(time), _p(d))
+
+
+GALAXY_FIELDS = ("n_particles", "mass", "radius", "position", "velocity", "orientation", "group_id", "thickness",
+                 "inclination")
+
+
+def _galaxy_row(g: dict):
+    return [g["n_particles"], g["mass"], g["radius"], *g.get("position", (0, 0, 0)), *g.get("velocity", (0, 0, 0)),
+            g.get("orientation", 0.0), g.get("group_id", 0), g.get("thickness", 0.0), g.get("inclination", 0.0)]
+
+
+def ref_generate_galaxies(galaxies, G, eps, seed):
+    """The reference's generate_galaxies (mt19937_64): dict of x..vz, m, group_id."""
+    cfg = np.array([_galaxy_row(g) for g in galaxies], dtype=np.float64).ravel()
+    n = ref().ref_generate_galaxies(len(galaxies), _p(cfg), G, eps, seed, *([None] * 8))
+    out = {k: np.zeros(n) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    grp = np.zeros(n, np.uint32)
+    ref().ref_generate_galaxies(len(galaxies), _p(cfg), G, eps, seed, *(_p(out[k]) for k in ("x", "y", "z", "vx", "vy",
+                                                                                              "vz", "m")), _p(grp))
+    out["group_id"] = grp
+    return out
+
+
+def generate_galaxies(galaxies, G, eps, seed):
+    """The oracle's restatement with the engine's counter-based draws (oracle_generate_disk)."""
+    lib = port()
+    parts = []
+    for k, g in enumerate(galaxies):
+        n = int(g["n_particles"])
+        if n <= 0 or not g["mass"] > 0 or not g["radius"] > 0:
+            continue
+        arr = {f: np.zeros(n) for f in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        pos = _f(np.array(g.get("position", (0, 0, 0)), np.float64))
+        vel = _f(np.array(g.get("velocity", (0, 0, 0)), np.float64))
+        lib.oracle_generate_disk(n, float(g["mass"]), float(g["radius"]), float(g.get("thickness", 0.0)),
+                                 float(g.get("orientation", 0.0)), float(g.get("inclination", 0.0)), _p(pos), _p(vel),
+                                 k, G, eps, seed, *(_p(arr[f]) for f in ("x", "y", "z", "vx", "vy", "vz", "m")))
+        arr["group_id"] = np.full(n, int(g.get("group_id", 0)), np.uint32)
+        parts.append(arr)
+    if not parts:
+        return {f: np.zeros(0) for f in ("x", "y", "z", "vx", "vy", "vz", "m", "group_id")}
+    return {f: np.concatenate([q[f] for q in parts]) for f in parts[0]}
 
 
 def ref_smoke80_inputs():

@@ -442,3 +442,72 @@ ORACLE_API void oracle_direct_vjp(int64_t n, const double* x, const double* y, c
         if (gm) gm[k] = G * h;
     }
 }
+
+/* ---- disk initial conditions ------------------------------------------------------------
+ * generate_disk_galaxy (cpp/core/initial_conditions.cpp:37-89) with the draws of the engine's
+ * counter-based generator: Philox4x32-10 (Salmon et al., SC'11) keyed by the seed, counter
+ * (body, body >> 32, galaxy index, block), two 53-bit uniforms per block, Box-Muller normals.
+ * One galaxy; `gal_index` is its position in the caller's galaxy list. */
+static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = (uint32_t)p1;
+        c[2] = n2;
+        c[3] = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+static double u53(uint32_t hi, uint32_t lo) {
+    return (double)((((uint64_t)hi << 32) | lo) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+ORACLE_API void oracle_generate_disk(int64_t n, double mass, double radius, double thickness, double orientation,
+                                     double inclination, const double* pos, const double* vel, uint32_t gal_index,
+                                     double G, double eps, uint64_t seed, double* x, double* y, double* z,
+                                     double* vx, double* vy, double* vz, double* m) {
+    const double pi = 3.141592653589793238462643383279502884;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const double pm = mass / (double)n;
+    const double disp = 0.025 * sqrt(G * mass / radius);
+    const double scale = radius / 3.0;
+    const double max_cdf = 1.0 - exp(-radius / scale);
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c[3][4];
+        for (uint32_t b = 0; b < 3; ++b) {
+            c[b][0] = (uint32_t)i;
+            c[b][1] = (uint32_t)((uint64_t)i >> 32);
+            c[b][2] = gal_index;
+            c[b][3] = b;
+            philox4x32_10(c[b], k0, k1);
+        }
+        const double u_r = u53(c[0][0], c[0][1]), u_t = u53(c[0][2], c[0][3]);
+        const double b1 = sqrt(-2.0 * log(1.0 - u53(c[1][0], c[1][1]))), a1 = 2.0 * pi * u53(c[1][2], c[1][3]);
+        const double b2 = sqrt(-2.0 * log(1.0 - u53(c[2][0], c[2][1]))), a2 = 2.0 * pi * u53(c[2][2], c[2][3]);
+        const double nz = b1 * cos(a1), nvx = b1 * sin(a1), nvy = b2 * cos(a2), nvz = b2 * sin(a2);
+        double u = u_r < 1.0e-12 ? 1.0e-12 : u_r;
+        if (u > 1.0 - 1.0e-12) u = 1.0 - 1.0e-12;
+        const double r = -scale * log(1.0 - u * max_cdf);            /* :28-33 */
+        const double th = 2.0 * pi * u_t;
+        const double lp[3] = {r * cos(th), r * sin(th), thickness > 0.0 ? thickness * nz : 0.0};
+        double frac = (r * r) / (radius * radius);
+        if (frac > 1.0) frac = 1.0;
+        const double menc = mass * frac > pm ? mass * frac : pm;       /* :66-67 */
+        const double sr2 = r * r + eps * eps;
+        const double vc = sqrt(G * menc * r * r / pow(sr2, 1.5));      /* :68-72 */
+        const double lv[3] = {-sin(th) * vc + disp * nvx, cos(th) * vc + disp * nvy, 0.25 * disp * nvz};
+        const double ci = cos(inclination), si = sin(inclination), co = cos(orientation), so = sin(orientation);
+        double* outp[3] = {x, y, z};
+        double* outv[3] = {vx, vy, vz};
+        for (int w = 0; w < 2; ++w) {                                   /* rotate_x, then rotate_z (:11-26) */
+            const double* v = w ? lv : lp;
+            const double y1 = ci * v[1] - si * v[2], z1 = si * v[1] + ci * v[2];
+            const double o[3] = {co * v[0] - so * y1, so * v[0] + co * y1, z1};
+            for (int a = 0; a < 3; ++a) (w ? outv : outp)[a][i] = (w ? vel : pos)[a] + o[a];
+        }
+        m[i] = pm;
+    }
+}

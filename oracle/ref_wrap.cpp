@@ -313,6 +313,34 @@ int ref_write_outputs(const char* directory, int64_t n, const double* x, const d
     return 0;
 }
 
+// generate_galaxies (initial_conditions.cpp:92-114).  Galaxy g is cfg[13 g .. 13 g + 12] =
+// n, mass, radius, position xyz, velocity xyz, orientation, group id, thickness, inclination.
+int64_t ref_generate_galaxies(int n_gal, const double* cfg, double G, double eps, uint64_t seed, double* x, double* y,
+                              double* z, double* vx, double* vy, double* vz, double* m, uint32_t* group) {
+    std::vector<fmmgalaxy::GalaxyConfig> gs((size_t)n_gal);
+    for (int g = 0; g < n_gal; ++g) {
+        const double* c = cfg + 13 * g;
+        gs[g].n_particles = (std::size_t)c[0];
+        gs[g].mass = c[1];
+        gs[g].radius = c[2];
+        gs[g].position = {c[3], c[4], c[5]};
+        gs[g].velocity = {c[6], c[7], c[8]};
+        gs[g].orientation = c[9];
+        gs[g].group_id = (std::uint32_t)c[10];
+        gs[g].thickness = c[11];
+        gs[g].inclination = c[12];
+    }
+    const auto p = fmmgalaxy::generate_galaxies(gs, physics(G, eps), seed);
+    if (x)
+        for (size_t i = 0; i < p.size(); ++i) {
+            x[i] = p[i].position.x; y[i] = p[i].position.y; z[i] = p[i].position.z;
+            vx[i] = p[i].velocity.x; vy[i] = p[i].velocity.y; vz[i] = p[i].velocity.z;
+            m[i] = p[i].mass;
+            group[i] = p[i].group_id;
+        }
+    return (int64_t)p.size();
+}
+
 // The inputs of the reference smoke test's solver-agreement case (smoke_tests.cpp:83-89):
 // 80 bodies at U(-1,1)^3 drawn from mt19937_64(7), mass 1/80.
 void ref_smoke80_inputs(double* x, double* y, double* z, double* m) {
