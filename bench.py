@@ -726,7 +726,7 @@ def wl_fmm(gx, torch, args) -> dict:
     p2p_ach = near_int * FP64_OPS_PER_P2P_PAIR / (ph["near_field"] / 1e3) / 1e12
     m2p_ach = stats.far_pairs * FP64_OPS_PER_M2P_PAIR / (ph["far_field"] / 1e3) / 1e12
     dominant = "near_field" if ph["near_field"] >= ph["far_field"] else "far_field"
-    roof = {"bound": "fp64_pipe", "kernel": "p2p_kernel (FP64 near field)" if dominant == "near_field"
+    roof = {"bound": "fp64_pipe", "kernel": "p2p_kernel<F64> (near field)" if dominant == "near_field"
             else "fmm_m2p_kernel<4> (far field)",
             "achieved": p2p_ach if dominant == "near_field" else m2p_ach, "peak": fp64_peak,
             "unit": "T FP64-pipe lane-ops/s",
@@ -738,7 +738,9 @@ def wl_fmm(gx, torch, args) -> dict:
                            "note": "phase = plan (count, scan) + kernel"},
             "far_field": {"pairs": stats.far_pairs, "ops_per_pair": FP64_OPS_PER_M2P_PAIR,
                           "phase_ms": ph["far_field"], "achieved": m2p_ach, "frac": m2p_ach / fp64_peak},
-            "traffic": None}
+            "traffic": None,
+            "traffic_note": "node records, bodies and lists stay in L2: ncu DRAM reads 7.7 MB (far) and 5.1 MB "
+                            "(near) per evaluation at this size (profiles/fmm_m2p_p2p_n65536_full.md)"}
 
     # e2e: the public API on host arrays (H2D of x, y, z, m and D2H of a inside the call)
     q = p.copy()

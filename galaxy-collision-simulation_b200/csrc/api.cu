@@ -1446,6 +1446,12 @@ int fmm_plan_host(FmmPlan& P, int64_t n, const double* hx, const double* hy, con
     }
     if (items.size() > (size_t)std::numeric_limits<int32_t>::max())
         return fail(GX_ERR_UNSUPPORTED, "FMM: too many far-field work items");
+    // largest items first (targets x nodes), as the device builder orders them
+    std::stable_sort(items.begin(), items.end(), [&](const M2PItem& u, const M2PItem& v) {
+        const int64_t cu = (int64_t)(T.leaf_off[u.leaf + 1] - T.leaf_off[u.leaf]) * (u.fe - u.fb);
+        const int64_t cv = (int64_t)(T.leaf_off[v.leaf + 1] - T.leaf_off[v.leaf]) * (v.fe - v.fb);
+        return cu > cv;
+    });
     fa.n_items = (int32_t)items.size();
     P.n_slots = slots;
     if (!items.empty()) GX_TRY(dev_copy(hs, items, &fa.items));
@@ -1584,6 +1590,21 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
     GX_TRY(dev_array(hs, fa.n_items, &items));
     la.items = items;
     GX_CUDA(launch_tree_lists_fill(la, nl, st));
+    // far-field items, largest first
+    M2PItem* sorted_items;
+    uint32_t *cost, *cost_alt;
+    int32_t *idx, *idx_alt;
+    GX_TRY(dev_array(hs, fa.n_items, &sorted_items));
+    GX_TRY(dev_array(hs, fa.n_items, &cost));
+    GX_TRY(dev_array(hs, fa.n_items, &cost_alt));
+    GX_TRY(dev_array(hs, fa.n_items, &idx));
+    GX_TRY(dev_array(hs, fa.n_items, &idx_alt));
+    const size_t order_bytes = item_order_temp_bytes(fa.n_items);
+    void* order_temp;
+    GX_TRY(dev_array(hs, (int64_t)order_bytes, (char**)&order_temp));
+    GX_CUDA(launch_item_order(items, la.leaf_off, fa.n_items, cost, cost_alt, idx, idx_alt, order_temp, order_bytes,
+                              sorted_items, st));
+    items = sorted_items;
     GX_TRY(mark(tm, 3, st));
     fa.leaf_off = la.leaf_off;
     fa.leaf_part = la.leaf_part;

@@ -70,4 +70,5 @@ constexpr int kM2PChunk = 512;  // far nodes per work item
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st);
 cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st);
 
+
 }  // namespace gx

@@ -590,6 +590,22 @@ __global__ void __launch_bounds__(256) items_kernel(const TreeListArgs a, int n_
     }
 }
 
+// Far-field items, largest first (cost = targets x nodes): fewer long items at the tail.
+__global__ void __launch_bounds__(256) item_cost_kernel(const M2PItem* items, const int32_t* leaf_off, int n,
+                                                        uint32_t* cost, int32_t* idx) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k >= n) return;
+    const M2PItem it = items[k];
+    cost[k] = (uint32_t)(leaf_off[it.leaf + 1] - leaf_off[it.leaf]) * (uint32_t)(it.fe - it.fb);
+    idx[k] = k;
+}
+
+__global__ void __launch_bounds__(256) item_gather_kernel(const M2PItem* items, const int32_t* idx, int n,
+                                                          M2PItem* out) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k < n) out[k] = items[idx[k]];
+}
+
 size_t scan_bytes(int count) {
     size_t b = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b, (const int32_t*)nullptr, (int32_t*)nullptr, count);
@@ -668,6 +684,28 @@ cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cuda
     walk_kernel<true><<<(n_leaves + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
     long_sort_kernel<<<296, 1024, 0, st>>>(a);
     items_kernel<<<(n_leaves + 255) / 256, 256, 0, st>>>(a, n_leaves);
+    return cudaGetLastError();
+}
+
+size_t item_order_temp_bytes(int32_t n_items) {
+    size_t b = 0;
+    cub::DoubleBuffer<uint32_t> k(nullptr, nullptr);
+    cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, b, k, v, n_items);
+    return b;
+}
+
+cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int32_t n_items, uint32_t* cost,
+                              uint32_t* cost_alt, int32_t* idx, int32_t* idx_alt, void* temp, size_t temp_bytes,
+                              M2PItem* out, cudaStream_t st) {
+    if (n_items == 0) return cudaSuccess;
+    const int g = (n_items + 255) / 256;
+    item_cost_kernel<<<g, 256, 0, st>>>(items, leaf_off, n_items, cost, idx);
+    cub::DoubleBuffer<uint32_t> k(cost, cost_alt);
+    cub::DoubleBuffer<int32_t> v(idx, idx_alt);
+    cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, temp_bytes, k, v, n_items, 0, 32, st);
+    if (e != cudaSuccess) return e;
+    item_gather_kernel<<<g, 256, 0, st>>>(items, v.Current(), n_items, out);
     return cudaGetLastError();
 }
 

@@ -104,5 +104,11 @@ size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes);
 cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
 // The fill walk (each leaf's lists sorted into depth-first order) and the far-field work items.
 cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st);
+// The far-field items reordered by decreasing cost (targets x nodes) into out.
+struct M2PItem;
+size_t item_order_temp_bytes(int32_t n_items);
+cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int32_t n_items, uint32_t* cost,
+                              uint32_t* cost_alt, int32_t* idx, int32_t* idx_alt, void* temp, size_t temp_bytes,
+                              M2PItem* out, cudaStream_t st);
 
 }  // namespace gx
