@@ -69,3 +69,38 @@ class ShardedLeapfrog:
         self.gather_positions(X)
         A.copy_(self.force(X, m, b, e))
         V.add_(A * h)
+
+
+def direct_force(params, precision=None) -> ForceFn:
+    """The engine's direct sum over all bodies for the owned targets (GPU tensors)."""
+    from . import _ffi
+    from .adjoint import _rows
+    prec = _ffi.PRECISION_F64 if precision is None else precision
+
+    def force(X: torch.Tensor, m: torch.Tensor, b: int, e: int) -> torch.Tensor:
+        A = torch.empty(3, e - b, dtype=X.dtype, device=X.device)
+        _ffi.call("gx_direct_accel_targets", X.shape[1], *_rows(X), m.data_ptr(), b, e, None, 0, params.ffi(),
+                  _ffi.precision_code(prec), *_rows(A), torch.cuda.current_stream().cuda_stream)
+        return A
+
+    return force
+
+
+def fmm_force(params, options=None, precision=None) -> ForceFn:
+    """The engine's FMM for the owned targets -- the reference's MPI FMM path
+    (compute_fmm_accelerations_for_targets, cpp/fmm/fmm_solver.cpp:324-333): every rank builds
+    the whole tree and evaluates its own range."""
+    from . import _ffi
+    from .fmm import FmmOptions, fmm_accelerations
+    prec = _ffi.PRECISION_F64 if precision is None else precision
+    opt = options or FmmOptions()
+
+    def force(X: torch.Tensor, m: torch.Tensor, b: int, e: int) -> torch.Tensor:
+        n = X.shape[1]
+        A = torch.zeros(3, n, dtype=X.dtype, device=X.device)
+        Xc = X.contiguous()
+        fmm_accelerations(Xc[0], Xc[1], Xc[2], m, A[0], A[1], A[2], params, opt, prec, b, e,
+                          stream=torch.cuda.current_stream().cuda_stream)
+        return A[:, b:e].clone()
+
+    return force
