@@ -830,7 +830,24 @@ def wl_snapshots(gx, torch, args) -> dict:
     finally:
         shutil.rmtree(out, ignore_errors=True)
     over = (res["with"]["device_ms"] - res["without"]["device_ms"]) / snaps
+    cpu = None
+    import oracle
+    if oracle.ref_available():
+        # the reference's SnapshotWriter on the same state (one snapshot, single thread)
+        ref_dir = tempfile.mkdtemp(prefix="gx_refsnap_")
+        try:
+            st0 = {k: getattr(p, k) for k in ("x", "y", "z", "vx", "vy", "vz")}
+            st0.update(ax=np.zeros(n), ay=np.zeros(n), az=np.zeros(n))
+            t0 = time.perf_counter()
+            oracle.ref_write_outputs(ref_dir, st0, p.m, None, 0, 0.0, np.zeros(13))
+            cs = time.perf_counter() - t0
+        finally:
+            shutil.rmtree(ref_dir, ignore_errors=True)
+        cpu = {"value": cs * 1e3, "unit": "ms", "cores": 1, "kind": "reference",
+               "sample": "SnapshotWriter::write_snapshot of the same N=2^20 state (the reference writes on the "
+                         "step loop's own thread, after a full device-to-host copy)"}
     return {"metric": "stream time per snapshot (N=2^20, device copy)", "value": float(np.median(copies)),
+            "cpu_baseline": cpu,
             "unit": "ms", "step_overhead_ms_per_snapshot": over,
             "higher_is_better": False, "steps": steps, "snapshot_every": every, "snapshots": snaps,
             "step_ms_without": res["without"]["device_ms"] / steps, "step_ms_with": res["with"]["device_ms"] / steps,
