@@ -119,8 +119,22 @@ __global__ void __launch_bounds__(kScanBlock) p2p_scan_kernel(const P2PArgs a) {
     }
 }
 
+// Slot-ordered copy of the sources: src[k] = (x, y, z, m) of body leaf_part[k], for every
+// leaf slot k, when the slots fit the buffer (cap of them; a CSR that lists a body in
+// several leaves can have more, and the leaf kernel then reads through leaf_part).
+__global__ void __launch_bounds__(256) p2p_gather_kernel(const P2PArgs a, int64_t cap) {
+    const int64_t np = a.leaf_off[a.n_leaves];
+    const bool ok = np <= cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.src_ok = ok ? 1 : 0;
+    if (!ok) return;
+    for (int64_t k = (int64_t)blockIdx.x * 256 + threadIdx.x; k < np; k += (int64_t)gridDim.x * 256) {
+        const int j = a.leaf_part[k];
+        a.src[k] = make_double4(a.x[j], a.y[j], a.z[j], a.m[j]);
+    }
+}
+
 template <int MODE, bool EPS0>
-__global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
+__global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
     __shared__ __align__(16) double sxd[kP2PJT];
     __shared__ __align__(16) double syd[kP2PJT];
     __shared__ __align__(16) double szd[kP2PJT];
@@ -131,8 +145,13 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
     __shared__ double s_red[6][kP2PBlock];
     __shared__ int s_item, s_last;
 
+    // body indices of the staged sources are needed only to skip the target itself where a
+    // zero distance does not already give a zero term
+    constexpr bool kNeedIdx = MODE == kF64Exact || EPS0;
+    constexpr int kStageU = kP2PJT / kP2PBlock;  // slots a thread stages per pass
     const int tid = threadIdx.x;
     const int n_items = *a.plan_n_items;
+    const bool by_slot = *a.src_ok != 0;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(a.ticket, 1);
         __syncthreads();
@@ -161,22 +180,22 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
         const int first = a.leaf_part[tb];
         const double ox = a.x[first], oy = a.y[first], oz = a.z[first];
 
-        auto stage = [&](int c, int j) {
-            sidx[c] = j;
+        auto stage = [&](int c, const double4 q, int j) {
+            if (kNeedIdx) sidx[c] = j;
             if (MODE == kMixed) {
                 float* sxf = reinterpret_cast<float*>(sxd);
                 float* syf = reinterpret_cast<float*>(syd);
                 float* szf = reinterpret_cast<float*>(szd);
                 float* smf = reinterpret_cast<float*>(smd);
-                sxf[c] = __double2float_rn(a.x[j] - ox);
-                syf[c] = __double2float_rn(a.y[j] - oy);
-                szf[c] = __double2float_rn(a.z[j] - oz);
-                smf[c] = __double2float_rn(a.m[j]);
+                sxf[c] = __double2float_rn(q.x - ox);
+                syf[c] = __double2float_rn(q.y - oy);
+                szf[c] = __double2float_rn(q.z - oz);
+                smf[c] = __double2float_rn(q.w);
             } else {
-                sxd[c] = a.x[j];
-                syd[c] = a.y[j];
-                szd[c] = a.z[j];
-                smd[c] = a.m[j];
+                sxd[c] = q.x;
+                syd[c] = q.y;
+                szd[c] = q.z;
+                smd[c] = q.w;
             }
         };
         // Every source slot [c_lo, c_hi) of this item staged kP2PJT at a time, compute(take)
@@ -214,16 +233,40 @@ __global__ void __launch_bounds__(kP2PBlock) p2p_kernel(const P2PArgs a) {
                 const int b_hi = (int)min((int64_t)total, c_hi - base);
                 for (int c0 = b_lo; c0 < b_hi; c0 += kP2PJT) {
                     const int take = min(kP2PJT, b_hi - c0);
-                    for (int c = tid; c < take; c += kP2PBlock) {
-                        const int sl = c0 + c;
-                        int l2 = 0, h2 = cnt;  // s_pre[l2] <= sl < s_pre[h2]
-                        while (h2 - l2 > 1) {
-                            const int mid = (l2 + h2) >> 1;
-                            if (s_pre[mid] <= sl) l2 = mid;
-                            else h2 = mid;
+                    // a thread's kStageU slots: positions first, then all loads, then the
+                    // stores, so that the loads of the slots are in flight together
+                    int pos[kStageU];
+#pragma unroll
+                    for (int u = 0; u < kStageU; ++u) {
+                        const int sl = c0 + tid + u * kP2PBlock;
+                        pos[u] = -1;
+                        if (tid + u * kP2PBlock < take) {
+                            int l2 = 0, h2 = cnt;  // s_pre[l2] <= sl < s_pre[h2]
+                            while (h2 - l2 > 1) {
+                                const int mid = (l2 + h2) >> 1;
+                                if (s_pre[mid] <= sl) l2 = mid;
+                                else h2 = mid;
+                            }
+                            pos[u] = s_beg[l2] + (sl - s_pre[l2]);
                         }
-                        stage(c, a.leaf_part[s_beg[l2] + (sl - s_pre[l2])]);
                     }
+                    double4 q[kStageU];
+                    int jx[kStageU];
+#pragma unroll
+                    for (int u = 0; u < kStageU; ++u) {
+                        if (pos[u] < 0) continue;
+                        if (by_slot) {
+                            q[u] = a.src[pos[u]];
+                            jx[u] = kNeedIdx ? a.leaf_part[pos[u]] : 0;
+                        } else {
+                            const int j = a.leaf_part[pos[u]];
+                            q[u] = make_double4(a.x[j], a.y[j], a.z[j], a.m[j]);
+                            jx[u] = j;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kStageU; ++u)
+                        if (pos[u] >= 0) stage(tid + u * kP2PBlock, q[u], jx[u]);
                     __syncthreads();
                     compute(take);
                     __syncthreads();
@@ -434,8 +477,10 @@ size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves) {
     // plan arrays (src and scratch offsets int64; chunks, item offsets, done counters int),
     // n_items + ticket, and the partial sums: a split leaf holds at most kMaxChunks partials
     // for each of its bodies.
+    // plus the slot-ordered sources (n of them, 32 bytes each).
     const size_t nl = (size_t)n_leaves + 1;
-    return nl * (8 + 8 + 4 + 4 + 4) + 128 + (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n;
+    return nl * (8 + 8 + 4 + 4 + 4) + 128 + (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n +
+           (size_t)n * sizeof(double4) + 32;
 }
 
 cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch, int sms, cudaStream_t st) {
@@ -456,12 +501,17 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     p = (char*)(((uintptr_t)p + 63) & ~(uintptr_t)63);
     a.plan_n_items = (int*)p;
     a.ticket = (int*)p + 1;
+    a.src_ok = (int*)p + 2;
     p += 64;
     a.scratch = (double*)p;
     a.scratch_capacity = (int64_t)kMaxChunks * n_bodies;
+    p += (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n_bodies;
+    p = (char*)(((uintptr_t)p + 31) & ~(uintptr_t)31);
+    a.src = (double4*)p;
     cudaError_t e = cudaMemsetAsync(a.plan_done, 0, nl * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
+    p2p_gather_kernel<<<sms * 8, 256, 0, st>>>(a, n_bodies);
     p2p_count_kernel<<<(a.n_leaves + 7) / 8, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0);
     p2p_scan_kernel<<<1, kScanBlock, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -31,6 +31,10 @@ struct P2PArgs {
     int* plan_done;         // chunks finished per leaf
     int* plan_n_items;
     int* ticket;
+    // (x, y, z, m) of leaf_part[k] at slot k, gathered once per launch when the leaf slots
+    // fit the buffer (src_ok); sources are then read by slot, without the leaf_part hop
+    double4* src;
+    int* src_ok;
     double* scratch;
     int64_t scratch_capacity;  // partial-sum slots (targets) the scratch holds
 };

@@ -65,6 +65,23 @@ def fmm1000():
                         **{f"{k}20": s20[k] for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}, **lists)
 
 
+def readme1000():
+    """experiments/validation/readme_1000_body_collision: the reference's 299-step FMM run
+    (dt 0.012, theta 0.58, leaf 16, softening 0.025, order 4) -- its step-0 state, the
+    accelerations at step 10, positions and velocities at steps 10, 40, 100 and 299, and every
+    diagnostics row."""
+    d = REF / "experiments/validation/readme_1000_body_collision"
+    s0 = load_csv(d / "snapshot_000000.csv")
+    out = {f"{k}0": s0[k] for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+    for step in (10, 40, 100, 299):
+        s = load_csv(d / f"snapshot_{step:06d}.csv")
+        keys = ("x", "y", "z", "vx", "vy", "vz") + (("ax", "ay", "az") if step == 10 else ())
+        out.update({f"{k}{step}": s[k] for k in keys})
+    np.savez_compressed(OUT / "readme1000.npz", m=s0["m"], group=s0["group"], diagnostics=load_diag(d / "diagnostics.csv"),
+                        dt=0.012, theta=0.58, leaf_capacity=16, softening=0.025, steps=299,
+                        checkpoints=np.array([10, 40, 100, 299]), **out)
+
+
 def cfg0():
     sys.path.insert(0, str(ROOT))
     import importlib.util
@@ -90,5 +107,6 @@ if __name__ == "__main__":
     smoke80()
     fmm1000()
     cfg0()
+    readme1000()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)

@@ -77,6 +77,26 @@ def test_fmm_leaf_lists_and_p2p(golden):
     assert np.array_equal(acc, golden_acc)
 
 
+def test_readme_run_diagnostics(golden):
+    """experiments/validation/readme_1000_body_collision: the oracle's diagnostics of the
+    reference's step-0 and step-10 states equal rows 0 and 10 of its diagnostics.csv, and
+    (where the reference library is built) its FMM of the step-0 state equals the snapshot's
+    accelerations."""
+    g = golden("readme1000.npz")
+    eps, diag = float(g["softening"]), g["diagnostics"]
+    for k in (0, 10):
+        d = oracle.diagnostics(*(g[f"{v}{k}"] for v in STATE[:6]), g["m"], 1.0, eps)
+        np.testing.assert_allclose(d, diag[k, 3:], rtol=1e-13, atol=1e-15)
+    if oracle.ref_available():
+        theta, cap = float(g["theta"]), int(g["leaf_capacity"])
+        a = oracle.ref_fmm(g["x0"], g["y0"], g["z0"], g["m"], 1.0, eps, theta, cap)
+        assert np.array_equal(a, np.stack([g["ax0"], g["ay0"], g["az0"]], 1))
+        # the reference's own KDK + FMM, rebuilt here, reproduces its published step 10 to a
+        # few ulps (the run is chaotic: the gap grows about tenfold every 20 steps)
+        s = oracle.ref_leapfrog_fmm({k: g[f"{k}0"] for k in STATE}, g["m"], 1.0, eps, float(g["dt"]), 10, theta, cap)
+        assert max(np.abs(s[k] - g[f"{k}10"]).max() for k in STATE) <= 1e-15
+
+
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built in this tree")
 def test_oracle_vs_reference_random():
     rng = np.random.default_rng(11)
