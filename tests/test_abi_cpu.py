@@ -14,7 +14,7 @@ from gx import _ffi
 
 def header_functions():
     text = _ffi.HEADER_PATH.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(gx_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(gx_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
