@@ -24,24 +24,41 @@
 // The exact form uses one chunk per leaf and one lane per target and walks the sources in
 // the reference's order starting from the incoming acceleration (the far field), which
 // makes it bit-identical to the reference's evaluate_particle.
+#include <algorithm>
+
+#include <cub/device/device_scan.cuh>
+
 #include "gx_device.cuh"
 #include "p2p.cuh"
 
 namespace gx {
 namespace {
 
-constexpr int kP2PBlock = 128;
-constexpr int kP2PJT = 512;      // sources staged per shared-memory pass
 constexpr int kNearBatch = 256;  // near leaves whose (start, length) sit in shared memory at once
 constexpr int kMaxChunks = 8;    // a leaf's source sequence is split into at most this many items
-constexpr int kMinChunk = 2048;  // ... of at least this many sources
-constexpr int kScanBlock = 1024;
+constexpr int kMinChunk = 256;   // ... of at least this many sources
+constexpr int kMinGroup = 8;     // targets of a group, when a leaf's targets are split
+constexpr int kStageCost = 8;    // staging one source costs about this many interactions
+constexpr int kWarpBlockMaxMean = 12;  // mean bodies per leaf up to which blocks are one warp
 
-// Per leaf (one warp each): number of sources, number of chunks, scratch demand (split
-// leaves only).
-__global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exact) {
+// Per leaf (one warp each): number of sources, and the split of the leaf into target groups
+// x source chunks of cost at most about item_cost each, where an item of g targets and s
+// sources costs s x (g + kStageCost).  Target groups need no partial sums, so a heavy leaf
+// is cut into groups first when kMaxChunks chunks would still leave items above item_cost.
+// A split leaf needs chunks partial sums per target; chunks <= kMaxChunks keeps the total
+// within kMaxChunks x (leaf slots), and leaves are not split at all when the slots exceed
+// split_max_slots (a CSR that repeats bodies).  Entry n_leaves of the counts is zero, so
+// that the exclusive scans end with the totals.
+__global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exact, int64_t item_cost) {
     const int l = (int)((blockIdx.x * 256u + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (l >= a.n_leaves) return;
+    if (l > a.n_leaves) return;
+    if (l == a.n_leaves) {
+        if (lane == 0) {
+            a.plan_cnt[l] = 0;
+            a.plan_need[l] = 0;
+        }
+        return;
+    }
     int64_t src = 0;
     for (int q = a.near_off[l] + lane; q < a.near_off[l + 1]; q += 32) {
         const int s = a.near_leaf[q];
@@ -50,73 +67,27 @@ __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exa
     for (int o = 16; o > 0; o >>= 1) src += __shfl_xor_sync(0xffffffffu, src, o);
     if (lane != 0) return;
     const int nt = a.leaf_off[l + 1] - a.leaf_off[l];
-    int chunks = 0;
+    int chunks = 0, groups = 1;
     if (nt > 0 && src > 0) {
-        const int64_t c = (src + kMinChunk - 1) / kMinChunk;
-        chunks = exact ? 1 : (int)(c < kMaxChunks ? c : kMaxChunks);
+        chunks = 1;
+        if (!exact) {
+            const int64_t cap = kMaxChunks * item_cost;
+            int64_t g = nt;
+            if (src * (g + kStageCost) > cap) g = max((int64_t)kMinGroup, cap / src - kStageCost);
+            g = min(g, (int64_t)nt);
+            groups = (int)((nt + g - 1) / g);
+            g = (nt + groups - 1) / groups;  // equal groups
+            const int64_t c_cost = (src * (g + kStageCost) + item_cost - 1) / item_cost;
+            const int64_t c_src = (src + kMinChunk - 1) / kMinChunk;
+            chunks = (int)max((int64_t)1, min((int64_t)kMaxChunks, min(c_cost, c_src)));
+            if (a.leaf_off[a.n_leaves] > a.split_max_slots) chunks = 1;
+        }
     }
     a.plan_src[l] = src;
     a.plan_chunks[l] = chunks;
-    a.plan_scratch[l] = chunks > 1 ? (int64_t)chunks * nt : 0;
-}
-
-// Single-block exclusive scans: item offsets (plan_item_off, n_leaves + 1 entries) and
-// scratch offsets (plan_scratch rewritten in place as offsets, in units of targets).
-__global__ void __launch_bounds__(kScanBlock) p2p_scan_kernel(const P2PArgs a) {
-    __shared__ int64_t s_a[kScanBlock];
-    __shared__ int64_t s_b[kScanBlock];
-    const int n = a.n_leaves;
-    const int per = (n + kScanBlock - 1) / kScanBlock;
-    const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
-    int64_t ta = 0, tb = 0;
-    for (int l = b0; l < b1; ++l) {
-        ta += a.plan_chunks[l];
-        tb += a.plan_scratch[l];
-    }
-    s_a[threadIdx.x] = ta;
-    s_b[threadIdx.x] = tb;
-    __syncthreads();
-    // Capacity guard: if the split leaves would need more partial sums than the scratch holds
-    // (rows that repeat bodies can do that), every leaf falls back to a single chunk.
-    __shared__ int64_t s_demand;
-    if (threadIdx.x == 0) {
-        int64_t d = 0;
-        for (int w = 0; w < kScanBlock; ++w) d += s_b[w];
-        s_demand = d;
-    }
-    __syncthreads();
-    if (s_demand > a.scratch_capacity) {
-        ta = 0;
-        for (int l = b0; l < b1; ++l) {
-            if (a.plan_chunks[l] > 1) a.plan_chunks[l] = 1;
-            a.plan_scratch[l] = 0;
-            ta += a.plan_chunks[l];
-        }
-        s_a[threadIdx.x] = ta;
-        s_b[threadIdx.x] = 0;
-        __syncthreads();
-    }
-    for (int o = 1; o < kScanBlock; o <<= 1) {  // Hillis-Steele inclusive scan
-        const int64_t va = threadIdx.x >= (unsigned)o ? s_a[threadIdx.x - o] : 0;
-        const int64_t vb = threadIdx.x >= (unsigned)o ? s_b[threadIdx.x - o] : 0;
-        __syncthreads();
-        s_a[threadIdx.x] += va;
-        s_b[threadIdx.x] += vb;
-        __syncthreads();
-    }
-    int64_t ra = threadIdx.x ? s_a[threadIdx.x - 1] : 0;
-    int64_t rb = threadIdx.x ? s_b[threadIdx.x - 1] : 0;
-    for (int l = b0; l < b1; ++l) {
-        const int64_t ca = a.plan_chunks[l], cb = a.plan_scratch[l];
-        a.plan_item_off[l] = (int)ra;
-        a.plan_scratch[l] = rb;
-        ra += ca;
-        rb += cb;
-    }
-    if (threadIdx.x == kScanBlock - 1) {
-        a.plan_item_off[n] = (int)s_a[kScanBlock - 1];
-        *a.plan_n_items = (int)s_a[kScanBlock - 1];
-    }
+    a.plan_groups[l] = groups;
+    a.plan_cnt[l] = chunks * groups;
+    a.plan_need[l] = chunks > 1 ? (int64_t)chunks * nt : 0;
 }
 
 // Slot-ordered copy of the sources: src[k] = (x, y, z, m) of body leaf_part[k], for every
@@ -133,8 +104,12 @@ __global__ void __launch_bounds__(256) p2p_gather_kernel(const P2PArgs a, int64_
     }
 }
 
-template <int MODE, bool EPS0>
-__global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
+// BS threads per block (a multiple of 32), 4 x BS sources staged per pass; the launch
+// bounds keep 640 threads (20 warps) resident per SM whatever BS.
+template <int MODE, bool EPS0, int BS>
+__global__ void __launch_bounds__(BS, 640 / BS) p2p_kernel(const P2PArgs a) {
+    constexpr int kP2PBlock = BS;
+    constexpr int kP2PJT = 4 * BS;  // sources staged per shared-memory pass
     __shared__ __align__(16) double sxd[kP2PJT];
     __shared__ __align__(16) double syd[kP2PJT];
     __shared__ __align__(16) double szd[kP2PJT];
@@ -166,8 +141,9 @@ __global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
             else hi = mid;
         }
         const int leaf = lo;
-        const int chunks = a.plan_chunks[leaf];
-        const int chunk = item - a.plan_item_off[leaf];
+        const int chunks = a.plan_chunks[leaf], groups = a.plan_groups[leaf];
+        const int local = item - a.plan_item_off[leaf];
+        const int chunk = local % chunks, group = local / chunks;
         const int64_t src = a.plan_src[leaf];
         const int64_t per = (src + chunks - 1) / chunks;
         const int64_t c_lo = (int64_t)chunk * per;
@@ -175,6 +151,9 @@ __global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
 
         const int tb = a.leaf_off[leaf];
         const int nt = a.leaf_off[leaf + 1] - tb;
+        // this item's targets: group `group` of `groups` equal groups of the leaf's bodies
+        const int gsz = (nt + groups - 1) / groups;
+        const int g_lo = group * gsz, g_hi = min(nt, g_lo + gsz);
         const int nb = a.near_off[leaf], ne = a.near_off[leaf + 1];
         // Origin of the mixed form: the leaf's first body (near sources are close to it).
         const int first = a.leaf_part[tb];
@@ -321,8 +300,8 @@ __global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
             // H rows of two (row r holds targets r and r + H); every row gets L = block / H
             // lanes that split the staged sources, and a row's L partial sums are added in
             // lane order in shared memory.
-            for (int t0 = 0; t0 < nt; t0 += 2 * kP2PBlock) {
-                const int ntp = min(2 * kP2PBlock, nt - t0);
+            for (int t0 = g_lo; t0 < g_hi; t0 += 2 * kP2PBlock) {
+                const int ntp = min(2 * kP2PBlock, g_hi - t0);
                 const int H = (ntp + 1) >> 1;
                 const int L = max(1, kP2PBlock / H);
                 const bool act = tid < H * L;
@@ -430,7 +409,7 @@ __global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
         // Split leaf: the CTA that completes its last chunk adds the partials in chunk order.
         __threadfence();
         __syncthreads();
-        if (tid == 0) s_last = (atomicAdd(&a.plan_done[leaf], 1) == chunks - 1);
+        if (tid == 0) s_last = (atomicAdd(&a.plan_done[leaf], 1) == chunks * groups - 1);
         __syncthreads();
         if (!s_last) continue;
         __threadfence();
@@ -451,12 +430,12 @@ __global__ void __launch_bounds__(kP2PBlock, 5) p2p_kernel(const P2PArgs a) {
     }
 }
 
-template <int MODE, bool EPS0>
+template <int MODE, bool EPS0, int BS>
 int p2p_occupancy() {
     static int occ = 0;
     if (occ == 0) {
         int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, p2p_kernel<MODE, EPS0>, kP2PBlock, 0) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, p2p_kernel<MODE, EPS0, BS>, BS, 0) != cudaSuccess ||
             nb < 1)
             nb = 1;
         occ = nb;
@@ -464,23 +443,39 @@ int p2p_occupancy() {
     return occ;
 }
 
-template <int MODE, bool EPS0>
+template <int MODE, bool EPS0, int BS>
 cudaError_t launch_main(const P2PArgs& a, int sms, cudaStream_t st) {
-    const int grid = sms * p2p_occupancy<MODE, EPS0>();
-    p2p_kernel<MODE, EPS0><<<grid, kP2PBlock, 0, st>>>(a);
+    const int grid = sms * p2p_occupancy<MODE, EPS0, BS>();
+    p2p_kernel<MODE, EPS0, BS><<<grid, BS, 0, st>>>(a);
     return cudaGetLastError();
+}
+
+template <int MODE, bool EPS0>
+cudaError_t launch_bs(const P2PArgs& a, int bs, int sms, cudaStream_t st) {
+    return bs == 32 ? launch_main<MODE, EPS0, 32>(a, sms, st) : launch_main<MODE, EPS0, 128>(a, sms, st);
+}
+
+}  // namespace
+
+namespace {
+
+size_t plan_scan_temp_bytes(int32_t n_leaves) {
+    size_t b1 = 0, b2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b1, (const int*)nullptr, (int*)nullptr, n_leaves + 1);
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, (const int64_t*)nullptr, (int64_t*)nullptr, n_leaves + 1);
+    return (std::max(b1, b2) + 255) & ~(size_t)255;
 }
 
 }  // namespace
 
 size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves) {
-    // plan arrays (src and scratch offsets int64; chunks, item offsets, done counters int),
-    // n_items + ticket, and the partial sums: a split leaf holds at most kMaxChunks partials
-    // for each of its bodies.
-    // plus the slot-ordered sources (n of them, 32 bytes each).
+    // plan arrays (src, need and scratch offsets int64; chunks, groups, counts, item offsets,
+    // done counters int), the scan's temporary storage, src_ok + ticket, the partial sums (at
+    // most kMaxChunks per leaf slot, leaf slots <= n when leaves are split), and the
+    // slot-ordered sources (32 bytes per body); 256 bytes of alignment per piece.
     const size_t nl = (size_t)n_leaves + 1;
-    return nl * (8 + 8 + 4 + 4 + 4) + 128 + (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n +
-           (size_t)n * sizeof(double4) + 32;
+    return nl * (3 * 8 + 5 * 4) + plan_scan_temp_bytes(n_leaves) + 4 * 256 +
+           (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n + (size_t)n * sizeof(double4);
 }
 
 cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch, int sms, cudaStream_t st) {
@@ -488,36 +483,49 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     const bool eps0 = precision == kMixed ? (a.eps2f < 1e-24f) : (a.eps2 < 1e-200);
     const size_t nl = (size_t)a.n_leaves + 1;
     char* p = (char*)scratch;
-    a.plan_src = (int64_t*)p;
-    p += nl * 8;
-    a.plan_scratch = (int64_t*)p;
-    p += nl * 8;
-    a.plan_chunks = (int*)p;
-    p += nl * 4;
-    a.plan_item_off = (int*)p;
-    p += nl * 4;
-    a.plan_done = (int*)p;
-    p += nl * 4;
-    p = (char*)(((uintptr_t)p + 63) & ~(uintptr_t)63);
-    a.plan_n_items = (int*)p;
-    a.ticket = (int*)p + 1;
-    a.src_ok = (int*)p + 2;
-    p += 64;
-    a.scratch = (double*)p;
-    a.scratch_capacity = (int64_t)kMaxChunks * n_bodies;
-    p += (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n_bodies;
-    p = (char*)(((uintptr_t)p + 31) & ~(uintptr_t)31);
-    a.src = (double4*)p;
+    auto carve = [&](size_t bytes) {
+        char* q = p;
+        p += bytes;
+        return q;
+    };
+    auto align = [&] { p = (char*)(((uintptr_t)p + 255) & ~(uintptr_t)255); };
+    a.plan_src = (int64_t*)carve(nl * 8);
+    a.plan_need = (int64_t*)carve(nl * 8);
+    a.plan_scratch = (int64_t*)carve(nl * 8);
+    a.plan_chunks = (int*)carve(nl * 4);
+    a.plan_groups = (int*)carve(nl * 4);
+    a.plan_cnt = (int*)carve(nl * 4);
+    a.plan_item_off = (int*)carve(nl * 4);
+    a.plan_done = (int*)carve(nl * 4);
+    a.plan_n_items = a.plan_item_off + a.n_leaves;
+    align();
+    size_t temp_bytes = plan_scan_temp_bytes(a.n_leaves);
+    void* temp = carve(temp_bytes);
+    align();
+    a.ticket = (int*)carve(256);
+    a.src_ok = a.ticket + 1;
+    a.scratch = (double*)carve((size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n_bodies);
+    align();
+    a.src = (double4*)carve((size_t)n_bodies * sizeof(double4));
+    a.split_max_slots = n_bodies;
+    // Block size: with few bodies per leaf a leaf's item is small, and one-warp blocks (20
+    // independent warps per SM, no block-wide barriers) hide the latency of its gathers;
+    // larger leaves keep 4-warp blocks that share each staged source among more threads.
+    const int bs = n_bodies <= (int64_t)kWarpBlockMaxMean * a.n_leaves ? 32 : 128;
+    const int64_t item_cost = (int64_t)1024 * bs;
     cudaError_t e = cudaMemsetAsync(a.plan_done, 0, nl * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     p2p_gather_kernel<<<sms * 8, 256, 0, st>>>(a, n_bodies);
-    p2p_count_kernel<<<(a.n_leaves + 7) / 8, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0);
-    p2p_scan_kernel<<<1, kScanBlock, 0, st>>>(a);
+    p2p_count_kernel<<<(a.n_leaves + 8) / 8, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0, item_cost);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (precision == kF64Exact) return launch_main<kF64Exact, false>(a, sms, st);
-    if (precision == kF64) return eps0 ? launch_main<kF64, true>(a, sms, st) : launch_main<kF64, false>(a, sms, st);
-    return eps0 ? launch_main<kMixed, true>(a, sms, st) : launch_main<kMixed, false>(a, sms, st);
+    if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, a.plan_cnt, a.plan_item_off, (int)nl, st)) != cudaSuccess)
+        return e;
+    if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
+        return e;
+    if (precision == kF64Exact) return launch_bs<kF64Exact, false>(a, bs, sms, st);
+    if (precision == kF64) return eps0 ? launch_bs<kF64, true>(a, bs, sms, st) : launch_bs<kF64, false>(a, bs, sms, st);
+    return eps0 ? launch_bs<kMixed, true>(a, bs, sms, st) : launch_bs<kMixed, false>(a, bs, sms, st);
 }
 
 }  // namespace gx

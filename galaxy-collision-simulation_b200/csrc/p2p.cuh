@@ -25,18 +25,21 @@ struct P2PArgs {
     float eps2f;
     // work plan and partial sums, carved from the scratch passed to launch_p2p
     int64_t* plan_src;      // sources per leaf
-    int64_t* plan_scratch;  // per-leaf offset of its partial sums (split leaves), in targets
-    int* plan_chunks;       // items per leaf
-    int* plan_item_off;     // n_leaves + 1 item offsets
-    int* plan_done;         // chunks finished per leaf
-    int* plan_n_items;
+    int64_t* plan_need;     // partial sums a split leaf needs (chunks x targets), n_leaves + 1
+    int64_t* plan_scratch;  // per-leaf offset of its partial sums (exclusive scan of plan_need)
+    int* plan_chunks;       // source chunks per leaf
+    int* plan_groups;       // target groups per leaf
+    int* plan_cnt;          // items per leaf (groups x chunks), n_leaves + 1
+    int* plan_item_off;     // exclusive scan of plan_cnt
+    int* plan_done;         // items finished per leaf
+    int* plan_n_items;      // = plan_item_off + n_leaves
     int* ticket;
     // (x, y, z, m) of leaf_part[k] at slot k, gathered once per launch when the leaf slots
     // fit the buffer (src_ok); sources are then read by slot, without the leaf_part hop
     double4* src;
     int* src_ok;
     double* scratch;
-    int64_t scratch_capacity;  // partial-sum slots (targets) the scratch holds
+    int64_t split_max_slots;  // leaves are split only if their slots number at most this
 };
 
 // Device scratch launch_p2p needs for n bodies and n_leaves leaves.
