@@ -1285,8 +1285,14 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
     for (int32_t l = 0; l < n_leaves; ++l)
         if (leaf_offsets[l + 1] < leaf_offsets[l] || near_offsets[l + 1] < near_offsets[l])
             return fail(GX_ERR_INVALID_ARGUMENT, "%s: CSR offsets must be non-decreasing", fn);
-    for (int32_t k = 0; k < n_lp; ++k)
-        if (leaf_particles[k] < 0 || leaf_particles[k] >= n) return fail(GX_ERR_INVALID_ARGUMENT, "%s: body index out of range", fn);
+    {
+        std::vector<unsigned char> seen((size_t)n, 0);
+        for (int32_t k = 0; k < n_lp; ++k) {
+            const int32_t i = leaf_particles[k];
+            if (i < 0 || i >= n) return fail(GX_ERR_INVALID_ARGUMENT, "%s: body index out of range", fn);
+            if (seen[(size_t)i]++) return fail(GX_ERR_INVALID_ARGUMENT, "%s: body %d listed in two leaf slots", fn, (int)i);
+        }
+    }
     for (int32_t k = 0; k < n_nl; ++k)
         if (near_leaves[k] < 0 || near_leaves[k] >= n_leaves) return fail(GX_ERR_INVALID_ARGUMENT, "%s: leaf id out of range", fn);
     HostStage hs(st);

@@ -170,7 +170,10 @@ int gx_session_autotune(gx_session* s, int precision, double* best_ms);
 /* For every body i of leaf l (leaf_particles[leaf_offsets[l] .. leaf_offsets[l+1]]),
  * adds sum over near leaves s of leaf l (near_leaves[near_offsets[l] .. [l+1]]) and their
  * bodies j != i of the pair term to (ax[i], ay[i], az[i]).  Leaf ids are row numbers of
- * leaf_offsets.  Pass the far field in a to get the reference's full FMM result. */
+ * leaf_offsets.  Pass the far field in a to get the reference's full FMM result.  Each body
+ * sits in at most one leaf slot, as in the reference's octree: host CSR arrays that list a
+ * body twice are rejected (GX_ERR_INVALID_ARGUMENT); device CSR arrays are trusted, and a
+ * body listed twice there gets an unspecified sum (the kernel stays within its buffers). */
 int gx_p2p_leaves(int64_t n, const double* x, const double* y, const double* z,
                   const double* m, int32_t n_leaves, const int32_t* leaf_offsets,
                   const int32_t* leaf_particles, const int32_t* near_offsets,

@@ -68,6 +68,48 @@ def test_zero_softening_and_deep_coincident_leaves():
             assert rel_err(got, ref).max() <= 1e-11
 
 
+def window_lists(n, per_leaf, k, seed):
+    """Synthetic leaf lists: the bodies in a random order cut into leaves of per_leaf, each
+    leaf's near list the leaves within k of it, ascending."""
+    perm = np.random.default_rng(seed).permutation(n).astype(np.int32)
+    nl = (n + per_leaf - 1) // per_leaf
+    lo = np.minimum(np.arange(nl + 1) * per_leaf, n).astype(np.int32)
+    near = [np.arange(max(0, l - k), min(nl, l + k + 1), dtype=np.int32) for l in range(nl)]
+    no = np.zeros(nl + 1, np.int32)
+    no[1:] = np.cumsum([len(v) for v in near])
+    return gx.LeafLists(lo, perm, no, np.concatenate(near))
+
+
+@pytest.mark.parametrize("per_leaf,k", [(12, 900), (64, 150)])
+def test_heavy_leaves_split_into_groups_and_chunks(per_leaf, k):
+    """Leaves with ~20,000 sources each: the plan cuts them into target groups and source
+    chunks (partial sums merged in chunk order), with one-warp blocks (12 bodies per leaf) and
+    four-warp blocks (64 per leaf)."""
+    n = 24000
+    rng = np.random.default_rng(per_leaf)
+    x, y, z = (rng.uniform(-1, 1, n) for _ in range(3))
+    m = rng.uniform(0.5, 1.5, n) / n
+    lists = window_lists(n, per_leaf, k, 7)
+    L = dict(leaf_offsets=lists.leaf_offsets, leaf_particles=lists.leaf_particles, near_offsets=lists.near_offsets,
+             near_leaves=lists.near_leaves)
+    ref = oracle.p2p_near(x, y, z, m, 1.0, 0.02, L)
+    assert np.array_equal(run_p2p(x, y, z, m, lists, 0.02, EXACT), ref)
+    e = rel_err(run_p2p(x, y, z, m, lists, 0.02, F64), ref)
+    assert np.median(e) <= 1e-13 and e.max() <= 1e-11
+    e = rel_err(run_p2p(x, y, z, m, lists, 0.02, MIX), ref)
+    assert np.median(e) <= 1e-6 and e.max() <= 1e-4
+
+
+def test_host_lists_with_a_repeated_body_are_rejected():
+    p = gx.ics.two_disk_encounter(500, 500, 29, 0.02)
+    lists = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 16)
+    lp = lists.leaf_particles.copy()
+    lp[5] = lp[0]
+    bad = gx.LeafLists(lists.leaf_offsets, lp, lists.near_offsets, lists.near_leaves)
+    with pytest.raises(gx.GxError, match="two leaf slots"):
+        run_p2p(p.x, p.y, p.z, p.m, bad, 0.02, F64)
+
+
 def test_device_arrays():
     p = gx.ics.two_disk_encounter(4000, 4000, 17, 0.02)
     lists = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 64)
