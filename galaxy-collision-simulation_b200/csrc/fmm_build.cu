@@ -306,15 +306,30 @@ __global__ void __launch_bounds__(256) walk_pack_kernel(const TreeListArgs a) {
     a.wn[k] = w;
 }
 
+// well_separated (fmm_solver.cpp:228-241): 2 (hw_t + hw_s) / dist < theta, dist != 0, with
+// the reference's operations.  The reference's quotient is within 1.5 ulp of the exact
+// num / sqrt(r2), so wherever num^2 and theta^2 r2 (each within a few ulp) differ by more
+// than 1e-12 relative the squares give the same answer without the square root and the
+// division; only near-ties, and magnitudes where the squares could overflow or underflow,
+// take the reference's own operations.
+__device__ __forceinline__ bool well_separated(const WalkNode& T, const WalkNode& S, double theta) {
+    const double dx = dsub(S.cx, T.cx), dy = dsub(S.cy, T.cy), dz = dsub(S.cz, T.cz);
+    const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+    if (r2 == 0.0) return false;  // dist == 0
+    const double num = dmul(2.0, dadd(T.hw, S.hw));
+    const double lhs = dmul(num, num), rhs = dmul(dmul(theta, theta), r2);
+    if (theta > 0.0 && rhs > 1e-290 && rhs < 1e290 && lhs < 1e290) {
+        if (lhs < dmul(rhs, 1.0 - 1e-12)) return true;
+        if (lhs > dmul(rhs, 1.0 + 1e-12)) return false;
+    }
+    return __ddiv_rn(num, __dsqrt_rn(r2)) < theta;
+}
+
 // One node of the walk (build_leaf_interactions, fmm_solver.cpp:254-277): 1 far, 2 near,
-// 3 expand, 0 massless; well_separated (:228-241) with the reference's operations.
+// 3 expand, 0 massless.
 __device__ __forceinline__ int classify(const WalkNode& T, int t, const WalkNode& S, int s, double theta) {
     if (!(S.mass > 0.0)) return 0;
-    if (s != t) {
-        const double dx = dsub(S.cx, T.cx), dy = dsub(S.cy, T.cy), dz = dsub(S.cz, T.cz);
-        const double dist = __dsqrt_rn(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
-        if (dist != 0.0 && __ddiv_rn(dmul(2.0, dadd(T.hw, S.hw)), dist) < theta) return 1;
-    }
+    if (s != t && well_separated(T, S, theta)) return 1;
     return S.child < 0 ? 2 : 3;
 }
 
