@@ -30,6 +30,37 @@ def ownership_range(count: int, rank: int, size: int) -> tuple[int, int]:
     return begin, begin + base + (1 if rank < rem else 0)
 
 
+def partition_instances(sizes, world: int) -> list[list[int]]:
+    """Independent encounters of a batched ensemble over ranks, with no exchange between
+    them: instances in decreasing cost (N_b (N_b - 1) pair terms per force evaluation; ties
+    by index) each go to the rank with the least cost so far (lowest rank on ties).  Every
+    rank computes the same answer.  Returns each rank's instance indices, ascending."""
+    sizes = [int(v) for v in sizes]
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i] * (sizes[i] - 1), i))
+    load = [0] * max(1, world)
+    parts: list[list[int]] = [[] for _ in range(max(1, world))]
+    for i in order:
+        r = min(range(len(load)), key=lambda q: (load[q], q))
+        load[r] += sizes[i] * (sizes[i] - 1)
+        parts[r].append(i)
+    return [sorted(q) for q in parts]
+
+
+def ensemble_shard(offsets, rank: int, world: int):
+    """This rank's part of a batched ensemble given as concatenated bodies with instance
+    offsets (n_instances + 1): (instance ids, offsets of the rank's sub-batch, body indices
+    into the full arrays), from partition_instances."""
+    import numpy as np
+
+    off = np.asarray(offsets, dtype=np.int64)
+    sizes = np.diff(off)
+    ids = np.asarray(partition_instances(sizes, world)[rank] if world > 1 else range(len(sizes)), dtype=np.int64)
+    sub = np.zeros(len(ids) + 1, dtype=np.int64)
+    sub[1:] = np.cumsum(sizes[ids])
+    body = np.concatenate([np.arange(off[i], off[i + 1]) for i in ids]) if len(ids) else np.zeros(0, np.int64)
+    return ids, sub, body
+
+
 # force(X_full (3, n), m (n,), begin, end) -> A_owned (3, end - begin)
 ForceFn = Callable[[torch.Tensor, torch.Tensor, int, int], torch.Tensor]
 

@@ -14,7 +14,7 @@ import torch.multiprocessing as mp
 
 import conftest  # noqa: F401  (registers the engine package as `gx` in spawned ranks too)
 import oracle
-from gx.sharded import ShardedLeapfrog, ownership_range
+from gx.sharded import ShardedLeapfrog, ensemble_shard, ownership_range, partition_instances
 
 
 def _free_port():
@@ -77,3 +77,61 @@ def test_two_rank_step_matches_single_process(tmp_path, n):
     ref = oracle.leapfrog(st, p.m, 1.0, 0.05, 0.005, steps, solver=1)
     expect = np.stack([ref[k] for k in ("x", "y", "z", "vx", "vy", "vz")])
     assert np.array_equal(got, expect)
+
+
+def test_partition_instances_cover_and_balance():
+    import gx
+    off, _, _ = gx.ics.ensemble(512, seed=7)
+    sizes = np.diff(off)
+    cost = sizes * (sizes - 1)
+    for world in (1, 2, 3, 8):
+        parts = partition_instances(sizes, world)
+        assert len(parts) == world
+        flat = sorted(i for q in parts for i in q)
+        assert flat == list(range(512)) and all(q == sorted(q) for q in parts)
+        loads = [int(cost[q].sum()) for q in parts]
+        assert max(loads) <= 1.01 * sum(loads) / world
+    assert partition_instances([5, 5, 9], 2) == [[2], [0, 1]]
+
+
+def _ensemble_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import gx
+        off, p, _ = gx.ics.ensemble(6, seed=3, n_min=64, n_max=160)
+        ids, sub, body = ensemble_shard(off, rank, world)
+        # each rank steps its own encounters (oracle forces, per instance), no exchange
+        res = np.zeros((6, len(p.x)))
+        for q, i in enumerate(ids):
+            b = body[sub[q]:sub[q + 1]]
+            a = oracle.direct_targets(p.x[b], p.y[b], p.z[b], p.m[b], 1.0, 0.05)
+            st = dict(x=p.x[b], y=p.y[b], z=p.z[b], vx=p.vx[b], vy=p.vy[b], vz=p.vz[b], ax=a[:, 0], ay=a[:, 1],
+                      az=a[:, 2])
+            r = oracle.leapfrog(st, p.m[b], 1.0, 0.05, 0.005, 2, solver=1)
+            for k, name in enumerate(("x", "y", "z", "vx", "vy", "vz")):
+                res[k, b] = r[name]
+        t = torch.from_numpy(res)
+        dist.all_reduce(t)  # bodies are owned by exactly one rank: the sum assembles the state
+        if rank == 0:
+            np.save(out, t.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_ensemble_by_instance(tmp_path):
+    """Instances split over two gloo ranks and stepped independently equal the whole
+    ensemble stepped in one process."""
+    out = str(tmp_path / "ens.npy")
+    mp.start_processes(_ensemble_worker, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
+    got = np.load(out)
+    import gx
+    off, p, _ = gx.ics.ensemble(6, seed=3, n_min=64, n_max=160)
+    for i in range(6):
+        b = np.arange(off[i], off[i + 1])
+        a = oracle.direct_targets(p.x[b], p.y[b], p.z[b], p.m[b], 1.0, 0.05)
+        st = dict(x=p.x[b], y=p.y[b], z=p.z[b], vx=p.vx[b], vy=p.vy[b], vz=p.vz[b], ax=a[:, 0], ay=a[:, 1], az=a[:, 2])
+        r = oracle.leapfrog(st, p.m[b], 1.0, 0.05, 0.005, 2, solver=1)
+        for k, name in enumerate(("x", "y", "z", "vx", "vy", "vz")):
+            assert np.array_equal(got[k, b], r[name]), (i, name)
