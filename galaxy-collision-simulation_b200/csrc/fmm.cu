@@ -308,8 +308,9 @@ __device__ __forceinline__ void m2p_one(const double* __restrict__ r, double tx,
 
 // Shared-memory stride of a staged node record: slots 0..45 (16-byte multiple).
 constexpr int kStageStride = 46;
-constexpr int kM2PSub = 64;  // node records per shared-memory buffer
-constexpr size_t kM2PDynSmem = 2 * kM2PSub * kStageStride * sizeof(double);
+constexpr int kM2PSub = 64;     // node records per shared-memory buffer
+constexpr int kM2PStages = 2;   // buffers in the cp.async ring
+constexpr size_t kM2PDynSmem = (size_t)kM2PStages * kM2PSub * kStageStride * sizeof(double);
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -320,11 +321,12 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Work item = (target leaf, up to kM2PChunk far nodes).  The item's node records stream
-// through two shared-memory buffers of kM2PSub records: while the block evaluates one
-// buffer, cp.async fills the other.  Thread t evaluates target t % W against nodes t / W,
-// t / W + S, ... of each buffer (W = the leaf's targets, at most one block; S = block / W
-// node slots, so at most W - 1 threads idle); the S partial sums of a target are added in
-// slot order, so results do not depend on scheduling.
+// through a ring of kM2PStages shared-memory buffers: while the block evaluates one, cp.async
+// fills the next ones.  Thread t evaluates target t % W against nodes t / W, t / W + S, ...
+// of each buffer (W = the leaf's targets, at most one block; S = block / W node slots, so at
+// most W - 1 threads idle); a buffer is filled with a multiple of S records, so every slot
+// evaluates the same number of nodes between barriers.  The S partial sums of a target are
+// added in slot order, so results do not depend on scheduling.
 template <int P>
 __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
     constexpr int PIECES = P == 0 ? 2 : (P == 2 ? (kRecTrQ + 2) / 2 : kStageStride / 2);  // 16-byte pieces
@@ -335,21 +337,26 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
         const M2PItem w = a.items[it];
         const int cnt = w.fe - w.fb;
-        const int nsub = (cnt + kM2PSub - 1) / kM2PSub;
-        auto stage = [&](int sc) {
-            double* buf = s_dyn + (sc & 1) * (kM2PSub * kStageStride);
-            const int j0 = sc * kM2PSub, m = min(kM2PSub, cnt - j0);
-            for (int k = tid; k < m * PIECES; k += kM2PBlock) {
-                const int j = k / PIECES, pc = k - j * PIECES;
-                const double* src = a.rec + (size_t)a.far_node[w.fb + j0 + j] * kFmmRec + 2 * pc;
-                cp_async16(buf + j * kStageStride + 2 * pc, src);
-            }
-            cp_async_commit();
-        };
         const int tb = a.leaf_off[w.leaf], nt = a.leaf_off[w.leaf + 1] - tb;
         const int W = min(nt, kM2PBlock);
         const int S = kM2PBlock / W;
         const int q = tid / W, tl = tid - q * W;
+        const int R = S <= kM2PSub ? S * (kM2PSub / S) : kM2PSub;  // records per buffer
+        const int nsub = (cnt + R - 1) / R;
+        // fills buffer sc % kM2PStages with records sc * R ..; one commit group per call, empty
+        // past the end, so that the waits below count groups uniformly
+        auto stage = [&](int sc) {
+            if (sc < nsub) {
+                double* buf = s_dyn + (sc % kM2PStages) * (kM2PSub * kStageStride);
+                const int j0 = sc * R, m = min(R, cnt - j0);
+                for (int k = tid; k < m * PIECES; k += kM2PBlock) {
+                    const int j = k / PIECES, pc = k - j * PIECES;
+                    const double* src = a.rec + (size_t)a.far_node[w.fb + j0 + j] * kFmmRec + 2 * pc;
+                    cp_async16(buf + j * kStageStride + 2 * pc, src);
+                }
+            }
+            cp_async_commit();
+        };
         for (int t0 = 0; t0 < nt; t0 += W) {
             const int t = t0 + tl;
             double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -365,21 +372,18 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
                     i = -1;
                 }
             }
-            stage(0);
+            for (int sc = 0; sc < kM2PStages - 1; ++sc) stage(sc);
             for (int sc = 0; sc < nsub; ++sc) {
-                if (sc + 1 < nsub) {
-                    stage(sc + 1);
-                    cp_async_wait<1>();
-                } else {
-                    cp_async_wait<0>();
-                }
+                stage(sc + kM2PStages - 1);  // into the buffer released at the end of sc - 1
+                cp_async_wait<kM2PStages - 1>();
                 __syncthreads();
-                const double* buf = s_dyn + (sc & 1) * (kM2PSub * kStageStride);
-                const int m = min(kM2PSub, cnt - sc * kM2PSub);
+                const double* buf = s_dyn + (sc % kM2PStages) * (kM2PSub * kStageStride);
+                const int m = min(R, cnt - sc * R);
                 if (i >= 0)
                     for (int j = q; j < m; j += S) m2p_one<P>(buf + j * kStageStride, tx, ty, tz, a.eps2, fx, fy, fz);
-                __syncthreads();  // the next stage() overwrites this buffer
+                __syncthreads();  // a later stage() overwrites this buffer
             }
+            cp_async_wait<0>();  // the empty trailing groups
             s_red[tid * 3 + 0] = fx;
             s_red[tid * 3 + 1] = fy;
             s_red[tid * 3 + 2] = fz;
