@@ -6,24 +6,27 @@
 //
 // Work decomposition.  The bodies of a target leaf's near leaves form one source sequence
 // (near-list order, then leaf order).  Leaf costs are very uneven (in the N = 65,536
-// two-disk tree the heaviest leaf has 13x the mean number of sources), so a leaf's sequence
-// is cut into at most kMaxChunks chunks of at least kMinChunk sources.  A plan computed on
-// the device (p2p_count_kernel + p2p_scan_kernel) numbers the (leaf, chunk) items; a
-// persistent grid takes items from a ticket counter.  A leaf with one chunk adds its sums to
-// the accelerations directly.  A split leaf writes per-chunk partial sums to scratch; the CTA
-// that finishes the leaf's last chunk (a per-leaf counter, after a memory fence) adds the
-// partials in chunk order -- no CTA ever waits for another, and the order of summation does
-// not depend on scheduling.
+// two-disk tree the heaviest leaf has 13x the mean number of sources), so a leaf is cut into
+// target groups x source chunks (at most kMaxChunks chunks of at least kMinChunk sources),
+// items of bounded cost.  A plan computed on the device (p2p_count_kernel, then CUB scans)
+// numbers the items; a persistent grid takes them from a ticket counter.  Items of an
+// unsplit leaf add their sums to the accelerations directly (target groups are disjoint).
+// A leaf split into chunks writes per-chunk partial sums to scratch; the block that finishes
+// the leaf's last item (a per-leaf counter, after a memory fence) adds the partials in chunk
+// order -- no block ever waits for another, and the order of summation does not depend on
+// scheduling.
 //
-// Inside an item: a warp scan of the near leaves' sizes lets every thread gather its own
-// slots of the chunk (by index, from the SoA state) into shared memory JT at a time.  In the
-// fast forms every thread serves two targets (halving the shared-memory reads per
-// interaction): a leaf's targets form H rows of two, each row gets L = block / H threads
-// that split the staged sources (any L, so a 22-body leaf keeps 121 of 128 threads busy),
-// and a row's L partial sums are added in lane order.
-// The exact form uses one chunk per leaf and one lane per target and walks the sources in
-// the reference's order starting from the incoming acceleration (the far field), which
-// makes it bit-identical to the reference's evaluate_particle.
+// Inside an item: a warp scan of the near leaves' sizes lets every thread find its own
+// slots of the chunk and stage them into shared memory 4 x block at a time, from a copy of
+// (x, y, z, m) in leaf-slot order gathered once per launch.  In the fast forms every thread
+// serves two targets (halving the shared-memory reads per interaction): a group's targets
+// form H rows of two, each row gets L = block / H threads that split the staged sources (any
+// L, so a 22-body leaf keeps 121 of 128 threads busy), and a row's L partial sums are added
+// in lane order.  Blocks are one warp when the mean leaf is small (independent items hide the
+// gathers' latency) and four warps otherwise.
+// The exact form uses one chunk and one group per leaf and one lane per target, and walks
+// the sources in the reference's order starting from the incoming acceleration (the far
+// field), which makes it bit-identical to the reference's evaluate_particle.
 #include <algorithm>
 
 #include <cub/device/device_scan.cuh>
