@@ -1724,7 +1724,17 @@ int fmm_accel(const char* fn, int64_t n, const double* x, const double* y, const
         GX_CUDA(cudaMemsetAsync(done.p, 0, (size_t)P->n_leaves * sizeof(int), st));
         fa.scratch = part.d();
         fa.done = (int*)done.p;
-        GX_CUDA(launch_fmm_m2p(fa, st));
+        // the mixed form evaluates the far field in FP32 on FP64 offsets, from FP32 copies
+        // of the node records
+        AsyncBuf rec32;
+        const bool mixed = precision == kMixed;
+        fa.rec32 = nullptr;
+        fa.eps2f = (float)fa.eps2;
+        if (mixed) {
+            GX_TRY(rec32.alloc((size_t)std::max<int32_t>(fa.n_nodes, 1) * kRec32 * sizeof(float), st));
+            fa.rec32 = (float*)rec32.p;
+        }
+        GX_CUDA(launch_fmm_m2p(fa, mixed, st));
         GX_TRY(mark(tm.get(), 4, st));
 
         P2PArgs pa;

@@ -242,60 +242,64 @@ __global__ void __launch_bounds__(256) fmm_m2m_kernel(const FmmArgs a, int lb) {
     if (lane == 0) write_traces(r);
 }
 
-// One far node's contribution at one target (without the factor G).
-template <int P>
-__device__ __forceinline__ void m2p_one(const double* __restrict__ r, double tx, double ty, double tz, double eps2,
-                                        double& fx, double& fy, double& fz) {
-    const double dx = r[0] - tx, dy = r[1] - ty, dz = r[2] - tz;
-    const double s = dx * dx + dy * dy + dz * dz + eps2;
-    if (s == 0.0) return;  // h0 == 0 (multipole.cpp:272-275)
-    const double ri = rsqrt_f64(s);
-    const double r2 = ri * ri;
-    const double g1 = -ri * r2;
-    double cd = -r[kRecMass] * g1;  // coefficient of d
-    double vx = 0.0, vy = 0.0, vz = 0.0;
+__device__ __forceinline__ double rsqrt_t(double s) { return rsqrt_f64(s); }
+__device__ __forceinline__ float rsqrt_t(float s) { return rsqrt_f32(s); }
+
+// One far node's contribution at one target (without the factor G), from the offset d =
+// centre of mass - target and the node's values r[k] = record slot k (k >= 3).  T = double
+// is the FP64 far field; T = float the mixed-precision one (d taken in FP64, then rounded).
+template <int P, typename T>
+__device__ __forceinline__ void m2p_terms(const T* __restrict__ r, const T dx, const T dy, const T dz, const T eps2,
+                                          T& fx, T& fy, T& fz) {
+    const T s = dx * dx + dy * dy + dz * dz + eps2;
+    if (s == T(0)) return;  // h0 == 0 (multipole.cpp:272-275)
+    const T ri = rsqrt_t(s);
+    const T r2 = ri * ri;
+    const T g1 = -ri * r2;
+    T cd = -r[kRecMass] * g1;  // coefficient of d
+    T vx = T(0), vy = T(0), vz = T(0);
     if (P >= 2) {
-        const double g2 = -3.0 * g1 * r2, g3 = -5.0 * g2 * r2;
-        const double mx = r[4] * dx + r[5] * dy + r[6] * dz;
-        const double my = r[5] * dx + r[7] * dy + r[8] * dz;
-        const double mz = r[6] * dx + r[8] * dy + r[9] * dz;
-        const double mdd = dx * mx + dy * my + dz * mz;
-        cd -= 0.5 * (g3 * mdd + g2 * r[kRecTrQ]);
+        const T g2 = T(-3.0) * g1 * r2, g3 = T(-5.0) * g2 * r2;
+        const T mx = r[4] * dx + r[5] * dy + r[6] * dz;
+        const T my = r[5] * dx + r[7] * dy + r[8] * dz;
+        const T mz = r[6] * dx + r[8] * dy + r[9] * dz;
+        const T mdd = dx * mx + dy * my + dz * mz;
+        cd -= T(0.5) * (g3 * mdd + g2 * r[kRecTrQ]);
         vx -= g2 * mx;
         vy -= g2 * my;
         vz -= g2 * mz;
         if (P >= 4) {
-            const double g4 = -7.0 * g3 * r2, g5 = -9.0 * g4 * r2;
+            const T g4 = T(-7.0) * g3 * r2, g5 = T(-9.0) * g4 * r2;
             // degree-2 monomials of d weighted 2/nu!
-            const double qxx = dx * dx, qxy = 2.0 * dx * dy, qxz = 2.0 * dx * dz, qyy = dy * dy,
-                         qyz = 2.0 * dy * dz, qzz = dz * dz;
-            const double ox = r[10] * qxx + r[11] * qxy + r[12] * qxz + r[13] * qyy + r[14] * qyz + r[15] * qzz;
-            const double oy = r[11] * qxx + r[13] * qxy + r[14] * qxz + r[16] * qyy + r[17] * qyz + r[18] * qzz;
-            const double oz = r[12] * qxx + r[14] * qxy + r[15] * qxz + r[17] * qyy + r[18] * qyz + r[19] * qzz;
-            const double oddd = dx * ox + dy * oy + dz * oz;
-            const double wd = r[kRecW] * dx + r[kRecW + 1] * dy + r[kRecW + 2] * dz;
-            cd -= g4 * oddd * (1.0 / 6.0) + 0.5 * g3 * wd;
-            vx -= 0.5 * (g3 * ox + g2 * r[kRecW]);
-            vy -= 0.5 * (g3 * oy + g2 * r[kRecW + 1]);
-            vz -= 0.5 * (g3 * oz + g2 * r[kRecW + 2]);
+            const T qxx = dx * dx, qxy = T(2.0) * dx * dy, qxz = T(2.0) * dx * dz, qyy = dy * dy,
+                    qyz = T(2.0) * dy * dz, qzz = dz * dz;
+            const T ox = r[10] * qxx + r[11] * qxy + r[12] * qxz + r[13] * qyy + r[14] * qyz + r[15] * qzz;
+            const T oy = r[11] * qxx + r[13] * qxy + r[14] * qxz + r[16] * qyy + r[17] * qyz + r[18] * qzz;
+            const T oz = r[12] * qxx + r[14] * qxy + r[15] * qxz + r[17] * qyy + r[18] * qyz + r[19] * qzz;
+            const T oddd = dx * ox + dy * oy + dz * oz;
+            const T wd = r[kRecW] * dx + r[kRecW + 1] * dy + r[kRecW + 2] * dz;
+            cd -= g4 * oddd * T(1.0 / 6.0) + T(0.5) * g3 * wd;
+            vx -= T(0.5) * (g3 * ox + g2 * r[kRecW]);
+            vy -= T(0.5) * (g3 * oy + g2 * r[kRecW + 1]);
+            vz -= T(0.5) * (g3 * oz + g2 * r[kRecW + 2]);
             // degree-3 monomials of d weighted 6/mu!
-            const double cxxx = qxx * dx, cxxy = 3.0 * qxx * dy, cxxz = 3.0 * qxx * dz, cxyy = 3.0 * dx * qyy,
-                         cxyz = 3.0 * qxy * dz, cxzz = 3.0 * dx * qzz, cyyy = qyy * dy, cyyz = 3.0 * qyy * dz,
-                         cyzz = 3.0 * dy * qzz, czzz = qzz * dz;
-            const double hx = r[20] * cxxx + r[21] * cxxy + r[22] * cxxz + r[23] * cxyy + r[24] * cxyz +
-                              r[25] * cxzz + r[26] * cyyy + r[27] * cyyz + r[28] * cyzz + r[29] * czzz;
-            const double hy = r[21] * cxxx + r[23] * cxxy + r[24] * cxxz + r[26] * cxyy + r[27] * cxyz +
-                              r[28] * cxzz + r[30] * cyyy + r[31] * cyyz + r[32] * cyzz + r[33] * czzz;
-            const double hz = r[22] * cxxx + r[24] * cxxy + r[25] * cxxz + r[27] * cxyy + r[28] * cxyz +
-                              r[29] * cxzz + r[31] * cyyy + r[32] * cyyz + r[33] * cyzz + r[34] * czzz;
-            const double hdddd = dx * hx + dy * hy + dz * hz;
-            const double* T = r + kRecT2;  // xx xy xz yy yz zz
-            const double tx2 = T[0] * dx + T[1] * dy + T[2] * dz;
-            const double ty2 = T[1] * dx + T[3] * dy + T[4] * dz;
-            const double tz2 = T[2] * dx + T[4] * dy + T[5] * dz;
-            const double tdd = dx * tx2 + dy * ty2 + dz * tz2;
-            cd -= g5 * hdddd * (1.0 / 24.0) + 0.25 * g4 * tdd + 0.125 * g3 * r[kRecTr2];
-            const double k4 = g4 * (1.0 / 6.0), k3 = 0.5 * g3;
+            const T cxxx = qxx * dx, cxxy = T(3.0) * qxx * dy, cxxz = T(3.0) * qxx * dz, cxyy = T(3.0) * dx * qyy,
+                    cxyz = T(3.0) * qxy * dz, cxzz = T(3.0) * dx * qzz, cyyy = qyy * dy, cyyz = T(3.0) * qyy * dz,
+                    cyzz = T(3.0) * dy * qzz, czzz = qzz * dz;
+            const T hx = r[20] * cxxx + r[21] * cxxy + r[22] * cxxz + r[23] * cxyy + r[24] * cxyz + r[25] * cxzz +
+                         r[26] * cyyy + r[27] * cyyz + r[28] * cyzz + r[29] * czzz;
+            const T hy = r[21] * cxxx + r[23] * cxxy + r[24] * cxxz + r[26] * cxyy + r[27] * cxyz + r[28] * cxzz +
+                         r[30] * cyyy + r[31] * cyyz + r[32] * cyzz + r[33] * czzz;
+            const T hz = r[22] * cxxx + r[24] * cxxy + r[25] * cxxz + r[27] * cxyy + r[28] * cxyz + r[29] * cxzz +
+                         r[31] * cyyy + r[32] * cyyz + r[33] * cyzz + r[34] * czzz;
+            const T hdddd = dx * hx + dy * hy + dz * hz;
+            const T* Tq = r + kRecT2;  // xx xy xz yy yz zz
+            const T tx2 = Tq[0] * dx + Tq[1] * dy + Tq[2] * dz;
+            const T ty2 = Tq[1] * dx + Tq[3] * dy + Tq[4] * dz;
+            const T tz2 = Tq[2] * dx + Tq[4] * dy + Tq[5] * dz;
+            const T tdd = dx * tx2 + dy * ty2 + dz * tz2;
+            cd -= g5 * hdddd * T(1.0 / 24.0) + T(0.25) * g4 * tdd + T(0.125) * g3 * r[kRecTr2];
+            const T k4 = g4 * T(1.0 / 6.0), k3 = T(0.5) * g3;
             vx -= k4 * hx + k3 * tx2;
             vy -= k4 * hy + k3 * ty2;
             vz -= k4 * hz + k3 * tz2;
@@ -306,11 +310,41 @@ __device__ __forceinline__ void m2p_one(const double* __restrict__ r, double tx,
     fz += cd * dz + vz;
 }
 
-// Shared-memory stride of a staged node record: slots 0..45 (16-byte multiple).
-constexpr int kStageStride = 46;
+// A staged record at one target: the FP64 record, or the mixed record (kRec32 layout).
+template <int P>
+__device__ __forceinline__ void m2p_one(const double* __restrict__ r, double tx, double ty, double tz, double eps2,
+                                        double& fx, double& fy, double& fz) {
+    m2p_terms<P, double>(r, r[0] - tx, r[1] - ty, r[2] - tz, eps2, fx, fy, fz);
+}
+template <int P>
+__device__ __forceinline__ void m2p_one(const float* __restrict__ r, double tx, double ty, double tz, float eps2,
+                                        float& fx, float& fy, float& fz) {
+    const double* com = reinterpret_cast<const double*>(r);
+    m2p_terms<P, float>(r + 3, (float)(com[0] - tx), (float)(com[1] - ty), (float)(com[2] - tz), eps2, fx, fy, fz);
+}
+
+// The mixed-precision records (kRec32) from the FP64 ones, one thread per node.
+__global__ void __launch_bounds__(256) fmm_rec32_kernel(const FmmArgs a) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k >= a.n_nodes) return;
+    const double* r = a.rec + (size_t)k * kFmmRec;
+    float* o = a.rec32 + (size_t)k * kRec32;
+    double* oc = reinterpret_cast<double*>(o);
+    oc[0] = r[0];
+    oc[1] = r[1];
+    oc[2] = r[2];
+    for (int q = kRecMass; q <= kRecTr2; ++q) o[q + 3] = __double2float_rn(r[q]);
+    for (int q = kRecTr2 + 4; q < kRec32; ++q) o[q] = 0.0f;
+}
+
+// Shared-memory stride of a staged node record, in elements: slots 0..45 of an FP64 record
+// (16-byte multiple), or a whole mixed record.
+template <typename T>
+__host__ __device__ constexpr int stage_stride() { return sizeof(T) == 8 ? 46 : kRec32; }
 constexpr int kM2PSub = 64;     // node records per shared-memory buffer
 constexpr int kM2PStages = 2;   // buffers in the cp.async ring
-constexpr size_t kM2PDynSmem = (size_t)kM2PStages * kM2PSub * kStageStride * sizeof(double);
+template <typename T>
+constexpr size_t m2p_dyn_smem() { return (size_t)kM2PStages * kM2PSub * stage_stride<T>() * sizeof(T); }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -327,10 +361,19 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // most W - 1 threads idle); a buffer is filled with a multiple of S records, so every slot
 // evaluates the same number of nodes between barriers.  The S partial sums of a target are
 // added in slot order, so results do not depend on scheduling.
-template <int P>
+template <int P, typename T>
 __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
-    constexpr int PIECES = P == 0 ? 2 : (P == 2 ? (kRecTrQ + 2) / 2 : kStageStride / 2);  // 16-byte pieces
-    extern __shared__ __align__(16) double s_dyn[];
+    // record elements the order reads, staged in 16-byte pieces
+    constexpr bool F64 = sizeof(T) == 8;
+    constexpr int kElems = F64 ? (P == 0 ? 4 : P == 2 ? kRecTrQ + 1 : 46) : (P == 0 ? 7 : P == 2 ? kRecTrQ + 4 : kRecTr2 + 4);
+    constexpr int PIECES = (kElems * (int)sizeof(T) + 15) / 16;
+    constexpr int kPer = 16 / (int)sizeof(T);  // elements per piece
+    constexpr int kStride = stage_stride<T>();
+    constexpr int kGlobal = F64 ? kFmmRec : kRec32;  // record stride in global memory
+    const T* rec = F64 ? reinterpret_cast<const T*>(a.rec) : reinterpret_cast<const T*>(a.rec32);
+    const T eps2 = F64 ? (T)a.eps2 : (T)a.eps2f;
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    T* s_dyn = reinterpret_cast<T*>(s_raw);
     __shared__ double s_red[kM2PBlock * 3];
     __shared__ int s_last;
     const int tid = threadIdx.x;
@@ -347,19 +390,19 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
         // past the end, so that the waits below count groups uniformly
         auto stage = [&](int sc) {
             if (sc < nsub) {
-                double* buf = s_dyn + (sc % kM2PStages) * (kM2PSub * kStageStride);
+                T* buf = s_dyn + (sc % kM2PStages) * (kM2PSub * kStride);
                 const int j0 = sc * R, m = min(R, cnt - j0);
                 for (int k = tid; k < m * PIECES; k += kM2PBlock) {
                     const int j = k / PIECES, pc = k - j * PIECES;
-                    const double* src = a.rec + (size_t)a.far_node[w.fb + j0 + j] * kFmmRec + 2 * pc;
-                    cp_async16(buf + j * kStageStride + 2 * pc, src);
+                    const T* src = rec + (size_t)a.far_node[w.fb + j0 + j] * kGlobal + kPer * pc;
+                    cp_async16(buf + j * kStride + kPer * pc, src);
                 }
             }
             cp_async_commit();
         };
         for (int t0 = 0; t0 < nt; t0 += W) {
             const int t = t0 + tl;
-            double fx = 0.0, fy = 0.0, fz = 0.0;
+            T fx = T(0), fy = T(0), fz = T(0);
             int i = -1;
             double tx = 0.0, ty = 0.0, tz = 0.0;
             if (q < S && t < nt) {
@@ -377,16 +420,16 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
                 stage(sc + kM2PStages - 1);  // into the buffer released at the end of sc - 1
                 cp_async_wait<kM2PStages - 1>();
                 __syncthreads();
-                const double* buf = s_dyn + (sc % kM2PStages) * (kM2PSub * kStageStride);
+                const T* buf = s_dyn + (sc % kM2PStages) * (kM2PSub * kStride);
                 const int m = min(R, cnt - sc * R);
                 if (i >= 0)
-                    for (int j = q; j < m; j += S) m2p_one<P>(buf + j * kStageStride, tx, ty, tz, a.eps2, fx, fy, fz);
+                    for (int j = q; j < m; j += S) m2p_one<P>(buf + j * kStride, tx, ty, tz, eps2, fx, fy, fz);
                 __syncthreads();  // a later stage() overwrites this buffer
             }
             cp_async_wait<0>();  // the empty trailing groups
-            s_red[tid * 3 + 0] = fx;
-            s_red[tid * 3 + 1] = fy;
-            s_red[tid * 3 + 2] = fz;
+            s_red[tid * 3 + 0] = (double)fx;
+            s_red[tid * 3 + 1] = (double)fy;
+            s_red[tid * 3 + 2] = (double)fz;
             __syncthreads();
             if (q == 0 && i >= 0) {
                 double sx = 0.0, sy = 0.0, sz = 0.0;
@@ -437,21 +480,31 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
     }
 }
 
-template <int P>
+template <int P, typename T>
 cudaError_t launch_m2p_order(const FmmArgs& a, cudaStream_t st) {
     // the shared-memory opt-in is a per-device setting of the kernel
     static std::atomic<unsigned long long> set_on{0};
+    constexpr size_t smem = m2p_dyn_smem<T>();
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(set_on.load() & bit)) {
-        e = cudaFuncSetAttribute(fmm_m2p_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kM2PDynSmem);
+        e = cudaFuncSetAttribute(fmm_m2p_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         set_on.fetch_or(bit);
     }
-    fmm_m2p_kernel<P><<<std::min(a.n_items, 1 << 20), kM2PBlock, kM2PDynSmem, st>>>(a);
+    fmm_m2p_kernel<P, T><<<std::min(a.n_items, 1 << 20), kM2PBlock, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_m2p_type(const FmmArgs& a, cudaStream_t st) {
+    switch (a.order) {
+        case 0: return launch_m2p_order<0, T>(a, st);
+        case 2: return launch_m2p_order<2, T>(a, st);
+        default: return launch_m2p_order<4, T>(a, st);
+    }
 }
 
 }  // namespace
@@ -478,13 +531,12 @@ cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, 
     return cudaSuccess;
 }
 
-cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st) {
+cudaError_t launch_fmm_m2p(const FmmArgs& a, bool mixed, cudaStream_t st) {
     if (a.n_items == 0) return cudaSuccess;
-    switch (a.order) {
-        case 0: return launch_m2p_order<0>(a, st);
-        case 2: return launch_m2p_order<2>(a, st);
-        default: return launch_m2p_order<4>(a, st);
-    }
+    if (!mixed) return launch_m2p_type<double>(a, st);
+    fmm_rec32_kernel<<<(a.n_nodes + 255) / 256, 256, 0, st>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e != cudaSuccess ? e : launch_m2p_type<float>(a, st);
 }
 
 }  // namespace gx

@@ -19,6 +19,11 @@ namespace gx {
 constexpr int kFmmRec = 48;
 constexpr int kRecMass = 3, kRecMom = 4, kRecTrQ = 35, kRecW = 36, kRecT2 = 39, kRecTr2 = 45;
 
+// The record of the mixed-precision far field, 52 floats (208 B): the centre of mass as
+// three doubles in floats [0..5] (offsets to the targets are taken in FP64), then slots
+// 3..45 of the FP64 record rounded to FP32 in floats [6..48], zero padding to [51].
+constexpr int kRec32 = 52;
+
 // Far-field work item: one target leaf and a chunk of its far list.
 struct M2PItem {
     int32_t leaf;
@@ -48,7 +53,8 @@ struct FmmArgs {
     const int32_t* leaf_off;
     const int32_t* leaf_part;
     const int32_t* far_node;
-    double* rec;  // n_nodes * kFmmRec
+    double* rec;   // n_nodes * kFmmRec
+    float* rec32;  // n_nodes * kRec32, mixed-precision far field only
     const M2PItem* items;
     int32_t n_items;
     double* scratch;  // partial sums of split leaves: 3 doubles per (chunk, target)
@@ -59,6 +65,7 @@ struct FmmArgs {
     int64_t t_begin, t_end;  // only bodies in [t_begin, t_end) are written
     double G;
     double eps2;
+    float eps2f;
     int order;  // effective expansion order: 0, 2 or 4
 };
 
@@ -68,7 +75,8 @@ constexpr int kM2PChunk = 512;  // far nodes per work item
 
 // Stream-ordered: leaf moments, then one launch per level (deepest first), then M2P.
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st);
-cudaError_t launch_fmm_m2p(const FmmArgs& a, cudaStream_t st);
+// mixed: FP32 multipole arithmetic on FP64 offsets (fills a.rec32 from a.rec first); else FP64.
+cudaError_t launch_fmm_m2p(const FmmArgs& a, bool mixed, cudaStream_t st);
 
 
 }  // namespace gx

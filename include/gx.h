@@ -262,9 +262,11 @@ typedef struct gx_fmm_stats {
 
 /* compute_fmm_accelerations_for_targets (fmm_solver.cpp:324-333); begin = 0, end = n is
  * compute_fmm_accelerations (:315-322).  The reference octree, its interaction lists,
- * the node moments (bit-identical to the reference's), the multipole far field (FP64)
- * and the P2P near field (in `precision`) all run on the device; trees deeper than 21
- * levels are built on the host.  Only bodies in [begin, min(end, n)) are written; bodies
+ * the node moments (bit-identical to the reference's), the multipole far field and the
+ * P2P near field all run on the device; trees deeper than 21 levels are built on the host.
+ * GX_PRECISION_F64 and _F64_EXACT evaluate the far field in FP64 (the exact form also makes
+ * the near field bit-identical to the reference's loop); GX_PRECISION_MIXED evaluates both
+ * fields in FP32 arithmetic on offsets taken in FP64.  Only bodies in [begin, min(end, n)) are written; bodies
  * of massless leaves get zero, as in the reference.  Masses must be >= 0 (host arrays are
  * checked).  Host or device arrays; `stats` may be NULL. */
 int gx_fmm_accel(int64_t n, const double* x, const double* y, const double* z, const double* m,

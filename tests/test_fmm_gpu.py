@@ -132,6 +132,19 @@ def test_smoke80_solver_agreement(golden):
     assert np.mean(rel_err(a, d)) < 1e-2
 
 
+@pytest.mark.parametrize("order", [0, 2, 4])
+def test_mixed_precision_fmm(order):
+    """The mixed form evaluates both fields in FP32 arithmetic on FP64 offsets (far field:
+    FP32 multipole terms on centre-of-mass offsets taken in FP64)."""
+    p = gx.ics.two_disk_encounter(6000, 3000, 40 + order, 0.02)
+    for cap in (8, 64):
+        f64, st = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, cap, order)
+        assert st.far_pairs > 0
+        a, _ = fmm(p.x, p.y, p.z, p.m, 0.02, 0.6, cap, order, prec=MIX)
+        e = rel_err(a, f64)
+        assert np.median(e) <= 1e-6 and e.max() <= 1e-4, (cap, np.median(e), e.max())
+
+
 @pytest.mark.parametrize("prec", [MIX, EXACT])
 def test_near_field_precisions(prec):
     p = gx.ics.two_disk_encounter(4000, 4000, 14, 0.02)
