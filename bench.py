@@ -786,13 +786,40 @@ def wl_fmm(gx, torch, args) -> dict:
         q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
     e2e = e2e_steps / (time.perf_counter() - t0)
 
+    # the mixed form (both fields in FP32 arithmetic on FP64 offsets) on the same system
+    Dm = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    Am = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(3)]
+
+    def step_mixed():
+        gx._ffi.call("gx_kick_drift", n, *P3(Dm["x"], Dm["y"], Dm["z"], Dm["vx"], Dm["vy"], Dm["vz"], *Am), 0.5 * dt, dt,
+                     sp)
+        gx.fmm.fmm_accelerations(Dm["x"], Dm["y"], Dm["z"], Dm["m"], *Am, params, opt, gx.PRECISION_MIXED, stream=sp)
+        gx._ffi.call("gx_kick", n, *P3(Dm["vx"], Dm["vy"], Dm["vz"], *Am), 0.5 * dt, sp)
+
+    with torch.cuda.stream(st):
+        gx.fmm.fmm_accelerations(Dm["x"], Dm["y"], Dm["z"], Dm["m"], *Am, params, opt, gx.PRECISION_MIXED, stream=sp)
+        am0 = torch.stack(Am, 1).cpu().numpy()
+        for _ in range(max(3, args.warmup)):
+            step_mixed()
+        st.synchronize()
+        m0, m1 = _events(torch)
+        m0.record(st)
+        for _ in range(steps):
+            step_mixed()
+        m1.record(st)
+        m1.synchronize()
+        ms_mixed = m0.elapsed_time(m1) / steps
+    em = np.linalg.norm(am0 - a0, axis=1) / np.linalg.norm(a0, axis=1)
+    mixed = {"value": 1e3 / ms_mixed, "unit": "steps/s", "ms_per_step": ms_mixed,
+             "rel_err_vs_f64": {"median": float(np.median(em)), "max": float(em.max()), "bodies": n}}
+
     out = {"metric": "FMM KDK steps/s (N=65536, leaf 64, theta 0.6, p=4, FP64)", "value": 1e3 / ms,
            "unit": "steps/s", "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "phases_ms_per_eval": ph, "stats": stats.__dict__,
            "gpu_launches": steps * (19 + stats.tree_levels + 2),
            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 3 * n * 8},
-           "roofline": roof, "clocks": clk,
+           "roofline": roof, "clocks": clk, "mixed": mixed,
            "config": {"workload": "fmm-n65536", "n": n, "leaf_capacity": cap, "theta": theta, "expansion_order": 4,
                       "softening": eps, "dt": dt, "near_field_precision": "f64",
                       "l2": "inputs (5 MiB) stay L2-resident; not flushed between steps"}}
