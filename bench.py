@@ -193,9 +193,10 @@ def main():
     ap.add_argument("--fit-iters", type=int, default=30, help="Adam iterations of the fit workload")
     ap.add_argument("--sharded", action="store_true",
                     help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
+    ap.add_argument("--leaf-capacity", type=int, default=64, help="leaf capacity of the fmm-evals workload")
     ap.add_argument("--workload", default="mixed-n1048576",
-                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "snapshots-n1048576", "ics-ensemble512", "p2p-n65536",
-                             "direct-n65536", "direct-n1000", "fit-n16384"],
+                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "fmm-evals", "snapshots-n1048576",
+                             "ics-ensemble512", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
                     help="headline (default) or one of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
@@ -841,6 +842,38 @@ def wl_fmm(gx, torch, args) -> dict:
     return out
 
 
+def wl_fmm_evals(gx, torch, args) -> dict:
+    """FMM force evaluations alone (no KDK step) of the N = 65,536 two-disk system (eps 0.02,
+    theta 0.6, order 4) on device arrays, with --leaf-capacity and --precision (f64 or mixed):
+    --warmup untimed evaluations, then --steps timed ones.  The case the FMM kernel profiles
+    capture (the P2P and M2P launches of one evaluation)."""
+    n, eps = 65536, 0.02
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, eps)
+    prec = gx.PRECISION_MIXED if args.precision == "mixed" else gx.PRECISION_F64
+    params, opt = gx.PhysicsParams(1.0, eps), gx.FmmOptions(0.6, args.leaf_capacity, 32, 4)
+    D = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("x", "y", "z", "m")}
+    A = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(3)]
+
+    def evaluate():
+        return gx.fmm.fmm_accelerations(D["x"], D["y"], D["z"], D["m"], *A, params, opt, prec)
+
+    for _ in range(args.warmup):
+        evaluate()
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    e0.record()
+    for _ in range(args.steps):
+        st = evaluate()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    return {"metric": "FMM evaluations/s (N=65536)", "value": 1e3 / ms, "unit": "evaluations/s", "ms_per_eval": ms,
+            "steps": args.steps, "warmup": args.warmup, "stats": st.__dict__, "dtype": args.precision,
+            "note": "includes the two host synchronisations of each evaluation (list sizes)",
+            "config": {"workload": "fmm-evals", "n": n, "leaf_capacity": args.leaf_capacity, "theta": 0.6,
+                       "expansion_order": 4, "softening": eps, "precision": args.precision}}
+
+
 def wl_snapshots(gx, torch, args) -> dict:
     """Snapshot output from the resident N = 2^20 session (mixed precision): 20 KDK steps with
     a snapshot (reference CSV + binary) every 5 steps vs the same steps without; the stepping
@@ -967,6 +1000,7 @@ def wl_ics(gx, torch, args) -> dict:
 OTHER_WORKLOADS = {
     "ensemble": wl_ensemble,
     "fmm-n65536": wl_fmm,
+    "fmm-evals": wl_fmm_evals,
     "snapshots-n1048576": wl_snapshots,
     "ics-ensemble512": wl_ics,
     "p2p-n65536": wl_p2p,
