@@ -36,7 +36,11 @@ namespace {
 constexpr int kBboxThreads = 256;
 constexpr int kBuildThreads = 1024;
 constexpr int kWalkThreads = 128;  // 4 warps, one leaf each
-constexpr int kWalkStack = 2048;   // shared stack slots per warp
+constexpr int kWalkStack = 1792;   // shared stack slots per warp
+// near lists up to this many entries are sorted in the warp's stack buffer (a bitonic network
+// pads to a power of two, so the largest power of two that fits kWalkStack / 2 keys)
+constexpr int pow2_floor(int v) { return v < 2 ? v : 2 * pow2_floor(v / 2); }
+constexpr int kSortCap = pow2_floor(kWalkStack / 2);
 constexpr int kStack = 7 * (kKeyLevels + 1) + 8;
 
 __global__ void __launch_bounds__(kBboxThreads) bbox_partial_kernel(const TreeBuildArgs t) {
@@ -337,8 +341,7 @@ __device__ __forceinline__ int classify(const WalkNode& T, int t, const WalkNode
 // out in that order: a bitonic sort in the shared buffer buf (kWalkStack / 2 slots) when the
 // list fits, else every key's rank (the number of smaller keys) computed from global memory.
 __device__ void sort_into(const uint64_t* v, int n, uint64_t* buf, int lane, int32_t* out) {
-    constexpr int kCap = kWalkStack / 2;
-    if (n <= kCap) {
+    if (n <= kSortCap) {
         int P = 1;
         while (P < n) P <<= 1;
         for (int i = lane; i < P; i += 32) buf[i] = i < n ? v[i] : ~0ull;
@@ -378,7 +381,7 @@ __device__ void sort_into(const uint64_t* v, int n, uint64_t* buf, int lane, int
 // (leaf ordinals are depth-first numbers), which the near field's exact form relies on.  When the stack would overflow, every lane finishes its share of
 // the pending nodes depth first with a private stack.
 template <bool FILL>
-__global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a) {
+__global__ void __launch_bounds__(kWalkThreads, 8) walk_kernel(const TreeListArgs a) {
     constexpr int W = kWalkThreads / 32;
     __shared__ __align__(16) int s_stk[W][kWalkStack];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -497,7 +500,7 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(const TreeListArgs a
         // the near list into the reference's depth-first order (leaf ordinals are depth-first
         // numbers)
         __syncwarp();
-        if (nn <= kWalkStack / 2) {
+        if (nn <= kSortCap) {
             sort_into(a.near_key + no, nn, reinterpret_cast<uint64_t*>(stk), lane, a.near_leaf + no);
         } else if (lane == 0) {
             a.long_leaf[atomicAdd(a.long_count, 1)] = l;  // sorted by long_sort_kernel
