@@ -166,14 +166,25 @@ def cpu_reference_rate(p, eps, seconds: float = 10.0, threads: int | None = None
 
 
 # ---------------------------------------------------------------------------------------
-# profiles: DRAM traffic of the dominant kernel from the committed ncu summary
+# DRAM traffic of the timed force launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)
 # ---------------------------------------------------------------------------------------
+# Measured per body on one launch of force_mixed_tp_kernel<256,6,512> at source split 8 with
+# the closing kick fused (the headline variant and split), captured at N = 262,144 with L2
+# flushed before the launch, and scaled to N by the bodies per launch: the launch's traffic
+# is per-body work (positions and masses read once, accelerations written, velocities read
+# and written); the partial sums of the split are consumed from L2 by the tile's last CTA.
+# None until a capture of the current kernel is recorded here.
+TRAFFIC_BYTES_PER_BODY = None
+TRAFFIC_CAPTURE = None
+# Algorithmic bytes per body of one force launch with the closing kick: x, y, z, m read
+# (32 B), a written (24 B), v read and written (48 B).
+ALGORITHMIC_BYTES_PER_BODY = 104
+
+
 def ncu_traffic(n: int):
-    f = ROOT / "profiles" / "force_mixed_n1048576.md"
-    if not f.exists():
+    if TRAFFIC_BYTES_PER_BODY is None:
         return None
-    m = re.search(r"traffic_bytes_per_launch_at_n1048576\s*=\s*([0-9.eE+]+)", f.read_text())
-    return float(m.group(1)) if m and n == 1 << 20 else None
+    return TRAFFIC_BYTES_PER_BODY * n
 
 
 # ---------------------------------------------------------------------------------------
@@ -194,6 +205,8 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
     ap.add_argument("--leaf-capacity", type=int, default=64, help="leaf capacity of the fmm-evals workload")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the N=1000, N=65536 and ensemble configurations of the default line")
     ap.add_argument("--workload", default="mixed-n1048576",
                     choices=["mixed-n1048576", "ensemble", "fmm-n65536", "fmm-evals", "snapshots-n1048576",
                              "ics-ensemble512", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
@@ -313,7 +326,7 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
     total_s = sum(step_ms) / 1e3
     value = args.steps * pairs / total_s / 1e9
     force_avg_s = force_ms / 1e3 / max(force_launches, 1)
-    launches_per_step = 2 + (1 if jsplit > 1 else 0)
+    launches_per_step = 2  # kick-drift, force (the split's reduction runs inside the force kernel)
     out.update({"value": value, "ms_per_step": sum(step_ms) / args.steps, "steps_per_s": args.steps / total_s,
                 "gpu_launches": args.steps * launches_per_step, "step_ms": [round(t, 3) for t in step_ms],
                 "other_gpu_processes": other_gpu_processes()})
@@ -326,7 +339,9 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
                           "MEASURED_PEAKS.json); the FP32 FMA pipe bounds this kernel, not HBM or tensor cores",
             "ops_per_interaction": FMA_PIPE_OPS_PER_INTERACTION,
             "kernel_ms_per_launch": force_avg_s * 1e3,
-            "traffic": ncu_traffic(n)}
+            "traffic": ncu_traffic(n),
+            "algorithmic_bytes": ALGORITHMIC_BYTES_PER_BODY * n,
+            "traffic_capture": TRAFFIC_CAPTURE}
     if clk.get("sm_mhz"):
         roof["frac_at_observed_clock"] = achieved / (sms * FP32_LANES_PER_SM * clk["sm_mhz"] * 1e6 / 1e12)
     if prec == gx.PRECISION_F64:
@@ -360,7 +375,11 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
 
     # -- FP64 direct path on the same system ---------------------------------------------
     if prec == gx.PRECISION_MIXED:
+        fclk = ClockSampler(torch.cuda.current_device())
+        fclk.start()
+        time.sleep(0.3)
         out["fp64"] = fp64_rate(gx, torch, sess, p, dt, flush)
+        out["fp64"]["clocks"] = fclk.stop()
         out["mixed_over_fp64"] = value / out["fp64"]["value"]
     sess.close()
 
@@ -373,10 +392,14 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
     # -- CPU baseline on the host cores -----------------------------------------------------
     q0 = gx.ParticleSet(p.x, p.y, p.z, p.vx, p.vy, p.vz, p.m)
     out["cpu_baseline"] = cpu_reference_rate(q0, eps, args.cpu_seconds)
+
+    # -- the other configurations, each with its own clock record and parity figures --------
+    if not args.no_configs:
+        out["configs"] = other_configs(gx, torch, args)
     return out
 
 
-def fp64_rate(gx, torch, sess, p, dt, flush, steps: int = 2) -> dict:
+def fp64_rate(gx, torch, sess, p, dt, flush, steps: int = 10) -> dict:
     n = len(p)
     stream = torch.cuda.current_stream()
     sess.set_particles(p)
@@ -464,41 +487,35 @@ def adjoint_ratio(gx, torch, n: int = 16384) -> dict:
 
 
 def run_sharded(gx, torch, dist, p, args, rank, world, eps, dt, prec) -> dict:
-    """Strong scaling: rank r owns the targets of ownership_range(n, r, world); every step
-    kicks and drifts the owned bodies, all-gathers positions (NCCL) and evaluates the owned
-    targets against all sources with the engine kernel."""
-    from gx.sharded import ShardedLeapfrog
+    """Strong scaling: rank r owns the targets of ownership_range(n, r, world).  Each rank's
+    state is resident in an engine session (padded rank-major slots, gx.sharded.ShardedSession);
+    a step is the session's kick-drift of the owned bodies, three in-place NCCL all-gathers
+    of x, y, z, and the session's force on the owned targets with the closing kick."""
+    from gx.sharded import ShardedSession
 
     n = len(p)
     params = gx.PhysicsParams(1.0, eps)
     pairs = n * (n - 1)
-    X = torch.tensor(np.stack([p.x, p.y, p.z]), device="cuda")
-    m = torch.tensor(p.m, device="cuda")
-    ffi = gx._ffi
-
-    def force(Xf, mm, b, e):
-        A = torch.empty(3, e - b, dtype=torch.float64, device="cuda")
-        ffi.call("gx_direct_accel_targets", n, Xf[0].data_ptr(), Xf[1].data_ptr(), Xf[2].data_ptr(), mm.data_ptr(),
-                 b, e, None, 0, params.ffi(), prec, A[0].data_ptr(), A[1].data_ptr(), A[2].data_ptr(),
-                 torch.cuda.current_stream().cuda_stream)
-        return A
-
-    sh = ShardedLeapfrog(n, force)
-    V = torch.tensor(np.stack([p.vx, p.vy, p.vz])[:, sh.begin:sh.end].copy(), device="cuda")
-    A = sh.initial_accelerations(X, m)
-    for _ in range(args.warmup):
-        sh.step(X, V, A, m, dt)
+    sh = ShardedSession(n, params)
+    sh.set_state(p.x, p.y, p.z, p.vx, p.vy, p.vz, p.m)
+    if args.variant is not None:
+        sh.backend.session.set_config(prec, args.variant, args.jsplit or 1)
+    elif not args.no_autotune and world == 1:
+        sh.backend.session.autotune(prec)
+    sh.compute_accelerations(prec)
+    sh.step(args.warmup, dt, prec)
     flush = l2_flusher(torch)
     torch.cuda.synchronize()
     dist.barrier()
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
+    time.sleep(0.3)
     evs = []
     for _ in range(args.steps):
         flush()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        sh.step(X, V, A, m, dt)
+        sh.step(1, dt, prec)
         b.record()
         evs.append((a, b))
     torch.cuda.synchronize()
@@ -507,14 +524,18 @@ def run_sharded(gx, torch, dist, p, args, rank, world, eps, dt, prec) -> dict:
     dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     clk = clocks.stop()
     total_s = float(ms) / 1e3
-    # engine kernels per step: the owned-range force evaluation and, when its source split is
-    # above 1, the ordered reduction (kick/drift of the owned range are torch element-wise ops)
+    v, js = sh.backend.session.get_config(prec)
+    sh.backend.close()
+    # engine kernels per step: the owned range's kick-drift and its force (split reduction fused)
     return {"metric": METRIC, "value": args.steps * pairs / total_s / 1e9, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(ms) / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec == 1 else "f64",
             "data": "synthetic", "gpu_launches": args.steps * 2, "clocks": clk,
             "config": {"workload": f"direct-mixed-n{n}", "n": n, "parallelism": f"targets{world}",
-                       "exchange": "NCCL all-gather of FP64 positions (24 B/body/step)", "softening": eps, "dt": dt,
+                       "kernel": gx.describe_variant(prec, v), "jsplit": js,
+                       "exchange": "three in-place NCCL all-gathers of FP64 positions (24 B/body/step) into the "
+                                   "session's padded rank-major arrays",
+                       "softening": eps, "dt": dt,
                        "l2": "flushed (256 MiB device write) before every timed step, outside the timed interval"}}
 
 
@@ -594,7 +615,17 @@ def wl_p2p(gx, torch, args) -> dict:
     out = {"metric": "Ginteractions/s (FMM P2P leaves)", "unit": UNIT, "n": n, "leaves": lists.n_leaves,
            "near_pairs_of_leaves": int(len(lists.near_leaves)), "interactions": int(pairs),
            "host_leaf_list_build_s": build_s, "config": {"workload": "p2p-n65536", "leaf_capacity": 64, "theta": 0.6}}
+    import oracle
+    L = dict(leaf_offsets=lists.leaf_offsets, leaf_particles=lists.leaf_particles,
+             near_offsets=lists.near_offsets, near_leaves=lists.near_leaves)
+    want = oracle.p2p_near(p.x, p.y, p.z, p.m, 1.0, 0.02, L)  # the reference's near loop, restated in C
+    wn = np.maximum(np.linalg.norm(want, axis=1), 1e-300)
     for name, prec in (("f64", gx.PRECISION_F64), ("mixed", gx.PRECISION_MIXED), ("f64_exact", gx.PRECISION_F64_EXACT)):
+        for a_ in acc:
+            a_.zero_()
+        gx.p2p_leaves(X["x"], X["y"], X["z"], X["m"], dl, params, *acc, prec)
+        got = torch.stack(acc, 1).cpu().numpy()
+        err = np.linalg.norm(got - want, axis=1) / wn
         for _ in range(3):
             gx.p2p_leaves(X["x"], X["y"], X["z"], X["m"], dl, params, *acc, prec)
         a, e = _events(torch)
@@ -605,22 +636,50 @@ def wl_p2p(gx, torch, args) -> dict:
         e.record()
         e.synchronize()
         ms = a.elapsed_time(e) / reps
-        out[name] = {"ms": ms, "value": pairs / (ms / 1e3) / 1e9}
+        out[name] = {"ms": ms, "value": pairs / (ms / 1e3) / 1e9,
+                     "rel_err_vs_oracle_near_field": {"median": float(np.median(err)), "max": float(err.max()),
+                                                      "bit_identical": bool(np.array_equal(got, want))}}
     out["value"] = out["f64"]["value"]
     return out
 
 
-def wl_direct(gx, torch, args, n, eps, dt, steps) -> dict:
+def wl_direct(gx, torch, args, n, eps, dt, steps, ref_targets: int = 0) -> dict:
+    """Resident direct-sum sessions (FP64, mixed, exact form) on the two-disk system: `steps`
+    KDK steps in CUDA graphs.  With ref_targets > 0, the accelerations of the initial
+    positions are checked against the reference's compute_direct_accelerations_for_targets
+    (oracle/_ref, or its C restatement) on ref_targets targets of each disk."""
+    import oracle
     p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps)
     params = gx.PhysicsParams(1.0, eps)
     out = {"metric": f"Ginteractions/s (direct, N={n})", "unit": UNIT, "n": n, "steps": steps,
            "config": {"workload": f"direct-n{n}", "softening": eps, "dt": dt}}
+    ref = None
+    if ref_targets:
+        ranges = [(0, ref_targets), (n // 2, n // 2 + ref_targets)]
+        threads = oracle.default_threads()
+        if oracle.ref_available():
+            ref = np.concatenate([oracle.ref_direct_targets(p.x, p.y, p.z, p.m, 1.0, eps, b, e, threads=threads)
+                                  for b, e in ranges])
+            kind = "reference (compute_direct_accelerations_for_targets, oracle/_ref)"
+        else:
+            idx = np.concatenate([np.arange(b, e) for b, e in ranges])
+            ref = oracle.direct_indexed(p.x, p.y, p.z, p.m, 1.0, eps, idx, threads=threads)
+            kind = "oracle restatement of compute_direct_accelerations_for_targets"
+        sel = np.concatenate([np.arange(b, e) for b, e in ranges])
+        out["parity"] = {"vs": kind, "targets": int(len(sel)), "at": "initial positions"}
     for name, prec in (("f64", gx.PRECISION_F64), ("mixed", gx.PRECISION_MIXED), ("f64_exact", gx.PRECISION_F64_EXACT)):
         s = gx.Session(n, params)
         s.set_particles(p)
         if name != "f64_exact":
             s.autotune(prec)
         s.compute_accelerations(prec)
+        res = {}
+        if ref is not None:
+            st0 = s.get_state()
+            a0 = np.stack([st0["ax"], st0["ay"], st0["az"]], 1)[sel]
+            e = np.linalg.norm(a0 - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-300)
+            res["rel_err"] = {"median": float(np.median(e)), "max": float(e.max()),
+                              "bit_identical": bool(np.array_equal(a0, ref))}
         e0 = s.diagnostics().total_energy
         s.step(3, dt, prec)
         s.synchronize()
@@ -633,12 +692,100 @@ def wl_direct(gx, torch, args, n, eps, dt, steps) -> dict:
         e.synchronize()
         ms = a.elapsed_time(e)
         e1 = s.diagnostics().total_energy
-        out[name] = {"ms_per_step": ms / steps, "value": steps * n * (n - 1) / (ms / 1e3) / 1e9,
-                     "steps_per_s": steps / (ms / 1e3), "energy_drift": abs(e1 - e0) / abs(e0),
-                     "kernel": gx.describe_variant(prec, s.get_config(prec)[0])}
+        res.update({"ms_per_step": ms / steps, "value": steps * n * (n - 1) / (ms / 1e3) / 1e9,
+                    "steps_per_s": steps / (ms / 1e3), "energy_drift": abs(e1 - e0) / abs(e0),
+                    "kernel": gx.describe_variant(prec, s.get_config(prec)[0])})
+        out[name] = res
         s.close()
     out["value"] = out["mixed"]["value"]
     return out
+
+
+def cfg0_n1000(gx, torch, args) -> dict:
+    """The reference CLI's own workload size: N = 1000 (two disks of 500), softening 0.05,
+    dt 0.005, 20 KDK steps in FP64.  The exact form's 20-step trajectory is compared with the
+    oracle's (the reference's per-target sum and leapfrog restated in C, pinned bit for bit
+    to the reference); the rate repeats the 20-step run for ~0.5 s.  Both step loops are
+    timed: one cooperative launch per call (the default for small systems) and CUDA graphs of
+    separate kick-drift and force launches."""
+    import oracle
+    n, eps, dt, steps = 1000, 0.05, 0.005, 20
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, eps)
+    params = gx.PhysicsParams(1.0, eps)
+    ref0 = oracle.direct_targets(p.x, p.y, p.z, p.m, 1.0, eps)
+    st0 = dict(x=p.x, y=p.y, z=p.z, vx=p.vx, vy=p.vy, vz=p.vz, ax=ref0[:, 0], ay=ref0[:, 1], az=ref0[:, 2])
+    want = oracle.leapfrog(st0, p.m, 1.0, eps, dt, steps, solver=1)
+    out = {"n": n, "steps": steps, "softening": eps, "dt": dt, "unit": "steps/s",
+           "parity_vs": "oracle leapfrog over compute_direct_accelerations_for_targets (20 steps)"}
+    forms = (("f64", gx.PRECISION_F64, True), ("f64_exact", gx.PRECISION_F64_EXACT, True),
+             ("f64_graphs", gx.PRECISION_F64, False), ("f64_exact_graphs", gx.PRECISION_F64_EXACT, False))
+    for name, prec, persistent in forms:
+        with gx.Session(n, params) as s:
+            s.set_persistent(persistent)
+            s.set_particles(p)
+            s.compute_accelerations(prec)
+            s.step(steps, dt, prec)
+            got = s.get_state()
+            dx = max(float(np.max(np.abs(got[k] - want[k]))) for k in ("x", "y", "z"))
+            same = all(np.array_equal(got[k], want[k]) for k in ("x", "y", "z", "vx", "vy", "vz"))
+            st = torch.cuda.Stream()
+            s.set_stream(st)
+            s.step(steps, dt, prec)
+            s.synchronize()
+            a, e = _events(torch)
+            reps = 0
+            t0 = time.perf_counter()
+            a.record(st)
+            while True:
+                s.step(steps, dt, prec)
+                reps += 1
+                if reps % 25 == 0:
+                    s.synchronize()
+                    if time.perf_counter() - t0 > 0.5:
+                        break
+            e.record(st)
+            e.synchronize()
+            ms = a.elapsed_time(e)
+        total = reps * steps
+        out[name] = {"steps_per_s": total / (ms / 1e3), "us_per_step": ms * 1e3 / total,
+                     "value_gint_s": total * n * (n - 1) / (ms / 1e3) / 1e9, "timed_steps": total,
+                     "max_abs_dx_20_steps": dx, "trajectory_bit_identical": same,
+                     "launch": "one cooperative launch per 20 steps (small.cu)" if persistent else
+                               "CUDA graph of 20 steps (kick-drift + force launches per step)"}
+    out["value"] = out["f64"]["steps_per_s"]
+    return out
+
+
+def _clocked(torch, fn):
+    c = ClockSampler(torch.cuda.current_device())
+    c.start()
+    time.sleep(0.25)
+    try:
+        r = fn()
+    finally:
+        clk = c.stop()
+    r["clocks"] = clk
+    return r
+
+
+def other_configs(gx, torch, args) -> dict:
+    """The reference's other configurations, measured in the default run so that their
+    figures come with the headline's: N = 1000 (the reference CLI workload), N = 65,536
+    (direct FP64 and mixed, the FMM's P2P leaves at capacity 64, the whole FMM on the
+    device, each with its error against the reference) and the 512-encounter ensemble."""
+    import copy
+    sub = copy.copy(args)
+    sub.steps, sub.warmup, sub.cpu_seconds = 10, 3, 3.0
+    res = {"cfg0_n1000": _clocked(torch, lambda: cfg0_n1000(gx, torch, sub))}
+    c1 = {}
+    c1["direct"] = _clocked(torch, lambda: wl_direct(gx, torch, sub, 65536, 0.02, 0.002, 100, ref_targets=512))
+    c1["p2p_leaf64"] = _clocked(torch, lambda: wl_p2p(gx, torch, sub))
+    c1["fmm_leaf64"] = _clocked(torch, lambda: wl_fmm(gx, torch, sub, e2e=False))
+    res["cfg1_n65536"] = c1
+    ens = copy.copy(sub)
+    ens.steps = 200
+    res["cfg3_ensemble512"] = _clocked(torch, lambda: wl_ensemble(gx, torch, ens))
+    return res
 
 
 def wl_fit(gx, torch, args) -> dict:
@@ -703,7 +850,7 @@ FP64_OPS_PER_M2P_PAIR = 171
 FP64_OPS_PER_P2P_PAIR = 17
 
 
-def wl_fmm(gx, torch, args) -> dict:
+def wl_fmm(gx, torch, args, e2e: bool = True) -> dict:
     """The reference FMM solver on the N = 65,536 two-disk workload (leaf_capacity 64,
     theta 0.6, expansion order 4, softening 0.02, dt 0.002): one KDK step = kick-drift,
     a full FMM force evaluation (octree, lists, moments, far and near field, all on the
@@ -772,20 +919,22 @@ def wl_fmm(gx, torch, args) -> dict:
             "far_field": {"pairs": stats.far_pairs, "ops_per_pair": FP64_OPS_PER_M2P_PAIR,
                           "phase_ms": ph["far_field"], "achieved": m2p_ach, "frac": m2p_ach / fp64_peak},
             "traffic": None,
-            "traffic_note": "node records, bodies and lists stay in L2: ncu DRAM reads 7.7 MB (far) and 5.1 MB "
-                            "(near) per evaluation at this size (profiles/fmm_m2p_p2p_n65536_full.md)"}
+            "traffic_note": "node records, bodies and lists stay in L2: ncu DRAM reads 7.7 MB (far field) and "
+                            "5.1 MB (near field) per evaluation at this size"}
 
     # e2e: the public API on host arrays (H2D of x, y, z, m and D2H of a inside the call)
-    q = p.copy()
-    gx.fmm.compute_fmm_accelerations(q, params, opt)
-    t0 = time.perf_counter()
-    e2e_steps = max(3, steps // 2)
-    for _ in range(e2e_steps):
-        q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
-        q.x += q.vx * dt; q.y += q.vy * dt; q.z += q.vz * dt
+    e2e_rate_ = None
+    if e2e:
+        q = p.copy()
         gx.fmm.compute_fmm_accelerations(q, params, opt)
-        q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
-    e2e = e2e_steps / (time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        e2e_steps = max(3, steps // 2)
+        for _ in range(e2e_steps):
+            q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
+            q.x += q.vx * dt; q.y += q.vy * dt; q.z += q.vz * dt
+            gx.fmm.compute_fmm_accelerations(q, params, opt)
+            q.vx += q.ax * (0.5 * dt); q.vy += q.ay * (0.5 * dt); q.vz += q.az * (0.5 * dt)
+        e2e_rate_ = e2e_steps / (time.perf_counter() - t0)
 
     # the mixed form (both fields in FP32 arithmetic on FP64 offsets) on the same system
     Dm = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
@@ -819,7 +968,8 @@ def wl_fmm(gx, torch, args) -> dict:
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "phases_ms_per_eval": ph, "stats": stats.__dict__,
            "gpu_launches": steps * (19 + stats.tree_levels + 2),
-           "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 3 * n * 8},
+           "e2e": None if e2e_rate_ is None else
+           {"value": e2e_rate_, "unit": "steps/s", "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 3 * n * 8},
            "roofline": roof, "clocks": clk, "mixed": mixed,
            "config": {"workload": "fmm-n65536", "n": n, "leaf_capacity": cap, "theta": theta, "expansion_order": 4,
                       "softening": eps, "dt": dt, "near_field_precision": "f64",

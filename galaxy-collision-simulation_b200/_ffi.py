@@ -90,6 +90,15 @@ class GalaxyStruct(ctypes.Structure):
                 ("reserved", ctypes.c_uint32), ("thickness", c_double), ("inclination", c_double)]
 
 
+class RunMetadataStruct(ctypes.Structure):
+    """gx_run_metadata: the SimulationConfig fields SnapshotWriter::write_metadata prints."""
+
+    _fields_ = [("name", c_char_p), ("solver", c_char_p), ("particle_count", c_int64), ("steps", c_int32),
+                ("snapshot_every", c_int32), ("dim", c_int32), ("fmm_expansion_order", c_int32), ("dt", c_double),
+                ("gravitational_constant", c_double), ("softening", c_double), ("tree_theta", c_double),
+                ("tree_leaf_capacity", c_int64)]
+
+
 P = c_void_p  # any array: numpy .ctypes.data, torch .data_ptr(), or None
 PP = POINTER(c_void_p)
 I64 = c_int64
@@ -119,6 +128,10 @@ _SIGNATURES = {
     "gx_session_step": [P, I64, D, c_int],
     "gx_session_diagnostics": [P, POINTER(DiagnosticsStruct)],
     "gx_session_synchronize": [P],
+    "gx_session_set_persistent": [P, c_int],
+    "gx_session_set_targets": [P, I64, I64],
+    "gx_session_kick_drift": [P, D, D],
+    "gx_session_force_kick": [P, D, c_int],
     "gx_session_synchronize_timeout": [P, D],
     "gx_session_enable_timing": [P, c_int],
     "gx_session_force_timing": [P, POINTER(D), POINTER(I64)],
@@ -133,6 +146,7 @@ _SIGNATURES = {
     "gx_snapshot_writer_destroy": [P],
     "gx_snapshot_write": [P, c_int, D, P, P, P, P, P, P, P, P, P, P, S],
     "gx_snapshot_write_diagnostics": [P, c_int, D, POINTER(DiagnosticsStruct)],
+    "gx_snapshot_write_metadata": [P, POINTER(RunMetadataStruct)],
     "gx_session_snapshot": [P, P, c_int, D],
     "gx_fmm_accel": [I64, P, P, P, P, Physics, FmmOptionsStruct, c_int, I64, I64, P, P, P, POINTER(FmmStatsStruct),
                      S],
@@ -165,6 +179,8 @@ _SIGNATURES = {
     "gx_variant_count": [c_int, POINTER(c_int)],
     "gx_variant_describe": [c_int, c_int, c_char_p, c_int],
     "gx_debug_fail_allocations": [c_int],
+    "gx_debug_stall_barrier": [I64],
+    "gx_debug_p2p_targets_per_thread": [c_int],
 }
 _RESTYPES = {"gx_last_error": c_char_p, "gx_galaxies_body_count": c_int64}
 

@@ -12,6 +12,7 @@
 #include "force.cuh"
 #include "integrate.cuh"
 #include "p2p.cuh"
+#include "small.cuh"
 #include "vjp.cuh"
 
 #include <algorithm>
@@ -41,6 +42,7 @@ using namespace gx;
 namespace {
 thread_local std::string g_err;
 std::atomic<int> g_fail_allocs{0};
+std::atomic<int64_t> g_stall_step{-1};  // gx_debug_stall_barrier
 
 int fail(int code, const char* fmt, ...) {
     char buf[1024];
@@ -88,12 +90,21 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
     return cudaMalloc(p, bytes ? bytes : 16);
 }
 
+cudaMemPool_t library_pool(int dev);
+
+// Stream-ordered scratch from the library's own memory pool (library_pool), never from the
+// device's default pool that the host application may be using.
 cudaError_t dev_alloc_async(void** p, size_t bytes, cudaStream_t st) {
     int left = g_fail_allocs.load();
     while (left > 0) {
         if (g_fail_allocs.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
     }
-    return cudaMallocAsync(p, bytes ? bytes : 16, st);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = library_pool(dev);
+    if (!pool) return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
 }
 
 // ======================================================================================
@@ -142,21 +153,31 @@ int sm_count(int dev) {
     return v;
 }
 
-// Stream-ordered scratch comes from the device's default pool; keep freed blocks in the pool
-// (release threshold = unlimited) so repeated calls on host arrays do not remap memory.
-void keep_pool_memory(int dev) {
+// Stream-ordered scratch comes from a memory pool the library creates for each device (its
+// release threshold is unlimited, so repeated calls on host arrays reuse the same memory
+// instead of remapping it).  The device's default pool, which the host application or torch
+// may use, is left as it is.  The pool lives until the process exits.
+cudaMemPool_t library_pool(int dev) {
     static std::mutex mu;
-    static std::map<int, bool> done;
+    static std::map<int, cudaMemPool_t> pools;
     std::lock_guard<std::mutex> lock(mu);
-    if (done[dev]) return;
-    done[dev] = true;
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t thr = UINT64_MAX;
-        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) != cudaSuccess) cudaGetLastError();
-    } else {
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
         cudaGetLastError();
+        return nullptr;
     }
+    uint64_t thr = UINT64_MAX;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) != cudaSuccess) cudaGetLastError();
+    pools[dev] = pool;
+    return pool;
 }
 
 struct DeviceGuard {
@@ -224,8 +245,6 @@ struct AsyncBuf {
     }
     int alloc(size_t bytes, cudaStream_t s) {
         st = s;
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) keep_pool_memory(dev);
         cudaError_t e = dev_alloc_async(&p, bytes, s);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -373,6 +392,7 @@ ForceArgs make_args(const ForceJob& j, const gx_physics& ph, const ForceVariant&
     a.ay = j.ay;
     a.az = j.az;
     a.part = part;
+    a.tile_count = nullptr;
     a.vx = j.vx;
     a.vy = j.vy;
     a.vz = j.vz;
@@ -383,14 +403,24 @@ ForceArgs make_args(const ForceJob& j, const gx_physics& ph, const ForceVariant&
     return a;
 }
 
+// Scratch of a split force evaluation: the tile tickets of the fused reduction first (zeroed
+// when the scratch is allocated and left zeroed by every launch), then the
+// nsplit * 3 * n_tgt partial sums.  The ticket area depends only on max(n_src, n_tgt) and
+// is sized for the smallest tile of any variant (64 targets), so a session's later
+// launches -- another variant, another split, fewer targets -- find the same zeroed
+// tickets and never write partial sums over them.
+size_t ticket_bytes(int64_t n) { return (((size_t)(n / 64 + 1) * sizeof(unsigned)) + 255) / 256 * 256; }
+
 size_t part_bytes(const ForceVariant& v, int64_t n_src, int64_t n_tgt, int nsplit) {
     int64_t chunk;
     int ns;
     split_layout(n_src, v.jt, nsplit, &chunk, &ns);
-    return ns > 1 ? (size_t)ns * 3 * (size_t)n_tgt * sizeof(double) : 0;
+    return ns > 1 ? ticket_bytes(std::max(n_src, n_tgt)) + (size_t)ns * 3 * (size_t)n_tgt * sizeof(double) : 0;
 }
 
-// Runs one force evaluation with scratch from `part` (or a stream-ordered allocation).
+// Runs one force evaluation with scratch from `part` (whose tickets are zero), or from a
+// stream-ordered allocation whose tickets are cleared here.  Split evaluations reduce in
+// the kernel (fused, tile tickets).
 int run_force(const ForceJob& j, const gx_physics& ph, int precision, Choice ch, int dev,
               cudaStream_t st, double* part, size_t part_cap) {
     int cnt;
@@ -399,12 +429,20 @@ int run_force(const ForceJob& j, const gx_physics& ph, int precision, Choice ch,
     if (ch.variant < 0) ch = heuristic_choice(dev, precision, eps0, j.n_tgt, j.n_src);
     const ForceVariant& v = all[ch.variant];
     const size_t need = part_bytes(v, j.n_src, j.n_tgt, ch.nsplit);
+    const size_t tb = ticket_bytes(std::max(j.n_src, j.n_tgt));
     AsyncBuf tmp;
     if (need > part_cap) {
         GX_TRY(tmp.alloc(need, st));
         part = tmp.d();
+        GX_CUDA(cudaMemsetAsync(part, 0, tb, st));
     }
-    const ForceArgs a = make_args(j, ph, v, ch.nsplit, part);
+    ForceArgs a = make_args(j, ph, v, ch.nsplit, part);
+    if (a.nsplit > 1) {
+        if (force_tiles(v, j.n_tgt) * (int64_t)sizeof(unsigned) > (int64_t)tb)
+            return fail(GX_ERR_UNSUPPORTED, "force variant tile smaller than 64 targets");
+        a.tile_count = (unsigned*)part;
+        a.part = (double*)((char*)part + tb);
+    }
     (void)cudaGetLastError();  // drop a stale non-sticky error of unrelated earlier work; sticky ones resurface below
     GX_CUDA(force_launch(v, a, st));
     return GX_OK;
@@ -473,6 +511,18 @@ extern "C" int gx_device_available(int* available) {
 
 extern "C" int gx_debug_fail_allocations(int count) {
     g_fail_allocs.store(count < 0 ? 0 : count);
+    return GX_OK;
+}
+
+extern "C" int gx_debug_p2p_targets_per_thread(int tpt) {
+    if (tpt != 0 && tpt != 2 && tpt != 4)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_debug_p2p_targets_per_thread: 0, 2 or 4");
+    p2p_set_targets_per_thread(tpt);
+    return GX_OK;
+}
+
+extern "C" int gx_debug_stall_barrier(int64_t step) {
+    g_stall_step.store(step < 0 ? -1 : step);
     return GX_OK;
 }
 
@@ -736,6 +786,11 @@ struct gx_session {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     double timed_ms = 0.0;
     int64_t timed_launches = 0;
+    int64_t t_begin = 0;        // owned targets [t_begin, t_begin + t_count): kicked, drifted and
+    int64_t t_count = 0;        // given forces by the session (all bodies unless set_targets)
+    bool persistent = true;     // small systems step in one cooperative launch (small.cu)
+    void* small = nullptr;      // its scratch: barrier words, status, two position buffers
+    bool small_pending = false; // a launch ran since the status word was last read
 
     void clear_graphs() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -747,7 +802,7 @@ namespace {
 
 int session_choice(gx_session* s, int precision, Choice* out) {
     if (s->cfg[precision].variant < 0) {
-        s->cfg[precision] = heuristic_choice(s->device, precision, eps0_of(precision, s->phys), s->n, s->n);
+        s->cfg[precision] = heuristic_choice(s->device, precision, eps0_of(precision, s->phys), s->t_count, s->n);
     }
     *out = s->cfg[precision];
     return GX_OK;
@@ -769,6 +824,7 @@ int session_ensure_part(gx_session* s, const Choice& ch) {
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc (session j-split scratch)");
     s->part = (double*)p;
     s->part_cap = need;
+    GX_CUDA(cudaMemsetAsync(p, 0, ticket_bytes(s->n), s->stream));  // tile tickets of the fused reduction
     return GX_OK;
 }
 
@@ -792,7 +848,8 @@ int session_force(gx_session* s, int precision, double kick_dt) {
     Choice ch;
     GX_TRY(session_choice(s, precision, &ch));
     GX_TRY(session_ensure_part(s, ch));
-    ForceJob j{s->x, s->y, s->z, s->m, s->n, nullptr, 0, s->n, s->ax, s->ay, s->az,
+    ForceJob j{s->x, s->y, s->z, s->m, s->n, nullptr, s->t_begin, s->t_count, s->ax + s->t_begin,
+               s->ay + s->t_begin, s->az + s->t_begin,
                kick_dt != 0.0 ? s->vx : nullptr, kick_dt != 0.0 ? s->vy : nullptr,
                kick_dt != 0.0 ? s->vz : nullptr, kick_dt};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -809,11 +866,18 @@ int session_force(gx_session* s, int precision, double kick_dt) {
     return r;
 }
 
+// Opening half of a step for the owned bodies: kick(kick_dt) then drift(drift_dt).
+int session_kick_drift(gx_session* s, double kick_dt, double drift_dt) {
+    const int64_t b = s->t_begin;
+    GX_CUDA(launch_kick_drift(s->t_count, s->x + b, s->y + b, s->z + b, s->vx + b, s->vy + b, s->vz + b, s->ax + b,
+                              s->ay + b, s->az + b, kick_dt, drift_dt, s->stream));
+    return GX_OK;
+}
+
 int session_enqueue_steps(gx_session* s, int64_t k, double dt, int precision) {
     const double half = 0.5 * dt;
     for (int64_t i = 0; i < k; ++i) {
-        GX_CUDA(launch_kick_drift(s->n, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, half, dt,
-                                  s->stream));
+        GX_TRY(session_kick_drift(s, half, dt));
         GX_TRY(session_force(s, precision, half));
     }
     return GX_OK;
@@ -855,6 +919,55 @@ int check_session(gx_session* s, const char* fn) {
     return GX_OK;
 }
 
+// Steps that run as one cooperative launch: small systems in FP64 or the exact form, unless
+// the caller turned it off or is timing force launches one by one.
+bool session_small_eligible(const gx_session* s, int precision) {
+    return s->persistent && !s->timing && s->n <= kSmallMaxBodies && s->t_begin == 0 && s->t_count == s->n &&
+           (precision == kF64 || precision == kF64Exact);
+}
+
+int session_small_steps(gx_session* s, int64_t k, double dt, int precision) {
+    if (!s->small) {
+        void* p = nullptr;
+        cudaError_t e = dev_alloc(&p, small_scratch_bytes((int)s->n));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc (session small-system scratch)");
+        s->small = p;
+    }
+    SmallArgs a;
+    a.n = (int)s->n;
+    a.x = s->x; a.y = s->y; a.z = s->z;
+    a.vx = s->vx; a.vy = s->vy; a.vz = s->vz;
+    a.ax = s->ax; a.ay = s->ay; a.az = s->az;
+    a.m = s->m;
+    a.G = s->phys.G;
+    a.eps2 = s->phys.softening * s->phys.softening;
+    a.dt = dt;
+    a.steps = k;
+    a.timeout_ns = 4000000000ull;
+    a.stall_step = g_stall_step.exchange(-1);
+    if (a.stall_step >= 0) a.timeout_ns = 200000000ull;
+    small_bind_scratch(a, s->small);
+    (void)cudaGetLastError();
+    const cudaError_t e = small_steps_launch(a, precision, eps0_of(precision, s->phys), s->device, s->stream);
+    if (e == cudaErrorNotSupported) return GX_ERR_UNSUPPORTED;
+    if (e != cudaSuccess) return fail_cuda(e, "small-system step launch");
+    s->small_pending = true;
+    return GX_OK;
+}
+
+// After the stream has been synchronized: GX_ERR_TIMEOUT when a cooperative step launch gave
+// up on a barrier since the last check.
+int session_small_status(gx_session* s) {
+    if (!s->small_pending) return GX_OK;
+    s->small_pending = false;
+    int st = 0;
+    GX_CUDA(cudaMemcpy(&st, (char*)s->small + 2 * sizeof(unsigned), sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0)
+        return fail(GX_ERR_TIMEOUT, "session step: a grid barrier of the single-launch step loop timed out; "
+                                    "the state is that of the last completed gx_session_step call");
+    return GX_OK;
+}
+
 }  // namespace
 
 extern "C" int gx_session_create(int64_t n, gx_physics phys, int device, gx_session** out) {
@@ -872,6 +985,7 @@ extern "C" int gx_session_create(int64_t n, gx_physics phys, int device, gx_sess
     gx_session* s = new gx_session();
     s->device = device;
     s->n = n;
+    s->t_count = n;
     s->phys = phys;
     void* p = nullptr;
     cudaError_t e = dev_alloc(&p, (size_t)n * 10 * sizeof(double));
@@ -912,6 +1026,7 @@ extern "C" int gx_session_destroy(gx_session* s) {
         cudaEventDestroy(ev.second);
     }
     s->clear_graphs();
+    if (s->small) cudaFree(s->small);
     if (s->part) cudaFree(s->part);
     if (s->diag) cudaFree(s->diag);
     if (s->host_diag) cudaFreeHost(s->host_diag);
@@ -980,7 +1095,7 @@ extern "C" int gx_session_get_state(gx_session* s, double* x, double* y, double*
     for (int k = 0; k < 9; ++k)
         if (dst[k]) GX_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, kind, s->stream));
     GX_CUDA(cudaStreamSynchronize(s->stream));
-    return GX_OK;
+    return session_small_status(s);
     GX_GUARD_END
 }
 
@@ -1018,6 +1133,10 @@ extern "C" int gx_session_step(gx_session* s, int64_t n_steps, double dt, int pr
     if (n_steps < 0 || !std::isfinite(dt)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: need n_steps >= 0, finite dt", fn);
     if (n_steps == 0) return GX_OK;
     DeviceGuard g(s->device);
+    if (session_small_eligible(s, precision)) {
+        const int r = session_small_steps(s, n_steps, dt, precision);
+        if (r != GX_ERR_UNSUPPORTED) return r;
+    }
     if (s->timing || s->stream == nullptr) return session_enqueue_steps(s, n_steps, dt, precision);
     const int64_t chunk = std::min<int64_t>(n_steps, 32);
     cudaGraphExec_t ge;
@@ -1042,7 +1161,7 @@ extern "C" int gx_session_diagnostics(gx_session* s, gx_diagnostics* out) {
     GX_CUDA(cudaMemcpyAsync(s->host_diag, s->diag, 13 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     GX_CUDA(cudaStreamSynchronize(s->stream));
     fill_diag(s->host_diag, out);
-    return GX_OK;
+    return session_small_status(s);
     GX_GUARD_END
 }
 
@@ -1050,7 +1169,48 @@ extern "C" int gx_session_synchronize(gx_session* s) {
     GX_TRY(check_session(s, "gx_session_synchronize"));
     DeviceGuard g(s->device);
     GX_CUDA(cudaStreamSynchronize(s->stream));
+    return session_small_status(s);
+}
+
+extern "C" int gx_session_set_persistent(gx_session* s, int enable) {
+    GX_TRY(check_session(s, "gx_session_set_persistent"));
+    s->persistent = enable != 0;
     return GX_OK;
+}
+
+extern "C" int gx_session_set_targets(gx_session* s, int64_t begin, int64_t count) {
+    GX_TRY(check_session(s, "gx_session_set_targets"));
+    if (begin < 0 || count < 0 || begin + count > s->n)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_set_targets: need 0 <= begin, 0 <= count, begin + count <= n");
+    DeviceGuard g(s->device);
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    s->t_begin = begin;
+    s->t_count = count;
+    for (auto& c : s->cfg) c = Choice();
+    s->clear_graphs();
+    return GX_OK;
+}
+
+extern "C" int gx_session_kick_drift(gx_session* s, double kick_dt, double drift_dt) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_session(s, "gx_session_kick_drift"));
+    if (!std::isfinite(kick_dt) || !std::isfinite(drift_dt))
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_kick_drift: time steps must be finite");
+    DeviceGuard g(s->device);
+    if (s->t_count == 0) return GX_OK;
+    return session_kick_drift(s, kick_dt, drift_dt);
+    GX_GUARD_END
+}
+
+extern "C" int gx_session_force_kick(gx_session* s, double kick_dt, int precision) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_session(s, "gx_session_force_kick"));
+    if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_force_kick: precision");
+    if (!std::isfinite(kick_dt)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_force_kick: kick_dt must be finite");
+    DeviceGuard g(s->device);
+    if (s->t_count == 0) return GX_OK;
+    return session_force(s, precision, kick_dt);
+    GX_GUARD_END
 }
 
 extern "C" int gx_session_synchronize_timeout(gx_session* s, double timeout_ms) {
@@ -1076,7 +1236,7 @@ extern "C" int gx_session_synchronize_timeout(gx_session* s, double timeout_ms) 
     }
     cudaEventDestroy(ev);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventQuery");
-    return GX_OK;
+    return session_small_status(s);
 }
 
 extern "C" int gx_session_enable_timing(gx_session* s, int enable) {
@@ -1140,7 +1300,8 @@ namespace {
 // session's state (results go to the session's acceleration array).
 int time_choice(gx_session* s, int precision, Choice ch, int64_t n_tgt, int reps, double* ms_out) {
     GX_TRY(session_ensure_part(s, ch));
-    ForceJob j{s->x, s->y, s->z, s->m, s->n, nullptr, 0, n_tgt, s->ax, s->ay, s->az, nullptr, nullptr, nullptr, 0.0};
+    ForceJob j{s->x, s->y, s->z, s->m, s->n, nullptr, s->t_begin, n_tgt, s->ax + s->t_begin, s->ay + s->t_begin,
+               s->az + s->t_begin, nullptr, nullptr, nullptr, 0.0};
     GX_TRY(run_force(j, s->phys, precision, ch, s->device, s->stream, s->part, s->part_cap));  // warm-up
     cudaEvent_t e0, e1;
     GX_CUDA(cudaEventCreate(&e0));
@@ -1182,13 +1343,13 @@ extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms
     Choice best;
     double bms = 1e300;
     int status = GX_OK;
-    const bool large = (double)s->n * (double)s->n > 4.0e10;
+    const bool large = (double)s->t_count * (double)s->n > 4.0e10;
     // Phase 1: every variant at the split the wave model prefers for it (small systems also try
     // a few fixed splits).  Phase 2 (large systems): other splits for the three best variants.
     std::vector<std::pair<double, Choice>> ranked;
     for (int k = 0; k < c && status == GX_OK; ++k) {
         const ForceVariant& v = all[ids[k]];
-        std::vector<int> splits = {best_split(v, s->n, s->n, sms)};
+        std::vector<int> splits = {best_split(v, s->t_count, s->n, sms)};
         if (!large) {
             for (int ns : {1, 2, 4, 8})
                 if (std::find(splits.begin(), splits.end(), ns) == splits.end() && (int64_t)ns * v.jt <= s->n)
@@ -1197,7 +1358,7 @@ extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms
         for (int ns : splits) {
             const Choice ch{ids[k], ns};
             double ms;
-            status = time_choice(s, precision, ch, s->n, large ? 1 : 3, &ms);
+            status = time_choice(s, precision, ch, s->t_count, large ? 1 : 3, &ms);
             if (status != GX_OK) break;
             ranked.emplace_back(ms, ch);
         }
@@ -1212,7 +1373,7 @@ extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms
                 if (ns == ranked[r].second.nsplit || (int64_t)ns * v.jt > s->n) continue;
                 const Choice ch{ranked[r].second.variant, ns};
                 double ms;
-                status = time_choice(s, precision, ch, s->n, 1, &ms);
+                status = time_choice(s, precision, ch, s->t_count, 1, &ms);
                 if (status != GX_OK) break;
                 extra.emplace_back(ms, ch);
             }
@@ -1232,7 +1393,7 @@ extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms
     s->cfg[precision] = best;
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tuned[std::make_tuple(s->device, precision, (int)eps0, s->n)] = best;
+        if (s->t_count == s->n) g_tuned[std::make_tuple(s->device, precision, (int)eps0, s->n)] = best;
     }
     s->clear_graphs();
     if (best_ms) *best_ms = bms;

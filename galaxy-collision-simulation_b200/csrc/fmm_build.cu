@@ -36,7 +36,11 @@ namespace {
 constexpr int kBboxThreads = 256;
 constexpr int kBuildThreads = 1024;
 constexpr int kWalkThreads = 128;  // 4 warps, one leaf each
-constexpr int kWalkStack = 1792;   // shared stack slots per warp
+// Shared stack slots per warp: 4 x 1760 x 4 B = 27.5 KiB per block, plus the 1 KiB the
+// runtime reserves per block, puts exactly 8 blocks (32 warps) in an SM's 228 KiB, the
+// count __launch_bounds__(kWalkThreads, 8) sizes the registers for (walk_kernel asks for
+// the largest shared-memory carveout).
+constexpr int kWalkStack = 1760;
 // near lists up to this many entries are sorted in the warp's stack buffer (a bitonic network
 // pads to a power of two, so the largest power of two that fits kWalkStack / 2 keys)
 constexpr int pow2_floor(int v) { return v < 2 ? v : 2 * pow2_floor(v / 2); }
@@ -667,6 +671,17 @@ size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes) {
     return std::max(scan_bytes(n + 1), scan_bytes(n_nodes + 1));
 }
 
+// Both walk kernels prefer the largest shared-memory carveout (8 blocks of 28.5 KiB).
+static cudaError_t walk_carveout() {
+    static cudaError_t once = [] {
+        cudaError_t e = cudaFuncSetAttribute(walk_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(walk_kernel<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        return e;
+    }();
+    return once;
+}
+
 cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st) {
     cudaError_t e;
     const size_t nb = (size_t)(a.n + 1) * sizeof(int32_t), lb = (size_t)(a.n_nodes + 1) * sizeof(int32_t);
@@ -684,6 +699,7 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.keep, a.newpos, a.n + 1, st)) != cudaSuccess) return e;
     leaf_emit_kernel<<<gn, 256, 0, st>>>(a);
     walk_pack_kernel<<<gn, 256, 0, st>>>(a);
+    if ((e = walk_carveout()) != cudaSuccess) return e;
     walk_kernel<false><<<(a.n_nodes + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int32_t* cnt[4] = {a.far_cnt, a.near_cnt, a.item_cnt, a.slot_cnt};

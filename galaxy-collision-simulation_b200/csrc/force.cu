@@ -1,5 +1,6 @@
-// force.cu -- one-system direct-sum kernels (grid = target tiles x source chunks), the
-// ordered j-split reduction and the table of compiled variants.  The arithmetic lives in
+// force.cu -- one-system direct-sum kernels (one CTA per target tile and source chunk,
+// chunk-minor), the ordered j-split reduction (fused into the last CTA of each tile, or a
+// second kernel) and the table of compiled variants.  The arithmetic lives in
 // force_tile.cuh.
 #include "force_tile.cuh"
 
@@ -8,7 +9,7 @@
 namespace gx {
 namespace {
 
-// Ordered reduction of the j-split partial sums, then G and the epilogue.
+// Ordered reduction of the j-split partial sums, then G and the epilogue (the unfused path).
 __global__ void __launch_bounds__(256) force_reduce_kernel(const ForceArgs a) {
     const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (t >= a.n_tgt) return;
@@ -22,19 +23,56 @@ __global__ void __launch_bounds__(256) force_reduce_kernel(const ForceArgs a) {
     write_result(a, t, target_body(a, t), a.G * s[0], a.G * s[1], a.G * s[2]);
 }
 
+// Fused reduction, run by every CTA after its tile body has written its partial sums: the
+// CTA that takes the tile's last ticket adds the tile's nsplit partials in chunk order --
+// the sums force_reduce_kernel forms -- and writes the results.  Each thread fences its
+// own partial stores before the ticket is taken; the last CTA reads the partials from L2
+// (ld.global.cg), so no stale L1 line can be seen.  No CTA waits for another.
+template <int BLOCK, int IPT>
+__device__ __forceinline__ void finish_tile(const ForceArgs& a, const int64_t tile, const int64_t t0) {
+    if (a.nsplit <= 1 || !a.tile_count) return;
+    __shared__ unsigned s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&a.tile_count[tile], 1u) == (unsigned)a.nsplit - 1u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        const int64_t t = t0 + k * BLOCK + threadIdx.x;
+        if (t >= a.n_tgt) continue;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int c = 0; c < a.nsplit; ++c) {
+            const size_t base = (size_t)c * 3 * (size_t)a.n_tgt + (size_t)t;
+            s0 += __ldcg(a.part + base);
+            s1 += __ldcg(a.part + base + (size_t)a.n_tgt);
+            s2 += __ldcg(a.part + base + 2 * (size_t)a.n_tgt);
+        }
+        write_result(a, t, target_body(a, t), a.G * s0, a.G * s1, a.G * s2);
+    }
+    if (threadIdx.x == 0) a.tile_count[tile] = 0u;
+}
+
 template <int BLOCK, int IPT, int JT, bool PACKED, bool EPS0>
 __global__ void __launch_bounds__(BLOCK) force_mixed_kernel(const ForceArgs a) {
-    mixed_tile<BLOCK, IPT, JT, PACKED, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+    const int64_t tile = blockIdx.x / a.nsplit;
+    mixed_tile<BLOCK, IPT, JT, PACKED, EPS0>(a, tile * (BLOCK * IPT), (int)(blockIdx.x % a.nsplit));
+    finish_tile<BLOCK, IPT>(a, tile, tile * (BLOCK * IPT));
 }
 
 template <int BLOCK, int IPT, int JT, bool EPS0, int MINB, int UNROLL = 4>
 __global__ void __launch_bounds__(BLOCK, MINB) force_mixed_tp_kernel(const ForceArgs a) {
-    mixed_tp_tile<BLOCK, IPT, JT, EPS0, UNROLL>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+    const int64_t tile = blockIdx.x / a.nsplit;
+    mixed_tp_tile<BLOCK, IPT, JT, EPS0, UNROLL>(a, tile * (BLOCK * IPT), (int)(blockIdx.x % a.nsplit));
+    finish_tile<BLOCK, IPT>(a, tile, tile * (BLOCK * IPT));
 }
 
 template <int BLOCK, int IPT, int JT, bool EPS0>
 __global__ void __launch_bounds__(BLOCK) force_f64_kernel(const ForceArgs a) {
-    f64_tile<BLOCK, IPT, JT, EPS0>(a, (int64_t)blockIdx.x * (BLOCK * IPT), (int)blockIdx.y);
+    const int64_t tile = blockIdx.x / a.nsplit;
+    f64_tile<BLOCK, IPT, JT, EPS0>(a, tile * (BLOCK * IPT), (int)(blockIdx.x % a.nsplit));
+    finish_tile<BLOCK, IPT>(a, tile, tile * (BLOCK * IPT));
 }
 
 template <int BLOCK, int JT>
@@ -94,14 +132,20 @@ int force_variant_ids(int precision, int eps0, int* ids, int max_ids) {
     return c;
 }
 
+int64_t force_tiles(const ForceVariant& v, int64_t n_tgt) {
+    const int64_t tile = (int64_t)v.block * v.ipt;
+    return (n_tgt + tile - 1) / tile;
+}
+
 cudaError_t force_launch(const ForceVariant& v, const ForceArgs& args, cudaStream_t stream) {
     if (args.n_tgt <= 0) return cudaSuccess;
-    const int64_t tile = (int64_t)v.block * v.ipt;
-    dim3 grid((unsigned)((args.n_tgt + tile - 1) / tile), (unsigned)args.nsplit, 1);
+    const int ns = v.precision == kF64Exact ? 1 : args.nsplit;
+    const int64_t blocks = force_tiles(v, args.n_tgt) * ns;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     ForceArgs a = args;
     void* params[] = {(void*)&a};
-    cudaError_t e = cudaLaunchKernel(v.fn, grid, dim3(v.block), params, 0, stream);
-    if (e != cudaSuccess || args.nsplit <= 1) return e;
+    cudaError_t e = cudaLaunchKernel(v.fn, dim3((unsigned)blocks), dim3(v.block), params, 0, stream);
+    if (e != cudaSuccess || args.nsplit <= 1 || args.tile_count) return e;
     force_reduce_kernel<<<(unsigned)((args.n_tgt + 255) / 256), 256, 0, stream>>>(a);
     return cudaGetLastError();
 }

@@ -31,14 +31,29 @@
 namespace gx {
 
 
+// Body index of target ordinal t.  An index-list entry outside [0, n_src) (device index
+// arrays are not checked on the host) is replaced by body 0 for the loads, and
+// write_result() stores NaN for that target instead of its sum.
+__device__ __forceinline__ bool target_ok(const ForceArgs& a, int64_t t) {
+    if (!a.tgt_idx) return true;
+    const int64_t i = a.tgt_idx[t];
+    return i >= 0 && i < a.n_src;
+}
+
 __device__ __forceinline__ int64_t target_body(const ForceArgs& a, int64_t t) {
-    return a.tgt_idx ? a.tgt_idx[t] : a.t_begin + t;
+    if (!a.tgt_idx) return a.t_begin + t;
+    const int64_t i = a.tgt_idx[t];
+    return (i >= 0 && i < a.n_src) ? i : 0;
 }
 
 // Final FP64 result of target t (body index `body`): store, then the optional closing kick
 // v += a*dt in the reference's rounding (integrator.cpp:7-11, no contraction).
 __device__ __forceinline__ void write_result(const ForceArgs& a, int64_t t, int64_t body,
                                              double fx, double fy, double fz) {
+    if (!target_ok(a, t)) {
+        a.ax[t] = a.ay[t] = a.az[t] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
     a.ax[t] = fx;
     a.ay[t] = fy;
     a.az[t] = fz;

@@ -28,6 +28,7 @@
 // the sources in the reference's order starting from the incoming acceleration (the far
 // field), which makes it bit-identical to the reference's evaluate_particle.
 #include <algorithm>
+#include <atomic>
 
 #include <cub/device/device_scan.cuh>
 
@@ -43,6 +44,8 @@ constexpr int kMinChunk = 256;   // ... of at least this many sources
 constexpr int kMinGroup = 8;     // targets of a group, when a leaf's targets are split
 constexpr int kStageCost = 8;    // staging one source costs about this many interactions
 constexpr int kWarpBlockMaxMean = 12;  // mean bodies per leaf up to which blocks are one warp
+constexpr int kFourTargetsMinMean = 24;  // mean bodies per leaf from which threads take four targets
+std::atomic<int> g_p2p_tpt{0};          // 0: by the mean leaf size; 2 or 4: forced (measurement)
 
 // Per leaf (one warp each): number of sources, and the split of the leaf into target groups
 // x source chunks of cost at most about item_cost each, where an item of g targets and s
@@ -107,20 +110,32 @@ __global__ void __launch_bounds__(256) p2p_gather_kernel(const P2PArgs a, int64_
     }
 }
 
-// BS threads per block (a multiple of 32), 4 x BS sources staged per pass; the launch
-// bounds keep 640 threads (20 warps) resident per SM whatever BS.
-template <int MODE, bool EPS0, int BS>
-__global__ void __launch_bounds__(BS, 640 / BS) p2p_kernel(const P2PArgs a) {
+// Resident threads per SM the launch bounds ask for: 640 (20 warps, 96 registers) with two
+// targets per thread; with four, 512 in the mixed form (128 registers) and 384 in FP64 (168
+// registers: four FP64 chains per thread in place of warps).
+constexpr int p2p_threads_per_sm(int mode, int tpt) { return tpt == 2 ? 640 : mode == kMixed ? 512 : 384; }
+
+// BS threads per block (a multiple of 32), 4 x BS sources staged per pass, TPT targets per
+// thread in the fast forms (2 or 4).
+template <int MODE, bool EPS0, int BS, int TPT>
+__global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_kernel(const P2PArgs a) {
     constexpr int kP2PBlock = BS;
     constexpr int kP2PJT = 4 * BS;  // sources staged per shared-memory pass
-    __shared__ __align__(16) double sxd[kP2PJT];
-    __shared__ __align__(16) double syd[kP2PJT];
-    __shared__ __align__(16) double szd[kP2PJT];
-    __shared__ __align__(16) double smd[kP2PJT];
+    static_assert(TPT == 2 || TPT == 4, "two or four targets per thread");
+    // FP64 forms: x, y, z, m as four arrays of kP2PJT doubles.  Mixed form: the same bytes
+    // as float4 (x, x, y, y)[kP2PJT] then (z, z, m, m)[kP2PJT] -- every source duplicated so
+    // that one 16-byte load gives a packed pair per coordinate (two targets per f32x2 op).
+    __shared__ __align__(16) double sbuf[4 * kP2PJT];
+    double* const sxd = sbuf;
+    double* const syd = sbuf + kP2PJT;
+    double* const szd = sbuf + 2 * kP2PJT;
+    double* const smd = sbuf + 3 * kP2PJT;
+    float4* const sA = reinterpret_cast<float4*>(sbuf);
+    float4* const sB = sA + kP2PJT;
     __shared__ int sidx[kP2PJT];
     __shared__ int s_beg[kNearBatch];
     __shared__ int s_pre[kNearBatch + 1];
-    __shared__ double s_red[6][kP2PBlock];
+    __shared__ double s_red[3 * TPT][kP2PBlock];
     __shared__ int s_item, s_last;
 
     // body indices of the staged sources are needed only to skip the target itself where a
@@ -165,14 +180,10 @@ __global__ void __launch_bounds__(BS, 640 / BS) p2p_kernel(const P2PArgs a) {
         auto stage = [&](int c, const double4 q, int j) {
             if (kNeedIdx) sidx[c] = j;
             if (MODE == kMixed) {
-                float* sxf = reinterpret_cast<float*>(sxd);
-                float* syf = reinterpret_cast<float*>(syd);
-                float* szf = reinterpret_cast<float*>(szd);
-                float* smf = reinterpret_cast<float*>(smd);
-                sxf[c] = __double2float_rn(q.x - ox);
-                syf[c] = __double2float_rn(q.y - oy);
-                szf[c] = __double2float_rn(q.z - oz);
-                smf[c] = __double2float_rn(q.w);
+                const float fx = __double2float_rn(q.x - ox), fy = __double2float_rn(q.y - oy);
+                const float fz = __double2float_rn(q.z - oz), fm = __double2float_rn(q.w);
+                sA[c] = make_float4(fx, fx, fy, fy);
+                sB[c] = make_float4(fz, fz, fm, fm);
             } else {
                 sxd[c] = q.x;
                 syd[c] = q.y;
@@ -299,99 +310,129 @@ __global__ void __launch_bounds__(BS, 640 / BS) p2p_kernel(const P2PArgs a) {
             }
             continue;
         } else {
-            // Two targets per thread: the leaf's targets (up to 2 x kP2PBlock per pass) form
-            // H rows of two (row r holds targets r and r + H); every row gets L = block / H
-            // lanes that split the staged sources, and a row's L partial sums are added in
-            // lane order in shared memory.
-            for (int t0 = g_lo; t0 < g_hi; t0 += 2 * kP2PBlock) {
-                const int ntp = min(2 * kP2PBlock, g_hi - t0);
-                const int H = (ntp + 1) >> 1;
+            // TPT targets per thread: the leaf's targets (up to TPT x kP2PBlock per pass) form
+            // H rows of TPT (row r holds targets r, r + H, r + 2H, ...); every row gets
+            // L = block / H lanes that split the staged sources, and a row's L partial sums
+            // are added in lane order in shared memory.
+            for (int t0 = g_lo; t0 < g_hi; t0 += TPT * kP2PBlock) {
+                const int ntp = min(TPT * kP2PBlock, g_hi - t0);
+                const int H = (ntp + TPT - 1) / TPT;
                 const int L = max(1, kP2PBlock / H);
                 const bool act = tid < H * L;
                 const int row = act ? tid / L : 0, lane = act ? tid - row * L : 0;
-                const bool has_b = act && row + H < ntp;
-                const int ia = a.leaf_part[tb + t0 + row];
-                const int ib = has_b ? a.leaf_part[tb + t0 + row + H] : ia;
-                const double xa = a.x[ia], ya = a.y[ia], za = a.z[ia];
-                const double xb = a.x[ib], yb = a.y[ib], zb = a.z[ib];
-                double f[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                int ti[TPT];
+                bool has[TPT];
+                double xt[TPT], yt[TPT], zt[TPT];
+#pragma unroll
+                for (int h = 0; h < TPT; ++h) {
+                    has[h] = act && row + h * H < ntp;
+                    ti[h] = a.leaf_part[tb + t0 + row + (has[h] ? h * H : 0)];
+                    xt[h] = a.x[ti[h]];
+                    yt[h] = a.y[ti[h]];
+                    zt[h] = a.z[ti[h]];
+                }
+                double f[3 * TPT];
+#pragma unroll
+                for (int k = 0; k < 3 * TPT; ++k) f[k] = 0.0;
                 if constexpr (MODE == kF64) {
                     sweep([&](int cnt) {
                         if (!act) return;
 #pragma unroll 2
                         for (int jj = lane; jj < cnt; jj += L) {
                             const double qx = sxd[jj], qy = syd[jj], qz = szd[jj], qm = smd[jj];
-                            const double dxa = qx - xa, dya = qy - ya, dza = qz - za;
-                            const double dxb = qx - xb, dyb = qy - yb, dzb = qz - zb;
-                            const double ra = fma(dza, dza, fma(dya, dya, fma(dxa, dxa, a.eps2)));
-                            const double rb = fma(dzb, dzb, fma(dyb, dyb, fma(dxb, dxb, a.eps2)));
-                            double ya3 = rsqrt_f64(ra), yb3 = rsqrt_f64(rb);
-                            if (EPS0) {
-                                ya3 = (ra == 0.0 || sidx[jj] == ia) ? 0.0 : ya3;
-                                yb3 = (rb == 0.0 || sidx[jj] == ib) ? 0.0 : yb3;
+#pragma unroll
+                            for (int h = 0; h < TPT; ++h) {
+                                const double dx = qx - xt[h], dy = qy - yt[h], dz = qz - zt[h];
+                                const double r = fma(dz, dz, fma(dy, dy, fma(dx, dx, a.eps2)));
+                                double y = rsqrt_f64(r);
+                                if (EPS0) y = (r == 0.0 || sidx[jj] == ti[h]) ? 0.0 : y;
+                                const double w = qm * (y * y * y);
+                                f[3 * h] = fma(dx, w, f[3 * h]);
+                                f[3 * h + 1] = fma(dy, w, f[3 * h + 1]);
+                                f[3 * h + 2] = fma(dz, w, f[3 * h + 2]);
                             }
-                            const double wa = qm * (ya3 * ya3 * ya3), wb = qm * (yb3 * yb3 * yb3);
-                            f[0] = fma(dxa, wa, f[0]);
-                            f[1] = fma(dya, wa, f[1]);
-                            f[2] = fma(dza, wa, f[2]);
-                            f[3] = fma(dxb, wb, f[3]);
-                            f[4] = fma(dyb, wb, f[4]);
-                            f[5] = fma(dzb, wb, f[5]);
                         }
                     });
                 } else {
-                    const float xfa = __double2float_rn(xa - ox), yfa = __double2float_rn(ya - oy),
-                                zfa = __double2float_rn(za - oz);
-                    const float xfb = __double2float_rn(xb - ox), yfb = __double2float_rn(yb - oy),
-                                zfb = __double2float_rn(zb - oz);
-                    CompF c[6];
+                    constexpr int NP = TPT / 2;  // packed target pairs
+                    f2 XI[NP], YI[NP], ZI[NP];
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) c[k].init();
+                    for (int q = 0; q < NP; ++q) {
+                        XI[q] = pk2(__double2float_rn(xt[2 * q] - ox), __double2float_rn(xt[2 * q + 1] - ox));
+                        YI[q] = pk2(__double2float_rn(yt[2 * q] - oy), __double2float_rn(yt[2 * q + 1] - oy));
+                        ZI[q] = pk2(__double2float_rn(zt[2 * q] - oz), __double2float_rn(zt[2 * q + 1] - oz));
+                    }
+                    const f2 E2 = pk2(a.eps2f, a.eps2f);
+                    CompF c[3 * TPT];
+#pragma unroll
+                    for (int k = 0; k < 3 * TPT; ++k) c[k].init();
                     sweep([&](int cnt) {
                         if (!act) return;
-                        const float* sxf = reinterpret_cast<const float*>(sxd);
-                        const float* syf = reinterpret_cast<const float*>(syd);
-                        const float* szf = reinterpret_cast<const float*>(szd);
-                        const float* smf = reinterpret_cast<const float*>(smd);
-                        float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                        f2 PX[NP], PY[NP], PZ[NP];
+#pragma unroll
+                        for (int q = 0; q < NP; ++q) PX[q] = PY[q] = PZ[q] = pk2(0.f, 0.f);
 #pragma unroll 2
                         for (int jj = lane; jj < cnt; jj += L) {
-                            const float qx = sxf[jj], qy = syf[jj], qz = szf[jj], qm = smf[jj];
-                            const float dxa = qx - xfa, dya = qy - yfa, dza = qz - zfa;
-                            const float dxb = qx - xfb, dyb = qy - yfb, dzb = qz - zfb;
-                            const float ra = fmaf(dza, dza, fmaf(dya, dya, fmaf(dxa, dxa, a.eps2f)));
-                            const float rb = fmaf(dzb, dzb, fmaf(dyb, dyb, fmaf(dxb, dxb, a.eps2f)));
-                            float ia3 = rsqrt_f32(ra), ib3 = rsqrt_f32(rb);
-                            if (EPS0) {
-                                ia3 = (ra == 0.f || sidx[jj] == ia) ? 0.f : ia3;
-                                ib3 = (rb == 0.f || sidx[jj] == ib) ? 0.f : ib3;
+                            f2 X, Y, Z, M;
+                            lds_v2b64(reinterpret_cast<const float*>(&sA[jj]), X, Y);
+                            lds_v2b64(reinterpret_cast<const float*>(&sB[jj]), Z, M);
+#pragma unroll
+                            for (int q = 0; q < NP; ++q) {
+                                const f2 dX = sub2(X, XI[q]);
+                                const f2 dY = sub2(Y, YI[q]);
+                                const f2 dZ = sub2(Z, ZI[q]);
+                                f2 R = fma2(dX, dX, E2);
+                                R = fma2(dY, dY, R);
+                                R = fma2(dZ, dZ, R);
+                                float r0, r1;
+                                upk2(R, r0, r1);
+                                float i0 = rsqrt_f32(r0), i1 = rsqrt_f32(r1);
+                                if (EPS0) {
+                                    i0 = (r0 == 0.f || sidx[jj] == ti[2 * q]) ? 0.f : i0;
+                                    i1 = (r1 == 0.f || sidx[jj] == ti[2 * q + 1]) ? 0.f : i1;
+                                }
+                                const f2 I = pk2(i0, i1);
+                                f2 T = mul2(I, I);
+                                T = mul2(T, I);
+                                const f2 W = mul2(M, T);
+                                PX[q] = fma2(dX, W, PX[q]);
+                                PY[q] = fma2(dY, W, PY[q]);
+                                PZ[q] = fma2(dZ, W, PZ[q]);
                             }
-                            const float wa = qm * (ia3 * ia3 * ia3), wb = qm * (ib3 * ib3 * ib3);
-                            p[0] = fmaf(dxa, wa, p[0]);
-                            p[1] = fmaf(dya, wa, p[1]);
-                            p[2] = fmaf(dza, wa, p[2]);
-                            p[3] = fmaf(dxb, wb, p[3]);
-                            p[4] = fmaf(dyb, wb, p[4]);
-                            p[5] = fmaf(dzb, wb, p[5]);
                         }
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) c[k].add(p[k]);
+                        for (int q = 0; q < NP; ++q) {
+                            float p0, p1;
+                            upk2(PX[q], p0, p1);
+                            c[6 * q].add(p0);
+                            c[6 * q + 3].add(p1);
+                            upk2(PY[q], p0, p1);
+                            c[6 * q + 1].add(p0);
+                            c[6 * q + 4].add(p1);
+                            upk2(PZ[q], p0, p1);
+                            c[6 * q + 2].add(p0);
+                            c[6 * q + 5].add(p1);
+                        }
                     });
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) f[k] = c[k].value();
+                    for (int k = 0; k < 3 * TPT; ++k) f[k] = c[k].value();
                 }
                 if (act)
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) s_red[k][tid] = f[k];
+                    for (int k = 0; k < 3 * TPT; ++k) s_red[k][tid] = f[k];
                 __syncthreads();
                 if (act && lane == 0) {
-                    double S[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                    double S[3 * TPT];
+#pragma unroll
+                    for (int k = 0; k < 3 * TPT; ++k) S[k] = 0.0;
                     for (int q = 0; q < L; ++q)
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) S[k] += s_red[k][tid + q];
-                    for (int h = 0; h < (has_b ? 2 : 1); ++h) {
+                        for (int k = 0; k < 3 * TPT; ++k) S[k] += s_red[k][tid + q];
+#pragma unroll
+                    for (int h = 0; h < TPT; ++h) {
+                        if (!has[h]) continue;
                         const int t = t0 + row + h * H;
-                        const int i = h ? ib : ia;
+                        const int i = ti[h];
                         if (i < a.t_begin || i >= a.t_end) continue;
                         if (chunks == 1) {
                             a.ax[i] = a.ax[i] + a.G * S[3 * h];
@@ -433,12 +474,12 @@ __global__ void __launch_bounds__(BS, 640 / BS) p2p_kernel(const P2PArgs a) {
     }
 }
 
-template <int MODE, bool EPS0, int BS>
+template <int MODE, bool EPS0, int BS, int TPT>
 int p2p_occupancy() {
     static int occ = 0;
     if (occ == 0) {
         int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, p2p_kernel<MODE, EPS0, BS>, BS, 0) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, p2p_kernel<MODE, EPS0, BS, TPT>, BS, 0) != cudaSuccess ||
             nb < 1)
             nb = 1;
         occ = nb;
@@ -446,16 +487,18 @@ int p2p_occupancy() {
     return occ;
 }
 
-template <int MODE, bool EPS0, int BS>
+template <int MODE, bool EPS0, int BS, int TPT>
 cudaError_t launch_main(const P2PArgs& a, int sms, cudaStream_t st) {
-    const int grid = sms * p2p_occupancy<MODE, EPS0, BS>();
-    p2p_kernel<MODE, EPS0, BS><<<grid, BS, 0, st>>>(a);
+    const int grid = sms * p2p_occupancy<MODE, EPS0, BS, TPT>();
+    p2p_kernel<MODE, EPS0, BS, TPT><<<grid, BS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
 template <int MODE, bool EPS0>
-cudaError_t launch_bs(const P2PArgs& a, int bs, int sms, cudaStream_t st) {
-    return bs == 32 ? launch_main<MODE, EPS0, 32>(a, sms, st) : launch_main<MODE, EPS0, 128>(a, sms, st);
+cudaError_t launch_bs(const P2PArgs& a, int bs, int tpt, int sms, cudaStream_t st) {
+    if (MODE == kF64Exact || tpt == 2)
+        return bs == 32 ? launch_main<MODE, EPS0, 32, 2>(a, sms, st) : launch_main<MODE, EPS0, 128, 2>(a, sms, st);
+    return bs == 32 ? launch_main<MODE, EPS0, 32, 4>(a, sms, st) : launch_main<MODE, EPS0, 128, 4>(a, sms, st);
 }
 
 }  // namespace
@@ -470,6 +513,8 @@ size_t plan_scan_temp_bytes(int32_t n_leaves) {
 }
 
 }  // namespace
+
+void p2p_set_targets_per_thread(int tpt) { g_p2p_tpt.store(tpt == 2 || tpt == 4 ? tpt : 0); }
 
 size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves) {
     // plan arrays (src, need and scratch offsets int64; chunks, groups, counts, item offsets,
@@ -515,6 +560,10 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     // independent warps per SM, no block-wide barriers) hide the latency of its gathers;
     // larger leaves keep 4-warp blocks that share each staged source among more threads.
     const int bs = n_bodies <= (int64_t)kWarpBlockMaxMean * a.n_leaves ? 32 : 128;
+    // Targets per thread: four (two packed pairs per staged source in the mixed form, four
+    // independent FP64 chains) once the mean leaf fills rows of four; two below that.
+    const int forced = g_p2p_tpt.load();
+    const int tpt = forced ? forced : (n_bodies >= (int64_t)kFourTargetsMinMean * a.n_leaves ? 4 : 2);
     const int64_t item_cost = (int64_t)1024 * bs;
     cudaError_t e = cudaMemsetAsync(a.plan_done, 0, nl * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(int), st);
@@ -526,9 +575,10 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
         return e;
     if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
         return e;
-    if (precision == kF64Exact) return launch_bs<kF64Exact, false>(a, bs, sms, st);
-    if (precision == kF64) return eps0 ? launch_bs<kF64, true>(a, bs, sms, st) : launch_bs<kF64, false>(a, bs, sms, st);
-    return eps0 ? launch_bs<kMixed, true>(a, bs, sms, st) : launch_bs<kMixed, false>(a, bs, sms, st);
+    if (precision == kF64Exact) return launch_bs<kF64Exact, false>(a, bs, 2, sms, st);
+    if (precision == kF64)
+        return eps0 ? launch_bs<kF64, true>(a, bs, tpt, sms, st) : launch_bs<kF64, false>(a, bs, tpt, sms, st);
+    return eps0 ? launch_bs<kMixed, true>(a, bs, tpt, sms, st) : launch_bs<kMixed, false>(a, bs, tpt, sms, st);
 }
 
 }  // namespace gx

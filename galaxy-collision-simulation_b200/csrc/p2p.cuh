@@ -42,6 +42,9 @@ struct P2PArgs {
     int64_t split_max_slots;  // leaves are split only if their slots number at most this
 };
 
+// Targets per thread of the fast forms: 2 or 4 forces that many, 0 restores the choice by
+// mean leaf size (for measurements).
+void p2p_set_targets_per_thread(int tpt);
 // Device scratch launch_p2p needs for n bodies and n_leaves leaves.
 size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves);
 // Stream-ordered: plan on the device, then the persistent leaf kernel (sms x occupancy CTAs).

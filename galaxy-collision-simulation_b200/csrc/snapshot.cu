@@ -351,11 +351,25 @@ extern "C" int gx_snapshot_write(gx_snapshot_writer* w, int step, double time, c
             return cuda_fail(e, "gx_snapshot_write: stream");
         w->device = dev;
     }
+    // each resource of the slot is made on its own, so a failed attempt leaves the slot
+    // usable: the next write that gets it retries what is still missing
     if (!s.dev) {
-        if ((e = cudaMalloc(&s.dev, (size_t)kFields * bytes + 16)) != cudaSuccess) return cuda_fail(e, "gx_snapshot_write");
-        if ((e = cudaMallocHost(&s.pinned, (size_t)kFields * bytes + 16)) != cudaSuccess) return cuda_fail(e, "gx_snapshot_write");
-        if ((e = cudaEventCreateWithFlags(&s.landed, cudaEventDisableTiming)) != cudaSuccess)
+        if ((e = cudaMalloc(&s.dev, (size_t)kFields * bytes + 16)) != cudaSuccess) {
+            s.dev = nullptr;
             return cuda_fail(e, "gx_snapshot_write");
+        }
+    }
+    if (!s.pinned) {
+        if ((e = cudaMallocHost(&s.pinned, (size_t)kFields * bytes + 16)) != cudaSuccess) {
+            s.pinned = nullptr;
+            return cuda_fail(e, "gx_snapshot_write");
+        }
+    }
+    if (!s.landed) {
+        if ((e = cudaEventCreateWithFlags(&s.landed, cudaEventDisableTiming)) != cudaSuccess) {
+            s.landed = nullptr;
+            return cuda_fail(e, "gx_snapshot_write");
+        }
     }
     s.from_device = true;
     cudaStream_t st = (cudaStream_t)stream;
@@ -386,4 +400,42 @@ extern "C" int gx_snapshot_write_diagnostics(gx_snapshot_writer* w, int step, do
                                d->center_of_mass[1], d->center_of_mass[2], d->angular_momentum[0],
                                d->angular_momentum[1], d->angular_momentum[2]);
     return r > 0 ? GX_OK : gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_snapshot_write_diagnostics: write failed");
+}
+
+// write_metadata (snapshot_writer.cpp:49-69).  The reference streams doubles with the
+// ostream defaults (no precision set on that stream): "%g", six significant digits.
+extern "C" int gx_snapshot_write_metadata(gx_snapshot_writer* w, const gx_run_metadata* md) {
+    if (!w || !md) return gxi_fail(GX_ERR_INVALID_ARGUMENT, "gx_snapshot_write_metadata: null argument");
+    auto esc = [](const char* s) {
+        std::string e;
+        for (const char* p = s ? s : ""; *p; ++p) {
+            if (*p == '"' || *p == '\\') e.push_back('\\');
+            e.push_back(*p);
+        }
+        return e;
+    };
+    const std::filesystem::path path = w->dir / "metadata.json";
+    FILE* f = std::fopen(path.string().c_str(), "w");
+    if (!f) return gxi_fail(GX_ERR_INVALID_ARGUMENT, ("could not write " + path.string()).c_str());
+    const int r = std::fprintf(f,
+                               "{\n"
+                               "  \"name\": \"%s\",\n"
+                               "  \"solver\": \"%s\",\n"
+                               "  \"particle_count\": %lld,\n"
+                               "  \"steps\": %d,\n"
+                               "  \"dt\": %g,\n"
+                               "  \"snapshot_every\": %d,\n"
+                               "  \"dim\": %d,\n"
+                               "  \"gravitational_constant\": %g,\n"
+                               "  \"softening\": %g,\n"
+                               "  \"tree_theta\": %g,\n"
+                               "  \"tree_leaf_capacity\": %lld,\n"
+                               "  \"fmm_expansion_order\": %d\n"
+                               "}\n",
+                               esc(md->name).c_str(), esc(md->solver).c_str(), (long long)md->particle_count,
+                               (int)md->steps, md->dt, (int)md->snapshot_every, (int)md->dim,
+                               md->gravitational_constant, md->softening, md->tree_theta,
+                               (long long)md->tree_leaf_capacity, (int)md->fmm_expansion_order);
+    const bool ok = r > 0 && std::fclose(f) == 0;
+    return ok ? GX_OK : gxi_fail(GX_ERR_INVALID_ARGUMENT, ("write failed: " + path.string()).c_str());
 }

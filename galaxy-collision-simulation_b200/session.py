@@ -82,6 +82,22 @@ class Session:
     def step(self, n_steps: int, dt: float, precision=PRECISION_F64):
         _ffi.call("gx_session_step", self._h, int(n_steps), float(dt), _ffi.precision_code(precision))
 
+    def set_persistent(self, enable: bool) -> None:
+        """Small FP64 / exact-form systems step in one cooperative launch (default True)."""
+        _ffi.call("gx_session_set_persistent", self._h, 1 if enable else 0)
+
+    def set_targets(self, begin: int, count: int) -> None:
+        """Owned bodies [begin, begin + count): the only ones kicked, drifted and given forces."""
+        _ffi.call("gx_session_set_targets", self._h, int(begin), int(count))
+
+    def kick_drift(self, kick_dt: float, drift_dt: float) -> None:
+        """Opening half of a KDK step of the owned bodies (stream-ordered)."""
+        _ffi.call("gx_session_kick_drift", self._h, float(kick_dt), float(drift_dt))
+
+    def force_kick(self, kick_dt: float, precision=PRECISION_F64) -> None:
+        """Closing half: forces on the owned bodies from all bodies, then the kick."""
+        _ffi.call("gx_session_force_kick", self._h, float(kick_dt), _ffi.precision_code(precision))
+
     def diagnostics(self) -> Diagnostics:
         d = _ffi.DiagnosticsStruct()
         _ffi.call("gx_session_diagnostics", self._h, ctypes.byref(d))

@@ -2,7 +2,7 @@
 (cpp/io/snapshot_writer.cpp:38-128), taken asynchronously from device-resident state.
 
 ``SnapshotWriter(directory, n, group_id)`` writes snapshot_%06d.csv files byte-identical to the
-reference's, diagnostics.csv rows, and optionally the binary SoA form snapshot_%06d.bin
+reference's, diagnostics.csv rows, metadata.json, and optionally the binary SoA form snapshot_%06d.bin
 (``read_binary`` loads one).  ``write`` accepts host numpy arrays, CUDA tensors or a
 ``ParticleSet``; ``Session.snapshot`` snapshots a session without stalling its stream.
 """
@@ -46,6 +46,18 @@ class SnapshotWriter:
                                     (ctypes.c_double * 3)(*d.momentum), (ctypes.c_double * 3)(*d.center_of_mass),
                                     (ctypes.c_double * 3)(*d.angular_momentum))
         _ffi.call("gx_snapshot_write_diagnostics", self._h, int(step), float(time), ctypes.byref(st))
+
+    def write_metadata(self, name: str, solver: str, particle_count: int, steps: int, dt: float,
+                       snapshot_every: int, dim: int = 3, gravitational_constant: float = 1.0,
+                       softening: float = 0.02, tree_theta: float = 0.6, tree_leaf_capacity: int = 16,
+                       fmm_expansion_order: int = 4) -> None:
+        """metadata.json of the run (SnapshotWriter::write_metadata, snapshot_writer.cpp:49-69);
+        the defaults are SimulationConfig's (cpp/core/config.hpp:20-35)."""
+        md = _ffi.RunMetadataStruct(str(name).encode(), str(solver).encode(), int(particle_count), int(steps),
+                                    int(snapshot_every), int(dim), int(fmm_expansion_order), float(dt),
+                                    float(gravitational_constant), float(softening), float(tree_theta),
+                                    int(tree_leaf_capacity))
+        _ffi.call("gx_snapshot_write_metadata", self._h, ctypes.byref(md))
 
     def flush(self) -> None:
         _ffi.call("gx_snapshot_writer_flush", self._h)

@@ -96,7 +96,10 @@ int gx_direct_accel(int64_t n, const double* x, const double* y, const double* z
 
 /* compute_direct_accelerations_for_targets (cpp/direct/direct_solver.cpp:59-83): targets
  * [begin, end) against all n sources; results at ax[i - begin].  With `targets` non-null,
- * targets[k] for k < n_targets instead of a range (begin/end ignored; n_targets used). */
+ * targets[k] for k < n_targets instead of a range (begin/end ignored; n_targets used).
+ * Host index arrays are checked (an entry outside [0, n) returns GX_ERR_INVALID_ARGUMENT);
+ * device index arrays are not read back: an entry outside [0, n) is never used as an
+ * address, and its row of ax, ay, az is NaN. */
 int gx_direct_accel_targets(int64_t n, const double* x, const double* y, const double* z,
                             const double* m, int64_t begin, int64_t end, const int64_t* targets,
                             int64_t n_targets, gx_physics phys, int precision, double* ax,
@@ -146,8 +149,27 @@ int gx_session_get_state(gx_session* s, double* x, double* y, double* z, double*
 /* Device pointers of the resident arrays, in the order x,y,z,vx,vy,vz,ax,ay,az,m. */
 int gx_session_device_arrays(gx_session* s, double** ptrs10);
 int gx_session_compute_accelerations(gx_session* s, int precision);
-/* n_steps KDK steps (kick dt/2, drift dt, force, kick dt/2 per step). */
+/* n_steps KDK steps (kick dt/2, drift dt, force, kick dt/2 per step).  Systems of at most
+ * 4096 bodies in GX_PRECISION_F64 or _F64_EXACT run all n_steps in one cooperative launch
+ * (each step: kick-drift, one grid barrier, force, kick; the exact form stays bit-identical
+ * to the reference); larger systems and the mixed form replay CUDA graphs of 32 steps.  A
+ * grid barrier that cannot complete within 4 s stops the launch, leaves the state of the
+ * previous call, and the next synchronising call returns GX_ERR_TIMEOUT. */
 int gx_session_step(gx_session* s, int64_t n_steps, double dt, int precision);
+/* Whether small systems use the single-launch step loop (default 1); 0 replays graphs of
+ * separate kick-drift and force launches instead.  No reference counterpart. */
+int gx_session_set_persistent(gx_session* s, int enable);
+/* The bodies this session owns: [begin, begin + count) (default: all n).  Steps, the two
+ * half steps below and compute_accelerations kick, drift and evaluate forces for the owned
+ * bodies only, with all n bodies as sources -- the ownership range of the reference's MPI
+ * step (cpp/mpi/distributed_solver.cpp:68-79, cpp/core/main.cpp:240-253).  A multi-process
+ * caller exchanges the owned positions between the two halves of each step. */
+int gx_session_set_targets(gx_session* s, int64_t begin, int64_t count);
+/* Opening half of a KDK step for the owned bodies: v += a * kick_dt, then x += v * drift_dt
+ * (kick and drift, cpp/core/integrator.cpp:7-17). */
+int gx_session_kick_drift(gx_session* s, double kick_dt, double drift_dt);
+/* Closing half: accelerations of the owned bodies from all n, then v += a * kick_dt. */
+int gx_session_force_kick(gx_session* s, double kick_dt, int precision);
 int gx_session_diagnostics(gx_session* s, gx_diagnostics* out);
 /* gx_snapshot_write of the session's state on the session's stream (declared below). */
 struct gx_snapshot_writer;
@@ -236,6 +258,27 @@ int gx_snapshot_write(gx_snapshot_writer* w, int step, double time, const double
 /* write_diagnostics (snapshot_writer.cpp:99-128): one row of diagnostics.csv. */
 int gx_snapshot_write_diagnostics(gx_snapshot_writer* w, int step, double time,
                                   const gx_diagnostics* d);
+
+/* The run description that SnapshotWriter::write_metadata takes from SimulationConfig
+ * (cpp/core/config.hpp:20-35) and the particle count. */
+typedef struct gx_run_metadata {
+    const char* name;
+    const char* solver;
+    int64_t particle_count;
+    int32_t steps;
+    int32_t snapshot_every;
+    int32_t dim;
+    int32_t fmm_expansion_order;
+    double dt;
+    double gravitational_constant;
+    double softening;
+    double tree_theta;
+    int64_t tree_leaf_capacity;
+} gx_run_metadata;
+/* write_metadata (snapshot_writer.cpp:49-69): metadata.json in the writer's directory, byte
+ * for byte the reference's (strings with '"' and '\' escaped; doubles as the default
+ * ostream format prints them, six significant digits). */
+int gx_snapshot_write_metadata(gx_snapshot_writer* w, const gx_run_metadata* md);
 
 /* ---- FMM (cpp/fmm/fmm_solver.hpp:15-20, fmm_solver.cpp:315-333) --------------------- */
 /* FmmOptions with the reference's defaults: theta 0.6, leaf_capacity 16, max_depth 32,
@@ -372,9 +415,19 @@ int gx_direct_accel_noalloc(int64_t n, const double* x, const double* y, const d
 int gx_variant_count(int precision, int* count);
 int gx_variant_describe(int precision, int variant, char* buf, int buflen);
 
-/* ---- fault injection for tests (host side only; never touches the GPU) ------------- */
+/* ---- fault injection for tests (no GPU fault: failures are made on the host or by a
+ * participant that leaves a bounded wait) ----------------------------------------------- */
 /* The next `count` device allocations made by the library fail with GX_ERR_OUT_OF_MEMORY. */
 int gx_debug_fail_allocations(int count);
+/* The next single-launch session step loop (gx_session_step on a small system) loses one
+ * participant: its first CTA leaves before the barrier of step `step` instead of arriving,
+ * and the barrier waits are cut to 0.2 s, so the other CTAs give up, the launch ends early
+ * and the next synchronising session call returns GX_ERR_TIMEOUT.  Nothing faults. */
+int gx_debug_stall_barrier(int64_t step);
+/* Targets per thread of the FP64 and mixed P2P kernels: 2 or 4 forces that shape, 0 (the
+ * default) picks it from the mean leaf size.  For measurements; results agree within the
+ * forms' tolerances either way. */
+int gx_debug_p2p_targets_per_thread(int tpt);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

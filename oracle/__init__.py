@@ -23,6 +23,7 @@ REF_PATH = ORACLE_DIR / "_ref" / "libgxref.so"
 REF_SIM_CPU = ORACLE_DIR / "_ref" / "fmm_galaxy_sim_cpu"
 REF_SIM_B200 = ORACLE_DIR / "_ref" / "fmm_galaxy_sim_b200"
 REF_SMOKE_B200 = ORACLE_DIR / "_ref" / "ref_smoke_tests_b200"
+REF_SIM_RESIDENT = ORACLE_DIR / "_ref" / "fmm_galaxy_sim_resident"
 
 _port = None
 _ref = None
@@ -78,6 +79,8 @@ def ref():
         lib.ref_smoke80_inputs.argtypes = [P, P, P, P]
         lib.ref_generate_galaxies.argtypes = [c_int, P, c_double, c_double, ctypes.c_uint64, P, P, P, P, P, P, P, P]
         lib.ref_generate_galaxies.restype = c_int64
+        lib.ref_write_metadata.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, c_int64, c_int, c_double,
+                                           c_int, c_int, c_double, c_double, c_double, c_int64, c_int]
         lib.ref_write_outputs.argtypes = [ctypes.c_char_p, c_int64, P, P, P, P, P, P, P, P, P, P, P, c_int, c_double,
                                           P]
         lib.ref_fmm_moments.argtypes = [c_int64, P, P, P, P, c_double, c_double, c_double, c_int64, c_int, c_int64, P,
@@ -273,6 +276,14 @@ def ref_write_outputs(directory, state: dict, m, group, step, time, diag13):
     d = _f(diag13)
     ref().ref_write_outputs(str(directory).encode(), len(arrs[0]), *map(_p, arrs), None if g is None else _p(g),
                             int(step), float(time), _p(d))
+
+
+def ref_write_metadata(directory, name, solver, particle_count, steps, dt, snapshot_every, dim, G, eps, theta,
+                       leaf_capacity, order):
+    """The reference SnapshotWriter writes metadata.json (and an empty diagnostics.csv)."""
+    ref().ref_write_metadata(str(directory).encode(), str(name).encode(), str(solver).encode(), int(particle_count),
+                             int(steps), float(dt), int(snapshot_every), int(dim), float(G), float(eps), float(theta),
+                             int(leaf_capacity), int(order))
 
 
 GALAXY_FIELDS = ("n_particles", "mass", "radius", "position", "velocity", "orientation", "group_id", "thickness",

@@ -313,6 +313,30 @@ int ref_write_outputs(const char* directory, int64_t n, const double* x, const d
     return 0;
 }
 
+// SnapshotWriter::write_metadata (snapshot_writer.cpp:49-69) of a SimulationConfig holding
+// these values.
+int ref_write_metadata(const char* directory, const char* name, const char* solver, int64_t particle_count,
+                       int steps, double dt, int snapshot_every, int dim, double G, double eps, double theta,
+                       int64_t leaf_capacity, int order) {
+    fmmgalaxy::SimulationConfig cfg;
+    cfg.output.directory = directory;
+    cfg.output.format = "csv";
+    cfg.name = name;
+    cfg.solver = solver;
+    cfg.steps = steps;
+    cfg.dt = dt;
+    cfg.snapshot_every = snapshot_every;
+    cfg.dim = dim;
+    cfg.physics.gravitational_constant = G;
+    cfg.physics.softening = eps;
+    cfg.tree_theta = theta;
+    cfg.tree_leaf_capacity = static_cast<std::size_t>(leaf_capacity);
+    cfg.fmm_expansion_order = order;
+    fmmgalaxy::SnapshotWriter w(cfg);
+    w.write_metadata(cfg, static_cast<std::size_t>(particle_count));
+    return 0;
+}
+
 // generate_galaxies (initial_conditions.cpp:92-114).  Galaxy g is cfg[13 g .. 13 g + 12] =
 // n, mass, radius, position xyz, velocity xyz, orientation, group id, thickness, inclination.
 int64_t ref_generate_galaxies(int n_gal, const double* cfg, double G, double eps, uint64_t seed, double* x, double* y,

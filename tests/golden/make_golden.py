@@ -1,5 +1,5 @@
-"""Regenerates the golden fixtures of tests/golden/ (run in a tree where the reference is
-present: python tests/golden/make_golden.py [REFERENCE_ROOT]).
+"""Regenerates the golden fixtures of tests/golden/ (run where a reference checkout is
+present: python tests/golden/make_golden.py REFERENCE_ROOT).
 
 Sources, all produced by the reference itself:
 * experiments/benchmarks/local_cpu/outputs/direct_{250,1000}_r1/ and fmm_1000_r1/ -- the
@@ -17,7 +17,9 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) < 2:
+    sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT (the reference checkout)")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).resolve().parent
 BENCH = REF / "experiments/benchmarks/local_cpu/outputs"
 

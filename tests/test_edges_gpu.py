@@ -146,3 +146,28 @@ def test_session_step_graph_cache_over_many_lengths():
     for _ in range(176):
         gx.cuda_direct_leapfrog_step(q, 0.001, gx.PhysicsParams(1.0, 0.05), F64)
     assert np.max(np.abs(st["x"] - q.x)) <= 1e-12
+
+
+@pytest.mark.parametrize("prec", [F64, MIX, EXACT])
+def test_device_target_indices_out_of_range_give_nan(prec):
+    """Device index arrays are not checked on the host: an entry outside [0, n) is never read
+    through (no out-of-bounds access) and its row of the result is NaN; the other rows are
+    the normal per-target sums."""
+    p = gx.ics.two_disk_encounter(300, 300, 31, 0.05)
+    n = len(p)
+    d = {k: torch.from_numpy(getattr(p, k)).cuda() for k in ("x", "y", "z", "m")}
+    idx = np.array([5, -1, 17, n, 599, -(2 ** 40), 0], np.int64)
+    di = torch.from_numpy(idx).cuda()
+    out = [torch.zeros(len(idx), dtype=torch.float64, device="cuda") for _ in range(3)]
+    lib = _ffi.load()
+    st = lib.gx_direct_accel_targets(n, *(d[k].data_ptr() for k in ("x", "y", "z", "m")), 0, 0, di.data_ptr(),
+                                     len(idx), _ffi.physics(1.0, 0.05), prec, *(o.data_ptr() for o in out),
+                                     torch.cuda.current_stream().cuda_stream)
+    assert st == 0, _ffi.last_error()
+    got = torch.stack(out, 1).cpu().numpy()
+    bad = (idx < 0) | (idx >= n)
+    assert np.all(np.isnan(got[bad]))
+    ok = idx[~bad]
+    want = oracle.direct_indexed(p.x, p.y, p.z, p.m, 1.0, 0.05, ok)
+    e = rel_err(got[~bad], want)
+    assert e.max() <= (0.0 if prec == EXACT else 1e-11 if prec == F64 else 1e-4)

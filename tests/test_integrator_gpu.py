@@ -170,3 +170,79 @@ def test_autotune_keeps_results():
         assert np.array_equal(before["ax"], after["ax"])  # tuning restores the state
         v, js = s.get_config(MIX)
         assert "mixed" in gx.describe_variant(MIX, v) and js >= 1
+
+
+@pytest.mark.parametrize("n,steps", [(1, 3), (2, 5), (33, 7), (1000, 20), (1185, 6), (4096, 3)])
+def test_single_launch_step_loop(n, steps):
+    """Small systems step in one cooperative launch (csrc/small.cu).  The exact form is the
+    oracle's per-target leapfrog bit for bit (and equals the graph-replayed step loop); the
+    FP64 form stays within the FP64 tolerance of the graph loop.  Sizes cover one, two and
+    four targets per warp (1185 > 148 SMs x 8 warps)."""
+    eps, dt = 0.05, 0.005
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 700 + n, eps)
+    params = gx.PhysicsParams(1.0, eps)
+    out = {}
+    for persistent in (True, False):
+        for prec in (EXACT, F64):
+            with gx.Session(n, params) as s:
+                s.set_persistent(persistent)
+                s.set_particles(p)
+                s.compute_accelerations(prec)
+                s.step(steps, dt, prec)
+                s.step(1, dt, prec)  # a second launch continues from the first one's state
+                out[persistent, prec] = s.get_state()
+    a0 = oracle.direct_targets(p.x, p.y, p.z, p.m, 1.0, eps)
+    st0 = dict(x=p.x, y=p.y, z=p.z, vx=p.vx, vy=p.vy, vz=p.vz, ax=a0[:, 0], ay=a0[:, 1], az=a0[:, 2])
+    want = oracle.leapfrog(st0, p.m, 1.0, eps, dt, steps + 1, solver=1)
+    for k in STATE:
+        assert np.array_equal(out[True, EXACT][k], want[k]), k
+        assert np.array_equal(out[False, EXACT][k], want[k]), k
+    for k in ("x", "y", "z"):
+        assert np.max(np.abs(out[True, F64][k] - out[False, F64][k])) <= 1e-12
+    acc = lambda st: np.stack([st["ax"], st["ay"], st["az"]], 1)
+    if n > 1:
+        assert rel_err(acc(out[True, F64]), acc(out[False, F64])).max() <= 1e-11
+
+
+def test_single_launch_step_loop_zero_softening():
+    """Coincident bodies with softening 0: the pair is skipped (s2 == 0) in both forms."""
+    n = 300
+    p = gx.ics.two_disk_encounter(150, 150, 77, 0.05)
+    p.x[5], p.y[5], p.z[5] = p.x[6], p.y[6], p.z[6]
+    params = gx.PhysicsParams(1.0, 0.0)
+    got = {}
+    for prec in (EXACT, F64):
+        with gx.Session(n, params) as s:
+            s.set_particles(p)
+            s.compute_accelerations(prec)
+            s.step(4, 1e-4, prec)
+            got[prec] = s.get_state()
+    a0 = oracle.direct_targets(p.x, p.y, p.z, p.m, 1.0, 0.0)
+    st0 = dict(x=p.x, y=p.y, z=p.z, vx=p.vx, vy=p.vy, vz=p.vz, ax=a0[:, 0], ay=a0[:, 1], az=a0[:, 2])
+    want = oracle.leapfrog(st0, p.m, 1.0, 0.0, 1e-4, 4, solver=1)
+    for k in STATE:
+        assert np.array_equal(got[EXACT][k], want[k]), k
+        assert np.all(np.isfinite(got[F64][k]))
+
+
+def test_single_launch_barrier_timeout_is_reported():
+    """A participant that leaves before a grid barrier (test hook) makes the others' bounded
+    waits run out: the launch ends early, the state stays that of the previous call, the next
+    synchronising call reports GX_ERR_TIMEOUT, and the session keeps working afterwards."""
+    n, eps, dt = 1000, 0.05, 0.005
+    p = gx.ics.two_disk_encounter(500, 500, 12, eps)
+    with gx.Session(n, gx.PhysicsParams(1.0, eps)) as s:
+        s.set_particles(p)
+        s.compute_accelerations(EXACT)
+        s.step(3, dt, EXACT)
+        before = s.get_state()
+        gx._ffi.call("gx_debug_stall_barrier", 2)
+        s.step(5, dt, EXACT)
+        with pytest.raises(gx.GxError) as ei:
+            s.synchronize()
+        assert ei.value.status == gx.GX_ERR_TIMEOUT
+        after = s.get_state()
+        for k in STATE:
+            assert np.array_equal(after[k], before[k]), k
+        s.step(2, dt, EXACT)  # the session still steps
+        s.synchronize()

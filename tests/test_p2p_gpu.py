@@ -160,3 +160,35 @@ def test_fmm_trajectory_with_gpu_near_field(golden):
         assert np.array_equal(st[k], ref[k]), k
         want = g[f"{k}20"]
         assert np.max(np.abs(st[k] - want)) <= 1e-12 * max(1.0, np.abs(want).max()), k
+
+
+@pytest.fixture
+def p2p_shape():
+    """Forces the P2P kernel's targets per thread for one test, then restores the default."""
+    def force(tpt):
+        gx._ffi.call("gx_debug_p2p_targets_per_thread", tpt)
+    yield force
+    gx._ffi.call("gx_debug_p2p_targets_per_thread", 0)
+
+
+@pytest.mark.parametrize("tpt", [2, 4])
+@pytest.mark.parametrize("n,cap,theta,eps", [(20000, 64, 0.6, 0.02), (6000, 16, 0.5, 0.02), (3000, 200, 0.6, 0.02),
+                                             (2000, 32, 0.6, 0.0)])
+@pytest.mark.parametrize("prec", [F64, MIX])
+def test_near_field_both_thread_shapes(p2p_shape, tpt, n, cap, theta, eps, prec):
+    """Two and four targets per thread (rows of a leaf's targets; the mixed form packs target
+    pairs into f32x2 lanes) give the oracle's near field within each form's tolerance, with
+    one-warp and four-warp blocks (small and large leaves), split leaves and zero softening."""
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, n + cap + tpt, 0.02)
+    if eps == 0.0:
+        p.x[7], p.y[7], p.z[7] = p.x[8], p.y[8], p.z[8]
+    lists = gx.build_leaf_lists(p.x, p.y, p.z, p.m, eps, theta, cap)
+    L = dict(leaf_offsets=lists.leaf_offsets, leaf_particles=lists.leaf_particles, near_offsets=lists.near_offsets,
+             near_leaves=lists.near_leaves)
+    ref = oracle.p2p_near(p.x, p.y, p.z, p.m, 1.0, eps, L)
+    p2p_shape(tpt)
+    got = run_p2p(p.x, p.y, p.z, p.m, lists, eps, prec)
+    assert np.all(np.isfinite(got))
+    e = rel_err(got, ref)
+    lim = (1e-13, 1e-11) if prec == F64 else (1e-6, 1e-4)
+    assert np.median(e) <= lim[0] and e.max() <= lim[1], (np.median(e), e.max())

@@ -135,3 +135,92 @@ def test_two_rank_ensemble_by_instance(tmp_path):
         r = oracle.leapfrog(st, p.m[b], 1.0, 0.05, 0.005, 2, solver=1)
         for k, name in enumerate(("x", "y", "z", "vx", "vy", "vz")):
             assert np.array_equal(got[k, b], r[name]), (i, name)
+
+
+class CpuShard:
+    """The engine-shard interface of ShardedSession on the CPU: the padded slot arrays as
+    torch tensors, the reference's kick/drift rounding (separate multiply and add), and the
+    oracle's per-target sum over all slots for the owned ones."""
+
+    def __init__(self, slots, eps):
+        self.slots, self.eps = slots, eps
+
+    def set_targets(self, begin, count):
+        self.sl = slice(begin, begin + count)
+
+    def set_state(self, arrays, acc):
+        self.s = {k: torch.from_numpy(np.array(arrays[k], dtype=np.float64)) for k in arrays}
+        for k, a in zip(("ax", "ay", "az"), acc or [np.zeros(self.slots)] * 3):
+            self.s[k] = torch.from_numpy(np.array(a, dtype=np.float64))
+
+    def position_tensors(self):
+        return [self.s["x"], self.s["y"], self.s["z"]]
+
+    @staticmethod
+    def send_view(t):
+        return t.clone()  # gloo's all-gather does not take a slice of its output as input
+
+    def kick_drift(self, h, dt):
+        s, sl = self.s, self.sl
+        for v, a, x in (("vx", "ax", "x"), ("vy", "ay", "y"), ("vz", "az", "z")):
+            s[v][sl] = s[v][sl] + s[a][sl] * h
+            s[x][sl] = s[x][sl] + s[v][sl] * dt
+
+    def force_kick(self, h, precision=None):
+        s, sl = self.s, self.sl
+        a = oracle.direct_targets(*(s[k].numpy() for k in ("x", "y", "z", "m")), 1.0, self.eps, sl.start, sl.stop)
+        for c, (ak, vk) in enumerate((("ax", "vx"), ("ay", "vy"), ("az", "vz"))):
+            s[ak][sl] = torch.from_numpy(np.ascontiguousarray(a[:, c]))
+            if h != 0.0:
+                s[vk][sl] = s[vk][sl] + s[ak][sl] * h
+
+    def state(self):
+        return {k: v.numpy().copy() for k, v in self.s.items()}
+
+
+def _session_worker(rank, world, port, n, steps, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import gx
+        from gx.sharded import ShardLayout, ShardedSession
+        p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 42, 0.05)
+        sh = ShardedSession(n, None, backend=CpuShard(ShardLayout(n, world).slots, 0.05))
+        sh.set_state(p.x, p.y, p.z, p.vx, p.vy, p.vz, p.m)
+        sh.compute_accelerations()
+        sh.step(steps, 0.005)
+        st = sh.get_state()
+        if rank == 0:
+            np.save(out, np.stack([st[k] for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n,world", [(101, 2), (7, 3)])
+def test_sharded_session_padded_layout_matches_single_process(tmp_path, n, world):
+    """ShardedSession's padded rank-major layout (zero-mass padding slots, in-place
+    all-gathers of x, y, z) reproduces the single-process per-target leapfrog of the oracle
+    bit for bit, accelerations included, with uneven ownership ranges."""
+    steps = 3
+    out = str(tmp_path / "state.npy")
+    mp.start_processes(_session_worker, args=(world, _free_port(), n, steps, out), nprocs=world, start_method="spawn")
+    got = np.load(out)
+    import gx
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 42, 0.05)
+    a0 = oracle.direct_targets(p.x, p.y, p.z, p.m, 1.0, 0.05)
+    st = dict(x=p.x, y=p.y, z=p.z, vx=p.vx, vy=p.vy, vz=p.vz, ax=a0[:, 0], ay=a0[:, 1], az=a0[:, 2])
+    ref = oracle.leapfrog(st, p.m, 1.0, 0.05, 0.005, steps, solver=1)
+    expect = np.stack([ref[k] for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")])
+    assert np.array_equal(got, expect)
+
+
+def test_shard_layout_round_trip():
+    from gx.sharded import ShardLayout
+    for n, world in ((0, 1), (1, 1), (10, 3), (101, 2), (1000, 8)):
+        L = ShardLayout(n, world)
+        a = np.arange(n, dtype=np.float64) + 0.5
+        padded = L.pad(a)
+        assert len(padded) == L.slots == L.chunk * world
+        assert np.array_equal(L.unpad(padded), a)
+        assert np.count_nonzero(padded) == n  # padding slots stay zero (zero mass)

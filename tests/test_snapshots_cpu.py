@@ -59,3 +59,24 @@ def test_writer_errors(tmp_path):
     f.write_text("x")
     with pytest.raises(gx.GxError):
         gx.SnapshotWriter(f / "sub", 10)
+
+
+@need_ref
+@pytest.mark.parametrize("md", [
+    dict(name="benchmark_direct_1000", solver="cuda-direct", particle_count=1000, steps=20, dt=0.01,
+         snapshot_every=20, dim=3, G=1.0, eps=0.025, theta=0.58, leaf_capacity=16, order=4),
+    dict(name='quote " and back\\slash', solver="fmm", particle_count=1 << 20, steps=123456, dt=1.0 / 3.0,
+         snapshot_every=7, dim=2, G=6.674e-11, eps=1e-300, theta=0.6, leaf_capacity=64, order=0),
+    dict(name="", solver="direct", particle_count=0, steps=0, dt=1e22, snapshot_every=1, dim=3, G=-0.0,
+         eps=123456789.0, theta=1e-5, leaf_capacity=1, order=3),
+])
+def test_metadata_matches_reference_writer(tmp_path, md):
+    """metadata.json (SnapshotWriter::write_metadata, snapshot_writer.cpp:49-69) byte for byte:
+    escaped strings, integers and doubles in the default six-digit ostream format."""
+    oracle.ref_write_metadata(tmp_path / "ref", md["name"], md["solver"], md["particle_count"], md["steps"], md["dt"],
+                              md["snapshot_every"], md["dim"], md["G"], md["eps"], md["theta"], md["leaf_capacity"],
+                              md["order"])
+    with gx.SnapshotWriter(tmp_path / "ours", 1) as w:
+        w.write_metadata(md["name"], md["solver"], md["particle_count"], md["steps"], md["dt"], md["snapshot_every"],
+                         md["dim"], md["G"], md["eps"], md["theta"], md["leaf_capacity"], md["order"])
+    assert (tmp_path / "ours" / "metadata.json").read_bytes() == (tmp_path / "ref" / "metadata.json").read_bytes()

@@ -7,15 +7,19 @@ The entry point keeps its scratch in a fixed device array inside the library ins
 
 Checked here through the C ABI: two calls in a row (different systems, so the second call
 finds the first call's leftovers in the shared array) give the same accelerations as the
-allocating entry point gx_direct_accel within the engine's tolerances; sizes above the fixed
-limit and host arrays are refused with a clear error.  This file is collected last and
-depends on no other test, so it also passes alone in a fresh process.
+allocating entry point gx_direct_accel within the engine's tolerances, and the same as the
+oracle's per-target direct sum (the reference's compute_direct_accelerations_for_targets
+restated in C): bit for bit in the exact form, within 1e-12 relative in FP64, at a size that
+needs no source split and at the limit, where the partial sums of a split fill the array;
+sizes above the fixed limit and host arrays are refused with a clear error.  This file is
+collected last and depends on no other test, so it also passes alone in a fresh process.
 """
 import numpy as np
 import pytest
 import torch
 
 import gx
+import oracle
 from gx import _ffi
 
 pytestmark = pytest.mark.gpu
@@ -54,6 +58,20 @@ def test_two_calls_in_a_row_match_the_allocating_entry_point(precision, median_t
         assert np.all(np.isfinite(got))
         e = _rel(got, want)
         assert np.median(e) <= median_tol and e.max() <= max_tol, (np.median(e), e.max())
+
+
+@pytest.mark.parametrize("n,seed,eps", [(3001, 303, 0.05), (LIMIT, 404, 0.02)])
+def test_two_calls_in_a_row_match_the_oracle(n, seed, eps):
+    d = _device_system(n, seed, eps)
+    h = {k: d[k].cpu().numpy() for k in ("x", "y", "z", "m")}
+    rng = np.random.default_rng(seed)
+    idx = np.arange(n) if n <= 4096 else np.sort(rng.choice(n, 2048, replace=False))
+    want = oracle.direct_indexed(h["x"], h["y"], h["z"], h["m"], 1.0, eps, idx, threads=oracle.default_threads())
+    for _ in range(2):  # the second call finds the first call's contents in the array
+        exact = _accel("gx_direct_accel_noalloc", d, eps, gx.PRECISION_F64_EXACT)[idx]
+        assert np.array_equal(exact, want)
+        f64 = _accel("gx_direct_accel_noalloc", d, eps, gx.PRECISION_F64)[idx]
+        assert _rel(f64, want).max() <= 1e-12
 
 
 def test_limits_are_refused_clearly():
