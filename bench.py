@@ -205,11 +205,14 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="use the multi-GPU (target-range + NCCL all-gather) step even on one rank")
     ap.add_argument("--leaf-capacity", type=int, default=64, help="leaf capacity of the fmm-evals workload")
+    ap.add_argument("--p2p-n", type=int, default=65536, help="bodies of the p2p and fmm-evals workloads")
+    ap.add_argument("--p2p-tpt", type=int, default=0, choices=[0, 2, 4],
+                    help="targets per thread of the P2P kernel (0: chosen by mean leaf size)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the N=1000, N=65536 and ensemble configurations of the default line")
     ap.add_argument("--workload", default="mixed-n1048576",
                     choices=["mixed-n1048576", "ensemble", "fmm-n65536", "fmm-evals", "snapshots-n1048576",
-                             "ics-ensemble512", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
+                             "ics-ensemble512", "p2p", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
                     help="headline (default) or one of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
@@ -598,13 +601,18 @@ def wl_ensemble(gx, torch, args) -> dict:
 
 
 def wl_p2p(gx, torch, args) -> dict:
-    """FMM near field of the N = 65,536 two-disk workload: reference octree leaf lists
-    (leaf_capacity 64, theta 0.6) built on the host, P2P on the device."""
-    n = 65536
-    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, 0.02)
+    """FMM near field of the two-disk workload (N = 65,536 by default, --p2p-n), reference
+    octree leaf lists (--leaf-capacity, default 64; theta 0.6) built on the device, P2P on the
+    device; --p2p-tpt forces the kernel's targets per thread.  Each form is timed over 20
+    launches and checked against the oracle's near loop (the reference's, restated in C)."""
+    n = int(getattr(args, "p2p_n", 65536))
+    cap = int(getattr(args, "leaf_capacity", 64))
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, 0.02)
     t0 = time.perf_counter()
-    lists = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, 64)
+    lists = gx.build_leaf_lists(p.x, p.y, p.z, p.m, 0.02, 0.6, cap, on_device=True)
     build_s = time.perf_counter() - t0
+    tpt = int(getattr(args, "p2p_tpt", 0))
+    gx._ffi.call("gx_debug_p2p_targets_per_thread", tpt)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     dl = gx.LeafLists(T(lists.leaf_offsets), T(lists.leaf_particles), T(lists.near_offsets), T(lists.near_leaves))
     X = {k: T(getattr(p, k)) for k in ("x", "y", "z", "m")}
@@ -614,7 +622,8 @@ def wl_p2p(gx, torch, args) -> dict:
     pairs = lists.n_pairs - n
     out = {"metric": "Ginteractions/s (FMM P2P leaves)", "unit": UNIT, "n": n, "leaves": lists.n_leaves,
            "near_pairs_of_leaves": int(len(lists.near_leaves)), "interactions": int(pairs),
-           "host_leaf_list_build_s": build_s, "config": {"workload": "p2p-n65536", "leaf_capacity": 64, "theta": 0.6}}
+           "leaf_list_build_s": build_s, "targets_per_thread": tpt or "auto",
+           "config": {"workload": f"p2p-n{n}", "leaf_capacity": cap, "theta": 0.6}}
     import oracle
     L = dict(leaf_offsets=lists.leaf_offsets, leaf_particles=lists.leaf_particles,
              near_offsets=lists.near_offsets, near_leaves=lists.near_leaves)
@@ -636,11 +645,28 @@ def wl_p2p(gx, torch, args) -> dict:
         e.record()
         e.synchronize()
         ms = a.elapsed_time(e) / reps
-        out[name] = {"ms": ms, "value": pairs / (ms / 1e3) / 1e9,
+        rate = pairs / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "value": rate,
                      "rel_err_vs_oracle_near_field": {"median": float(np.median(err)), "max": float(err.max()),
                                                       "bit_identical": bool(np.array_equal(got, want))}}
+        if name == "f64":
+            out[name]["fp64_pipe_frac"] = rate * 1e9 * FP64_OPS_PER_P2P_PAIR / fp64_peak_ops(torch)
+        elif name == "mixed":
+            out[name]["fp32_pipe_frac"] = rate * 1e9 * FMA_PIPE_OPS_PER_INTERACTION / fp32_peak_ops(torch)
+    gx._ffi.call("gx_debug_p2p_targets_per_thread", 0)
     out["value"] = out["f64"]["value"]
     return out
+
+
+def fp32_peak_ops(torch) -> float:
+    """FP32 pipe lane-ops/s: SMs x 128 lanes x the maximum SM clock (MEASURED_PEAKS.json)."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    return sms * FP32_LANES_PER_SM * float(measured_peaks().get("sm_max_mhz", 1965.0)) * 1e6
+
+
+def fp64_peak_ops(torch) -> float:
+    """FP64 pipe lane-ops/s: SMs x 64 lanes x the maximum SM clock."""
+    return fp32_peak_ops(torch) / 2.0
 
 
 def wl_direct(gx, torch, args, n, eps, dt, steps, ref_targets: int = 0) -> dict:
@@ -993,12 +1019,13 @@ def wl_fmm(gx, torch, args, e2e: bool = True) -> dict:
 
 
 def wl_fmm_evals(gx, torch, args) -> dict:
-    """FMM force evaluations alone (no KDK step) of the N = 65,536 two-disk system (eps 0.02,
-    theta 0.6, order 4) on device arrays, with --leaf-capacity and --precision (f64 or mixed):
-    --warmup untimed evaluations, then --steps timed ones.  The case the FMM kernel profiles
-    capture (the P2P and M2P launches of one evaluation)."""
-    n, eps = 65536, 0.02
-    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, eps)
+    """FMM force evaluations alone (no KDK step) of the two-disk system (N = 65,536 by default,
+    --p2p-n; eps 0.02, theta 0.6, order 4) on device arrays, with --leaf-capacity and
+    --precision (f64 or mixed): --warmup untimed evaluations, then --steps timed ones, and the
+    device time per phase (tree, moments, lists, far field, near field) of a few more.  The
+    case the FMM kernel profiles capture (the P2P and M2P launches of one evaluation)."""
+    n, eps = int(getattr(args, "p2p_n", 65536)), 0.02
+    p = gx.ics.two_disk_encounter(n // 2, n - n // 2, 20260502, eps)
     prec = gx.PRECISION_MIXED if args.precision == "mixed" else gx.PRECISION_F64
     params, opt = gx.PhysicsParams(1.0, eps), gx.FmmOptions(0.6, args.leaf_capacity, 32, 4)
     D = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("x", "y", "z", "m")}
@@ -1017,9 +1044,15 @@ def wl_fmm_evals(gx, torch, args) -> dict:
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    return {"metric": "FMM evaluations/s (N=65536)", "value": 1e3 / ms, "unit": "evaluations/s", "ms_per_eval": ms,
+    phases = []
+    for _ in range(3):
+        _, ph = gx.fmm.fmm_accelerations_timed(D["x"], D["y"], D["z"], D["m"], *A, params, opt, prec)
+        phases.append(ph)
+    ph = {k: float(np.median([q[k] for q in phases])) for k in gx.fmm.PHASES}
+    return {"metric": f"FMM evaluations/s (N={n})", "value": 1e3 / ms, "unit": "evaluations/s", "ms_per_eval": ms,
             "steps": args.steps, "warmup": args.warmup, "stats": st.__dict__, "dtype": args.precision,
-            "note": "includes the two host synchronisations of each evaluation (list sizes)",
+            "phases_ms": ph,
+            "note": "includes the two host synchronisations of each evaluation (node and list sizes)",
             "config": {"workload": "fmm-evals", "n": n, "leaf_capacity": args.leaf_capacity, "theta": 0.6,
                        "expansion_order": 4, "softening": eps, "precision": args.precision}}
 
@@ -1154,6 +1187,7 @@ OTHER_WORKLOADS = {
     "snapshots-n1048576": wl_snapshots,
     "ics-ensemble512": wl_ics,
     "p2p-n65536": wl_p2p,
+    "p2p": wl_p2p,
     "direct-n65536": lambda gx, torch, args: wl_direct(gx, torch, args, 65536, 0.02, 0.002, 100),
     "direct-n1000": lambda gx, torch, args: wl_direct(gx, torch, args, 1000, 0.05, 0.005, 20),
     "fit-n16384": wl_fit,

@@ -34,7 +34,6 @@ namespace gx {
 namespace {
 
 constexpr int kBboxThreads = 256;
-constexpr int kBuildThreads = 1024;
 constexpr int kWalkThreads = 128;  // 4 warps, one leaf each
 // Shared stack slots per warp: 4 x 1760 x 4 B = 27.5 KiB per block, plus the 1 KiB the
 // runtime reserves per block, puts exactly 8 blocks (32 warps) in an SM's 228 KiB, the
@@ -146,107 +145,134 @@ __device__ __forceinline__ int lower_octant(const uint64_t* keys, int b, int e, 
     return b;
 }
 
-// One CTA builds the whole topology level by level.  Per pass it classifies up to 1024 nodes
-// of the level (one per thread), compacts the ones that split, and gives each splitting node
-// 8 threads: thread c finds where octant c starts in the node's sorted range.
-__global__ void __launch_bounds__(kBuildThreads) tree_build_kernel(const TreeBuildArgs t, const uint64_t* keys) {
-    constexpr int kSplitPerSub = kBuildThreads / 8;
-    __shared__ int s_warp[kBuildThreads / 32];
-    __shared__ int s_split[kBuildThreads];
-    __shared__ int s_bound[kSplitPerSub][9];
-    __shared__ int s_over;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int j = tid >> 3, c = tid & 7;
-    if (tid == 0) {
+// The topology in parallel from the sorted path keys.  A node at depth L is a key prefix of
+// L octants (key >> 3 (kKeyLevels - L)); it splits when it holds more than cap bodies and
+// L < max_depth, and a splitting node's 8 children (all of them, empty ones included) are
+// the nodes of depth L + 1.  Nodes are numbered breadth-first with children in octant order,
+// i.e. level by level in key-prefix order, so a node's number follows from counts alone:
+//   flags[L n + i] = 1 when sorted body i is the first body of a splitting depth-L prefix,
+//   E = exclusive scan of flags over all levels (kKeyLevels n + 1 entries, in place),
+//   S_L = splitting nodes of depth L = E[(L + 1) n] - E[L n],
+//   level_off[L + 1] = level_off[L] + 8 S_(L-1)  (level_off[0] = 0, level_off[1] = 1),
+//   the rank of body i's depth-L prefix among the splitting ones = E[L n + i] - E[L n],
+//   and its children start at level_off[L + 1] + 8 rank.
+// A node's centre is the reference's recurrence (subdivide, fmm_solver.cpp:111-131) walked
+// from the root along its prefix -- the same operations in the same order as building level
+// by level, so the same bits.  A prefix of depth kKeyLevels that would still split needs a
+// deeper key: hdr[2] bit 0 hands the tree to the host builder.
+
+// Position one past the last body of the depth-L prefix that contains sorted body i.
+__device__ __forceinline__ int prefix_end(const uint64_t* keys, int n, int i, int L) {
+    const int sh = 3 * (kKeyLevels - L);
+    const uint64_t p = sh >= 64 ? 0 : keys[i] >> sh;
+    int b = i + 1, e = n;
+    while (b < e) {
+        const int mid = (b + e) >> 1;
+        const uint64_t q = sh >= 64 ? 0 : keys[mid] >> sh;
+        if (q == p) b = mid + 1;
+        else e = mid;
+    }
+    return b;
+}
+
+__device__ __forceinline__ bool prefix_first(const uint64_t* keys, int i, int L) {
+    if (i == 0) return true;
+    const int sh = 3 * (kKeyLevels - L);
+    return sh >= 64 ? false : (keys[i] >> sh) != (keys[i - 1] >> sh);
+}
+
+__global__ void __launch_bounds__(256) split_flags_kernel(const TreeBuildArgs t, const uint64_t* keys, int32_t* flags) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i == 0) flags[(size_t)kKeyLevels * t.n] = 0;
+    if (i >= t.n) return;
+    const int lmax = min(t.max_depth, kKeyLevels + 1);
+    for (int L = 0; L <= kKeyLevels; ++L) {
+        bool split = false;
+        if (L < lmax && prefix_first(keys, i, L) && prefix_end(keys, t.n, i, L) - i > t.cap) {
+            if (L == kKeyLevels) atomicOr(&t.hdr[2], 1);
+            else split = true;
+        }
+        if (L < kKeyLevels) flags[(size_t)L * t.n + i] = split ? 1 : 0;
+    }
+}
+
+// One thread: level offsets, node and level counts from the scanned flags.
+__global__ void tree_levels_kernel(const TreeBuildArgs t, const int32_t* E) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const size_t n = (size_t)t.n;
+    int64_t off = 1;
+    int levels = 1;
+    t.level_off[0] = 0;
+    t.level_off[1] = 1;
+    for (int L = 0; L < kKeyLevels; ++L) {
+        const int64_t s = (int64_t)E[(L + 1) * n] - (int64_t)E[L * n];
+        if (s == 0) break;
+        off += 8 * s;
+        t.level_off[L + 2] = off <= 0x7fffffffLL ? (int32_t)off : 0x7fffffff;
+        ++levels;
+    }
+    t.level_off[levels + 1] = t.level_off[levels];
+    t.hdr[0] = t.level_off[levels];
+    t.hdr[1] = levels;
+    if (off > t.capacity) atomicOr(&t.hdr[2], 2);
+}
+
+// Every node starts as a leaf (child -1); the root's record.
+__global__ void __launch_bounds__(256) tree_init_kernel(const TreeBuildArgs t) {
+    const int nodes = min(t.hdr[0], t.capacity);
+    for (int k = blockIdx.x * 256 + threadIdx.x; k < nodes; k += gridDim.x * 256) t.child[k] = -1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         t.beg[0] = 0;
         t.end[0] = t.n;
         t.cx[0] = t.root[0];
         t.cy[0] = t.root[1];
         t.cz[0] = t.root[2];
         t.hw[0] = t.root[3];
-        t.level_off[0] = 0;
-        t.level_off[1] = 1;
-        s_over = 0;
     }
-    __syncthreads();
-    int lb = 0, le = 1, L = 0;
-    while (lb < le) {
-        int next = le;
-        const int sh = 3 * (kKeyLevels - 1 - L);
-        for (int k0 = lb; k0 < le; k0 += kBuildThreads) {
-            const int k = k0 + tid;
-            int split = 0;
-            if (k < le && t.end[k] - t.beg[k] > t.cap && L < t.max_depth) {
-                if (L >= kKeyLevels) atomicOr(&s_over, 1);
-                else split = 1;
+}
+
+// Per sorted body i and depth L where i starts a splitting prefix: the node's child index
+// and its 8 children's records (body ranges by binary search on the octant at depth L).
+__global__ void __launch_bounds__(256) tree_nodes_kernel(const TreeBuildArgs t, const uint64_t* keys,
+                                                         const int32_t* E) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= t.n || (t.hdr[2] & 2)) return;
+    const size_t n = (size_t)t.n;
+    const int levels = t.hdr[1];
+    const uint64_t key = keys[i];
+    double cx = t.root[0], cy = t.root[1], cz = t.root[2], hw = t.root[3];
+    for (int L = 0; L + 1 < levels; ++L) {
+        if (E[L * n + i + 1] - E[L * n + i]) {
+            int self = 0;
+            if (L > 0) {
+                const int parent_rank = E[(L - 1) * n + i + 1] - E[(L - 1) * n] - 1;
+                const int oct = (int)((key >> (3 * (kKeyLevels - L))) & 7);
+                self = t.level_off[L] + 8 * parent_rank + oct;
             }
-            // block-wide exclusive scan of the split flags
-            int v = split;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int u = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += u;
+            const int c0 = t.level_off[L + 1] + 8 * (E[L * n + i] - E[L * n]);
+            t.child[self] = c0;
+            const int e = prefix_end(keys, t.n, i, L);
+            const int sh = 3 * (kKeyLevels - 1 - L);
+            const double chw = dmul(hw, 0.5);
+            int b = i;
+#pragma unroll 1
+            for (int c = 0; c < 8; ++c) {
+                const int nb = c == 7 ? e : lower_octant(keys, b, e, sh, c + 1);
+                t.beg[c0 + c] = b;
+                t.end[c0 + c] = nb;
+                t.cx[c0 + c] = child_centre(cx, chw, c & 1);
+                t.cy[c0 + c] = child_centre(cy, chw, c & 2);
+                t.cz[c0 + c] = child_centre(cz, chw, c & 4);
+                t.hw[c0 + c] = chw;
+                b = nb;
             }
-            if (lane == 31) s_warp[wid] = v;
-            __syncthreads();
-            if (wid == 0) {
-                int w = s_warp[lane];
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int u = __shfl_up_sync(0xffffffffu, w, o);
-                    if (lane >= o) w += u;
-                }
-                s_warp[lane] = w;
-            }
-            __syncthreads();
-            const int rank = v - split + (wid > 0 ? s_warp[wid - 1] : 0);
-            const int total = s_warp[kBuildThreads / 32 - 1];
-            const bool room = (int64_t)next + 8 * (int64_t)total <= (int64_t)t.capacity;
-            if (k < le && !(split && room)) t.child[k] = -1;
-            if (split && room) s_split[rank] = k;
-            if (!room && tid == 0) atomicOr(&s_over, 2);
-            __syncthreads();
-            if (room) {
-                for (int q0 = 0; q0 < total; q0 += kSplitPerSub) {
-                    const int q = q0 + j;
-                    int node = -1, b = 0, e = 0;
-                    if (q < total) {
-                        node = s_split[q];
-                        b = t.beg[node];
-                        e = t.end[node];
-                        s_bound[j][c] = c == 0 ? b : lower_octant(keys, b, e, sh, c);
-                        if (c == 0) s_bound[j][8] = e;
-                    }
-                    __syncthreads();
-                    if (q < total) {
-                        const int c0 = next + 8 * q;
-                        if (c == 0) t.child[node] = c0;
-                        const double chw = dmul(t.hw[node], 0.5);
-                        t.beg[c0 + c] = s_bound[j][c];
-                        t.end[c0 + c] = s_bound[j][c + 1];
-                        t.child[c0 + c] = -1;
-                        t.cx[c0 + c] = child_centre(t.cx[node], chw, c & 1);
-                        t.cy[c0 + c] = child_centre(t.cy[node], chw, c & 2);
-                        t.cz[c0 + c] = child_centre(t.cz[node], chw, c & 4);
-                        t.hw[c0 + c] = chw;
-                    }
-                    __syncthreads();
-                }
-            }
-            next += 8 * total;
-            __syncthreads();
-            if (s_over) break;
         }
-        if (s_over) break;
-        lb = le;
-        le = next;
-        ++L;
-        if (tid == 0) t.level_off[L + 1] = le;
-    }
-    if (tid == 0) {
-        t.hdr[0] = le;
-        t.hdr[1] = L;
-        t.hdr[2] = s_over;
+        // centre of the depth-(L + 1) node on this body's path
+        const int o = (int)((key >> (3 * (kKeyLevels - 1 - L))) & 7);
+        hw = dmul(hw, 0.5);
+        cx = child_centre(cx, hw, o & 1);
+        cy = child_centre(cy, hw, o & 2);
+        cz = child_centre(cz, hw, o & 4);
     }
 }
 
@@ -636,26 +662,44 @@ size_t scan_bytes(int count) {
 
 }  // namespace
 
+// Temporary storage of launch_tree_build: the radix sort's, then (reusing none of it) the
+// split flags / their scan, kKeyLevels n + 1 ints, and the scan's own storage.
 size_t tree_build_temp_bytes(int32_t n) {
     size_t b = 0;
     cub::DoubleBuffer<uint64_t> k(nullptr, nullptr);
     cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
     cub::DeviceRadixSort::SortPairs(nullptr, b, k, v, n, 0, 3 * kKeyLevels);
-    return b;
+    size_t sb = 0;
+    const int items = kKeyLevels * n + 1;
+    cub::DeviceScan::ExclusiveSum(nullptr, sb, (int32_t*)nullptr, (int32_t*)nullptr, items);
+    const size_t flags = ((size_t)items * sizeof(int32_t) + 255) & ~(size_t)255;
+    return flags + std::max((b + 255) & ~(size_t)255, sb);
 }
 
 cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st) {
+    const int items = kKeyLevels * t.n + 1;
+    const size_t flag_bytes = ((size_t)items * sizeof(int32_t) + 255) & ~(size_t)255;
+    int32_t* flags = (int32_t*)temp;
+    void* work = (char*)temp + flag_bytes;
+    size_t work_bytes = temp_bytes - flag_bytes;
+    cudaError_t e = cudaMemsetAsync(t.hdr, 0, 3 * sizeof(int32_t), st);
+    if (e != cudaSuccess) return e;
     bbox_partial_kernel<<<kBboxBlocks, kBboxThreads, 0, st>>>(t);
     bbox_final_kernel<<<1, kBboxThreads, 0, st>>>(t, kBboxBlocks);
     keys_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cub::DoubleBuffer<uint64_t> k(t.keys, t.keys_alt);
     cub::DoubleBuffer<int32_t> v(t.idx, t.perm);
-    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, k, v, t.n, 0, 3 * kKeyLevels, st);
-    if (e != cudaSuccess) return e;
+    if ((e = cub::DeviceRadixSort::SortPairs(work, work_bytes, k, v, t.n, 0, 3 * kKeyLevels, st)) != cudaSuccess)
+        return e;
     if (v.Current() != t.perm) gather_perm_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(v.Current(), t.perm, t.n);
-    tree_build_kernel<<<1, kBuildThreads, 0, st>>>(t, k.Current());
+    split_flags_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, k.Current(), flags);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    work_bytes = temp_bytes - flag_bytes;
+    if ((e = cub::DeviceScan::ExclusiveSum(work, work_bytes, flags, flags, items, st)) != cudaSuccess) return e;
+    tree_levels_kernel<<<1, 32, 0, st>>>(t, flags);
+    tree_init_kernel<<<148 * 4, 256, 0, st>>>(t);
+    tree_nodes_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, k.Current(), flags);
     return cudaGetLastError();
 }
 

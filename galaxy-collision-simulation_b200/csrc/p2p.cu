@@ -96,6 +96,17 @@ __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exa
     a.plan_need[l] = chunks > 1 ? (int64_t)chunks * nt : 0;
 }
 
+// The leaf of every item: item plan_item_off[l] + k belongs to leaf l (k < plan_cnt[l]).  One
+// thread per leaf writes its own items, so the table costs one pass; the leaf kernel then
+// finds an item's leaf with one load instead of a binary search of dependent loads over the
+// item offsets, which dominated items of small leaves.
+__global__ void __launch_bounds__(256) p2p_item_leaf_kernel(const P2PArgs a) {
+    const int l = blockIdx.x * 256 + threadIdx.x;
+    if (l >= a.n_leaves) return;
+    const int b = a.plan_item_off[l], c = a.plan_cnt[l];
+    for (int k = 0; k < c && b + k < a.plan_item_cap; ++k) a.plan_item_leaf[b + k] = l;
+}
+
 // Slot-ordered copy of the sources: src[k] = (x, y, z, m) of body leaf_part[k], for every
 // leaf slot k, when the slots fit the buffer (cap of them; a CSR that lists a body in
 // several leaves can have more, and the leaf kernel then reads through leaf_part).
@@ -151,14 +162,20 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
         const int item = s_item;
         __syncthreads();
         if (item >= n_items) return;
-        // leaf owning the item: largest l with plan_item_off[l] <= item
-        int lo = 0, hi = a.n_leaves;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (a.plan_item_off[mid] <= item) lo = mid;
-            else hi = mid;
+        // leaf owning the item: one load from the table p2p_item_leaf_kernel filled; items past
+        // the table (possible only with device CSR arrays that repeat bodies) search the offsets
+        int leaf;
+        if (item < a.plan_item_cap) {
+            leaf = a.plan_item_leaf[item];
+        } else {
+            int lo = 0, hi = a.n_leaves;  // largest l with plan_item_off[l] <= item
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (a.plan_item_off[mid] <= item) lo = mid;
+                else hi = mid;
+            }
+            leaf = lo;
         }
-        const int leaf = lo;
         const int chunks = a.plan_chunks[leaf], groups = a.plan_groups[leaf];
         const int local = item - a.plan_item_off[leaf];
         const int chunk = local % chunks, group = local / chunks;
@@ -505,6 +522,12 @@ cudaError_t launch_bs(const P2PArgs& a, int bs, int tpt, int sms, cudaStream_t s
 
 namespace {
 
+// Items of a plan: a leaf of nt targets has at most kMaxChunks chunks x ceil(nt / kMinGroup)
+// groups, so the total is at most kMaxChunks (n / kMinGroup + n_leaves) <= n + 8 n_leaves.
+size_t item_leaf_bytes(int64_t n, int32_t n_leaves) {
+    return ((size_t)kMaxChunks * ((size_t)n / kMinGroup + (size_t)n_leaves + 1) * sizeof(int) + 255) & ~(size_t)255;
+}
+
 size_t plan_scan_temp_bytes(int32_t n_leaves) {
     size_t b1 = 0, b2 = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b1, (const int*)nullptr, (int*)nullptr, n_leaves + 1);
@@ -518,11 +541,12 @@ void p2p_set_targets_per_thread(int tpt) { g_p2p_tpt.store(tpt == 2 || tpt == 4 
 
 size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves) {
     // plan arrays (src, need and scratch offsets int64; chunks, groups, counts, item offsets,
-    // done counters int), the scan's temporary storage, src_ok + ticket, the partial sums (at
-    // most kMaxChunks per leaf slot, leaf slots <= n when leaves are split), and the
-    // slot-ordered sources (32 bytes per body); 256 bytes of alignment per piece.
+    // done counters int), the item -> leaf table, the scan's temporary storage, src_ok +
+    // ticket, the partial sums (at most kMaxChunks per leaf slot, leaf slots <= n when leaves
+    // are split), and the slot-ordered sources (32 bytes per body); 256 bytes of alignment
+    // per piece.
     const size_t nl = (size_t)n_leaves + 1;
-    return nl * (3 * 8 + 5 * 4) + plan_scan_temp_bytes(n_leaves) + 4 * 256 +
+    return nl * (3 * 8 + 5 * 4) + item_leaf_bytes(n, n_leaves) + plan_scan_temp_bytes(n_leaves) + 5 * 256 +
            (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n + (size_t)n * sizeof(double4);
 }
 
@@ -546,6 +570,9 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     a.plan_item_off = (int*)carve(nl * 4);
     a.plan_done = (int*)carve(nl * 4);
     a.plan_n_items = a.plan_item_off + a.n_leaves;
+    align();
+    a.plan_item_leaf = (int*)carve(item_leaf_bytes(n_bodies, a.n_leaves));
+    a.plan_item_cap = (int)std::min<size_t>(item_leaf_bytes(n_bodies, a.n_leaves) / sizeof(int), 0x7fffffff);
     align();
     size_t temp_bytes = plan_scan_temp_bytes(a.n_leaves);
     void* temp = carve(temp_bytes);
@@ -575,6 +602,8 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
         return e;
     if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
         return e;
+    p2p_item_leaf_kernel<<<(a.n_leaves + 255) / 256, 256, 0, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (precision == kF64Exact) return launch_bs<kF64Exact, false>(a, bs, 2, sms, st);
     if (precision == kF64)
         return eps0 ? launch_bs<kF64, true>(a, bs, tpt, sms, st) : launch_bs<kF64, false>(a, bs, tpt, sms, st);

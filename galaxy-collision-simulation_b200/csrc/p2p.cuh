@@ -33,6 +33,8 @@ struct P2PArgs {
     int* plan_item_off;     // exclusive scan of plan_cnt
     int* plan_done;         // items finished per leaf
     int* plan_n_items;      // = plan_item_off + n_leaves
+    int* plan_item_leaf;    // leaf of each item (the first plan_item_cap items)
+    int plan_item_cap;
     int* ticket;
     // (x, y, z, m) of leaf_part[k] at slot k, gathered once per launch when the leaf slots
     // fit the buffer (src_ok); sources are then read by slot, without the leaf_part hop
