@@ -168,14 +168,19 @@ def cpu_reference_rate(p, eps, seconds: float = 10.0, threads: int | None = None
 # ---------------------------------------------------------------------------------------
 # DRAM traffic of the timed force launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)
 # ---------------------------------------------------------------------------------------
-# Measured per body on one launch of force_mixed_tp_kernel<256,6,512> at source split 8 with
-# the closing kick fused (the headline variant and split), captured at N = 262,144 with L2
-# flushed before the launch, and scaled to N by the bodies per launch: the launch's traffic
-# is per-body work (positions and masses read once, accelerations written, velocities read
-# and written); the partial sums of the split are consumed from L2 by the tile's last CTA.
-# None until a capture of the current kernel is recorded here.
-TRAFFIC_BYTES_PER_BODY = None
-TRAFFIC_CAPTURE = None
+# Measured per body on two launches of force_mixed_tp_kernel<256,6,512> at source split 8
+# with the closing kick fused (the headline variant and split; ncu flushes L2 before each
+# launch), captured at N = 262,144:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:force_mixed_tp -s 1 -c 2
+#       python bench.py --quick --n 262144 --variant 0 --jsplit 8 --steps 2 --warmup 2 --no-configs
+# read 15.22 / 15.46 MB, written 9.97 / 7.94 MB per launch = 92.7 B/body on average, scaled to
+# N by the bodies per launch (the launch's traffic is per-body work: positions and masses
+# read once, accelerations written, velocities read and written).  The split's partial sums
+# (8 x 24 B/body) do not reach DRAM: the tile's last CTA consumes them from L2.
+TRAFFIC_BYTES_PER_BODY = 92.7
+TRAFFIC_CAPTURE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, force_mixed_tp_kernel<256,6,512> split 8 "
+                   "with the closing kick, 2 launches at N=262144, 92.7 B/body, scaled to N")
 # Algorithmic bytes per body of one force launch with the closing kick: x, y, z, m read
 # (32 B), a written (24 B), v read and written (48 B).
 ALGORITHMIC_BYTES_PER_BODY = 104

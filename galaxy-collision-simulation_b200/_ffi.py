@@ -181,6 +181,7 @@ _SIGNATURES = {
     "gx_debug_fail_allocations": [c_int],
     "gx_debug_stall_barrier": [I64],
     "gx_debug_p2p_targets_per_thread": [c_int],
+    "gx_debug_small_targets_per_warp": [c_int],
 }
 _RESTYPES = {"gx_last_error": c_char_p, "gx_galaxies_body_count": c_int64}
 

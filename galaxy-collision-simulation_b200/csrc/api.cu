@@ -521,6 +521,13 @@ extern "C" int gx_debug_p2p_targets_per_thread(int tpt) {
     return GX_OK;
 }
 
+extern "C" int gx_debug_small_targets_per_warp(int tpw) {
+    if (tpw != 0 && tpw != 1 && tpw != 2 && tpw != 4)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_debug_small_targets_per_warp: 0, 1, 2 or 4");
+    small_set_targets_per_warp(tpw);
+    return GX_OK;
+}
+
 extern "C" int gx_debug_stall_barrier(int64_t step) {
     g_stall_step.store(step < 0 ? -1 : step);
     return GX_OK;
@@ -1652,7 +1659,7 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
     GX_TRY(dev_array(hs, n, &t.perm));
     GX_TRY(dev_array(hs, kKeyLevels + 3, &t.level_off));
     GX_TRY(dev_array(hs, 3, &t.hdr));
-    const size_t sort_bytes = tree_build_temp_bytes(t.n);
+    const size_t sort_bytes = tree_build_temp_bytes(t.n, cap);
     void* sort_temp;
     GX_TRY(dev_array(hs, (int64_t)sort_bytes, (char**)&sort_temp));
     // node slots: 1 + 8 per split node; at most n / (cap + 1) nodes split per level

@@ -161,34 +161,50 @@ __device__ __forceinline__ int lower_octant(const uint64_t* keys, int b, int e, 
 // by level, so the same bits.  A prefix of depth kKeyLevels that would still split needs a
 // deeper key: hdr[2] bit 0 hands the tree to the host builder.
 
-// Position one past the last body of the depth-L prefix that contains sorted body i.
-__device__ __forceinline__ int prefix_end(const uint64_t* keys, int n, int i, int L) {
+__device__ __forceinline__ uint64_t key_prefix(uint64_t key, int L) {
     const int sh = 3 * (kKeyLevels - L);
-    const uint64_t p = sh >= 64 ? 0 : keys[i] >> sh;
-    int b = i + 1, e = n;
-    while (b < e) {
-        const int mid = (b + e) >> 1;
-        const uint64_t q = sh >= 64 ? 0 : keys[mid] >> sh;
-        if (q == p) b = mid + 1;
-        else e = mid;
+    return sh >= 64 ? 0 : key >> sh;
+}
+
+// Position one past the last body of the depth-L prefix that starts at sorted body i:
+// galloping from i, then a binary search in the last gap (log of the prefix's size).
+__device__ __forceinline__ int prefix_end(const uint64_t* keys, int n, int i, int L) {
+    const uint64_t p = key_prefix(keys[i], L);
+    int lo = i + 1, step = 1;  // keys[lo - 1] has prefix p
+    while (lo < n && key_prefix(keys[lo], L) == p) {
+        const int nxt = lo + step;
+        if (nxt >= n || key_prefix(keys[nxt], L) != p) {
+            int b = lo + 1, e = min(nxt, n);  // first mismatch in (lo, nxt]
+            while (b < e) {
+                const int mid = (b + e) >> 1;
+                if (key_prefix(keys[mid], L) == p) b = mid + 1;
+                else e = mid;
+            }
+            return b;
+        }
+        lo = nxt + 1;
+        step <<= 1;
     }
-    return b;
+    return lo;
 }
 
 __device__ __forceinline__ bool prefix_first(const uint64_t* keys, int i, int L) {
-    if (i == 0) return true;
-    const int sh = 3 * (kKeyLevels - L);
-    return sh >= 64 ? false : (keys[i] >> sh) != (keys[i - 1] >> sh);
+    return i == 0 || key_prefix(keys[i], L) != key_prefix(keys[i - 1], L);
 }
 
+// flags[L n + i] = 1 when sorted body i starts a depth-L prefix holding more than cap bodies
+// (it does exactly when body i + cap shares the prefix: the keys are sorted) and L < max_depth.
 __global__ void __launch_bounds__(256) split_flags_kernel(const TreeBuildArgs t, const uint64_t* keys, int32_t* flags) {
     const int i = blockIdx.x * 256 + threadIdx.x;
     if (i == 0) flags[(size_t)kKeyLevels * t.n] = 0;
     if (i >= t.n) return;
     const int lmax = min(t.max_depth, kKeyLevels + 1);
+    const uint64_t key = keys[i];
+    const bool big = (int64_t)i + t.cap < (int64_t)t.n;
+    const uint64_t far = big ? keys[i + t.cap] : 0;
     for (int L = 0; L <= kKeyLevels; ++L) {
         bool split = false;
-        if (L < lmax && prefix_first(keys, i, L) && prefix_end(keys, t.n, i, L) - i > t.cap) {
+        if (L < lmax && big && prefix_first(keys, i, L) && key_prefix(far, L) == key_prefix(key, L)) {
             if (L == kKeyLevels) atomicOr(&t.hdr[2], 1);
             else split = true;
         }
@@ -217,6 +233,18 @@ __global__ void tree_levels_kernel(const TreeBuildArgs t, const int32_t* E) {
     if (off > t.capacity) atomicOr(&t.hdr[2], 2);
 }
 
+// The splitting nodes in global (level, key) order: split_pos[E[L n + i]] = L n + i.
+__global__ void __launch_bounds__(256) split_list_kernel(const TreeBuildArgs t, const int32_t* E, int32_t* split_pos,
+                                                         int split_cap) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= t.n) return;
+    const size_t n = (size_t)t.n;
+    for (int L = 0; L < kKeyLevels; ++L) {
+        const int32_t e0 = E[L * n + i];
+        if (E[L * n + i + 1] != e0 && e0 < split_cap) split_pos[e0] = L * t.n + i;
+    }
+}
+
 // Every node starts as a leaf (child -1); the root's record.
 __global__ void __launch_bounds__(256) tree_init_kernel(const TreeBuildArgs t) {
     const int nodes = min(t.hdr[0], t.capacity);
@@ -231,48 +259,45 @@ __global__ void __launch_bounds__(256) tree_init_kernel(const TreeBuildArgs t) {
     }
 }
 
-// Per sorted body i and depth L where i starts a splitting prefix: the node's child index
-// and its 8 children's records (body ranges by binary search on the octant at depth L).
-__global__ void __launch_bounds__(256) tree_nodes_kernel(const TreeBuildArgs t, const uint64_t* keys,
-                                                         const int32_t* E) {
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    if (i >= t.n || (t.hdr[2] & 2)) return;
+// One thread per (splitting node, child octant c): the node's child index (c == 0) and child
+// c's record -- its body range by binary search on the octant at depth L inside the node's
+// range, its centre by the reference's recurrence walked from the root along the path.
+__global__ void __launch_bounds__(256) tree_children_kernel(const TreeBuildArgs t, const uint64_t* keys,
+                                                            const int32_t* E, const int32_t* split_pos, int split_cap) {
+    if (t.hdr[2] & 2) return;
     const size_t n = (size_t)t.n;
-    const int levels = t.hdr[1];
-    const uint64_t key = keys[i];
-    double cx = t.root[0], cy = t.root[1], cz = t.root[2], hw = t.root[3];
-    for (int L = 0; L + 1 < levels; ++L) {
-        if (E[L * n + i + 1] - E[L * n + i]) {
-            int self = 0;
-            if (L > 0) {
-                const int parent_rank = E[(L - 1) * n + i + 1] - E[(L - 1) * n] - 1;
-                const int oct = (int)((key >> (3 * (kKeyLevels - L))) & 7);
-                self = t.level_off[L] + 8 * parent_rank + oct;
-            }
-            const int c0 = t.level_off[L + 1] + 8 * (E[L * n + i] - E[L * n]);
-            t.child[self] = c0;
-            const int e = prefix_end(keys, t.n, i, L);
-            const int sh = 3 * (kKeyLevels - 1 - L);
-            const double chw = dmul(hw, 0.5);
-            int b = i;
-#pragma unroll 1
-            for (int c = 0; c < 8; ++c) {
-                const int nb = c == 7 ? e : lower_octant(keys, b, e, sh, c + 1);
-                t.beg[c0 + c] = b;
-                t.end[c0 + c] = nb;
-                t.cx[c0 + c] = child_centre(cx, chw, c & 1);
-                t.cy[c0 + c] = child_centre(cy, chw, c & 2);
-                t.cz[c0 + c] = child_centre(cz, chw, c & 4);
-                t.hw[c0 + c] = chw;
-                b = nb;
-            }
+    const int total = min(E[kKeyLevels * n], split_cap);
+    for (int q = blockIdx.x * 256 + threadIdx.x; q < 8 * total; q += gridDim.x * 256) {
+        const int sidx = q >> 3, c = q & 7;
+        const int pos = split_pos[sidx];
+        const int L = pos / t.n, i = pos - L * t.n;
+        const uint64_t key = keys[i];
+        int self = 0;
+        if (L > 0) {
+            const int parent_rank = E[(L - 1) * n + i + 1] - E[(L - 1) * n] - 1;
+            self = t.level_off[L] + 8 * parent_rank + (int)((key >> (3 * (kKeyLevels - L))) & 7);
         }
-        // centre of the depth-(L + 1) node on this body's path
-        const int o = (int)((key >> (3 * (kKeyLevels - 1 - L))) & 7);
-        hw = dmul(hw, 0.5);
-        cx = child_centre(cx, hw, o & 1);
-        cy = child_centre(cy, hw, o & 2);
-        cz = child_centre(cz, hw, o & 4);
+        const int c0 = t.level_off[L + 1] + 8 * (sidx - E[L * n]);
+        if (c == 0) t.child[self] = c0;
+        const int e = prefix_end(keys, t.n, i, L);
+        const int sh = 3 * (kKeyLevels - 1 - L);
+        const int cb = c == 0 ? i : lower_octant(keys, i, e, sh, c);
+        const int ce = c == 7 ? e : lower_octant(keys, cb, e, sh, c + 1);
+        double cx = t.root[0], cy = t.root[1], cz = t.root[2], hw = t.root[3];
+        for (int d = 0; d < L; ++d) {
+            const int o = (int)((key >> (3 * (kKeyLevels - 1 - d))) & 7);
+            hw = dmul(hw, 0.5);
+            cx = child_centre(cx, hw, o & 1);
+            cy = child_centre(cy, hw, o & 2);
+            cz = child_centre(cz, hw, o & 4);
+        }
+        const double chw = dmul(hw, 0.5);
+        t.beg[c0 + c] = cb;
+        t.end[c0 + c] = ce;
+        t.cx[c0 + c] = child_centre(cx, chw, c & 1);
+        t.cy[c0 + c] = child_centre(cy, chw, c & 2);
+        t.cz[c0 + c] = child_centre(cz, chw, c & 4);
+        t.hw[c0 + c] = chw;
     }
 }
 
@@ -662,9 +687,18 @@ size_t scan_bytes(int count) {
 
 }  // namespace
 
-// Temporary storage of launch_tree_build: the radix sort's, then (reusing none of it) the
-// split flags / their scan, kKeyLevels n + 1 ints, and the scan's own storage.
-size_t tree_build_temp_bytes(int32_t n) {
+// Temporary storage of launch_tree_build: the split flags / their scan (kKeyLevels n + 1 ints),
+// the list of splitting nodes (at most kKeyLevels (n / (cap + 1) + 1): the depth-L prefixes that
+// split hold more than cap bodies each and are disjoint), then the radix sort's or the scan's
+// own storage (one after the other, sharing the space).
+namespace {
+int split_capacity(int32_t n, int64_t cap) {
+    const int64_t c = (int64_t)kKeyLevels * ((int64_t)n / (std::max<int64_t>(cap, 0) + 1) + 1);
+    return (int)std::min<int64_t>(c, 0x7fffffff);
+}
+}  // namespace
+
+size_t tree_build_temp_bytes(int32_t n, int64_t cap) {
     size_t b = 0;
     cub::DoubleBuffer<uint64_t> k(nullptr, nullptr);
     cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
@@ -673,15 +707,19 @@ size_t tree_build_temp_bytes(int32_t n) {
     const int items = kKeyLevels * n + 1;
     cub::DeviceScan::ExclusiveSum(nullptr, sb, (int32_t*)nullptr, (int32_t*)nullptr, items);
     const size_t flags = ((size_t)items * sizeof(int32_t) + 255) & ~(size_t)255;
-    return flags + std::max((b + 255) & ~(size_t)255, sb);
+    const size_t splits = ((size_t)split_capacity(n, cap) * sizeof(int32_t) + 255) & ~(size_t)255;
+    return flags + splits + std::max((b + 255) & ~(size_t)255, sb);
 }
 
 cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st) {
     const int items = kKeyLevels * t.n + 1;
     const size_t flag_bytes = ((size_t)items * sizeof(int32_t) + 255) & ~(size_t)255;
+    const int split_cap = split_capacity(t.n, t.cap);
+    const size_t split_bytes = ((size_t)split_cap * sizeof(int32_t) + 255) & ~(size_t)255;
     int32_t* flags = (int32_t*)temp;
-    void* work = (char*)temp + flag_bytes;
-    size_t work_bytes = temp_bytes - flag_bytes;
+    int32_t* split_pos = (int32_t*)((char*)temp + flag_bytes);
+    void* work = (char*)temp + flag_bytes + split_bytes;
+    size_t work_bytes = temp_bytes - flag_bytes - split_bytes;
     cudaError_t e = cudaMemsetAsync(t.hdr, 0, 3 * sizeof(int32_t), st);
     if (e != cudaSuccess) return e;
     bbox_partial_kernel<<<kBboxBlocks, kBboxThreads, 0, st>>>(t);
@@ -695,11 +733,12 @@ cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_by
     if (v.Current() != t.perm) gather_perm_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(v.Current(), t.perm, t.n);
     split_flags_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, k.Current(), flags);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    work_bytes = temp_bytes - flag_bytes;
+    work_bytes = temp_bytes - flag_bytes - split_bytes;
     if ((e = cub::DeviceScan::ExclusiveSum(work, work_bytes, flags, flags, items, st)) != cudaSuccess) return e;
     tree_levels_kernel<<<1, 32, 0, st>>>(t, flags);
+    split_list_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, flags, split_pos, split_cap);
     tree_init_kernel<<<148 * 4, 256, 0, st>>>(t);
-    tree_nodes_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, k.Current(), flags);
+    tree_children_kernel<<<148 * 8, 256, 0, st>>>(t, k.Current(), flags, split_pos, split_cap);
     return cudaGetLastError();
 }
 

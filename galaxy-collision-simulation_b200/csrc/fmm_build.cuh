@@ -38,7 +38,7 @@ struct TreeBuildArgs {
     int32_t* level_off;  // kKeyLevels + 3
     int32_t* hdr;        // 3
 };
-size_t tree_build_temp_bytes(int32_t n);
+size_t tree_build_temp_bytes(int32_t n, int64_t cap);
 cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st);
 // After a successful build: bodies of every leaf in ascending index order in t.perm
 // (uses t.idx as scratch).

@@ -44,8 +44,7 @@ constexpr int kMinChunk = 256;   // ... of at least this many sources
 constexpr int kMinGroup = 8;     // targets of a group, when a leaf's targets are split
 constexpr int kStageCost = 8;    // staging one source costs about this many interactions
 constexpr int kWarpBlockMaxMean = 12;  // mean bodies per leaf up to which blocks are one warp
-constexpr int kFourTargetsMinMean = 24;  // mean bodies per leaf from which threads take four targets
-std::atomic<int> g_p2p_tpt{0};          // 0: by the mean leaf size; 2 or 4: forced (measurement)
+std::atomic<int> g_p2p_tpt{0};          // 0: the default shape; 2 or 4: forced (measurement)
 
 // Per leaf (one warp each): number of sources, and the split of the leaf into target groups
 // x source chunks of cost at most about item_cost each, where an item of g targets and s
@@ -587,10 +586,11 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     // independent warps per SM, no block-wide barriers) hide the latency of its gathers;
     // larger leaves keep 4-warp blocks that share each staged source among more threads.
     const int bs = n_bodies <= (int64_t)kWarpBlockMaxMean * a.n_leaves ? 32 : 128;
-    // Targets per thread: four (two packed pairs per staged source in the mixed form, four
-    // independent FP64 chains) once the mean leaf fills rows of four; two below that.
+    // Targets per thread: two.  Four (two packed pairs per staged source in the mixed form,
+    // four FP64 chains per thread) measured 3-40% slower at every size and leaf capacity
+    // tried (N = 65,536 and 2^20, leaf 16 and 64); the shape stays selectable for measurement.
     const int forced = g_p2p_tpt.load();
-    const int tpt = forced ? forced : (n_bodies >= (int64_t)kFourTargetsMinMean * a.n_leaves ? 4 : 2);
+    const int tpt = forced ? forced : 2;
     const int64_t item_cost = (int64_t)1024 * bs;
     cudaError_t e = cudaMemsetAsync(a.plan_done, 0, nl * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(int), st);

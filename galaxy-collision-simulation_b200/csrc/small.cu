@@ -32,6 +32,8 @@
 #include "precision.cuh"
 #include "small.cuh"
 
+#include <atomic>
+
 namespace gx {
 namespace {
 
@@ -39,6 +41,7 @@ constexpr int kSmallThreads = 256;
 constexpr int kSmallWarps = kSmallThreads / 32;
 constexpr int kSmallJT = 512;  // sources staged per shared-memory pass
 constexpr size_t kSmallHeader = 256;  // barrier words + status, then the position buffers
+std::atomic<int> g_small_tpw{0};      // 0: chosen from n; 1, 2 or 4: forced (measurement)
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -149,6 +152,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
             }
             __syncthreads();
             if constexpr (PREC == kF64) {
+#pragma unroll 4
                 for (int jj = lane; jj < cnt; jj += 32) {
                     const double qx = sx[jj], qy = sy[jj], qz = sz[jj], qm = sm[jj];
 #pragma unroll
@@ -243,6 +247,8 @@ const void* pick(int tpw) {
 
 }  // namespace
 
+void small_set_targets_per_warp(int tpw) { g_small_tpw.store(tpw == 1 || tpw == 2 || tpw == 4 ? tpw : 0); }
+
 size_t small_scratch_bytes(int n) { return kSmallHeader + (size_t)6 * (size_t)n * sizeof(double); }
 
 void small_bind_scratch(SmallArgs& a, void* scratch) {
@@ -259,9 +265,14 @@ cudaError_t small_steps_launch(const SmallArgs& a, int precision, bool eps0, int
     if (e != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
     if (!coop) return cudaErrorNotSupported;
-    // the fewest targets per warp that let one CTA per SM cover every body
-    int tpw = 1;
-    while (tpw < 4 && (int64_t)sms * kSmallWarps * tpw < a.n) tpw *= 2;
+    // Targets per warp: the fewest that fit the bodies in at most half the SMs' worth of CTAs
+    // (each CTA is one arrival at every grid barrier; more targets per warp also give each
+    // lane independent chains), up to four; at most one CTA per SM either way.
+    int tpw = g_small_tpw.load();
+    if (tpw == 0) {
+        tpw = 1;
+        while (tpw < 4 && (int64_t)(sms / 2) * kSmallWarps * tpw < a.n) tpw *= 2;
+    }
     if ((int64_t)sms * kSmallWarps * tpw < a.n) return cudaErrorNotSupported;
     const int blocks = (a.n + kSmallWarps * tpw - 1) / (kSmallWarps * tpw);
     const void* fn = precision == kF64Exact ? pick<kF64Exact, true>(tpw)

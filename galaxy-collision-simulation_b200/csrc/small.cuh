@@ -22,6 +22,8 @@ struct SmallArgs {
     int64_t stall_step;             // test hook: CTA 0 leaves before this step's barrier (-1: never)
 };
 
+// Targets per warp: 1, 2 or 4 forces that many, 0 restores the choice from n (measurements).
+void small_set_targets_per_warp(int tpw);
 // Device bytes of the scratch a launch needs (position buffers, barrier, status); the barrier
 // and status words sit at the start and must be zero before each launch.
 size_t small_scratch_bytes(int n);

@@ -424,10 +424,13 @@ int gx_debug_fail_allocations(int count);
  * and the barrier waits are cut to 0.2 s, so the other CTAs give up, the launch ends early
  * and the next synchronising session call returns GX_ERR_TIMEOUT.  Nothing faults. */
 int gx_debug_stall_barrier(int64_t step);
-/* Targets per thread of the FP64 and mixed P2P kernels: 2 or 4 forces that shape, 0 (the
- * default) picks it from the mean leaf size.  For measurements; results agree within the
- * forms' tolerances either way. */
+/* Targets per thread of the FP64 and mixed P2P kernels: 2 or 4 forces that shape, 0 restores
+ * the default (2).  For measurements; results agree within the forms' tolerances either way. */
 int gx_debug_p2p_targets_per_thread(int tpt);
+/* Targets per warp of the single-launch step loop: 1, 2 or 4 forces that shape, 0 (default)
+ * picks it from n.  For measurements; results agree within the forms' tolerances (the exact
+ * form stays bit-identical) either way. */
+int gx_debug_small_targets_per_warp(int tpw);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -17,10 +17,11 @@ pytestmark = pytest.mark.gpu
 
 F64, MIX = gx.PRECISION_F64, gx.PRECISION_MIXED
 DEV = "cuda"
-# Mixed-precision bounds, measured on B200 (figures in the test bodies' comments).
-MIXED_VJP_MAX = 1e-3        # position VJP, max relative error per body vs the oracle
-MIXED_VJP_MASS_MAX = 1e-3   # mass VJP, max relative error per body vs the oracle
-MIXED_ORBIT_GRAD_TOL = 1e-3  # mixed orbit gradient vs FP64 central differences, relative to max |g|
+# Mixed-precision bounds, about 4x the figures measured on B200 for these inputs:
+MIXED_VJP_MAX = 2e-4         # position VJP, max relative error per body vs the oracle (measured 4.9e-5)
+MIXED_VJP_MASS_MAX = 1e-3    # mass VJP, max relative error per body vs the oracle (measured 1.7e-4)
+MIXED_ORBIT_GRAD_TOL = 2e-9  # mixed orbit gradient vs FP64 central differences, relative to
+                             # max |g| (measured 4.0e-10, the level of the differences' own error)
 
 
 def torch_accel(x, m, eps):

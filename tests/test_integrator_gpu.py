@@ -84,6 +84,7 @@ def test_graph_replay_equals_eager(prec):
     out = []
     for timing in (False, True):
         with gx.Session(len(p), params) as s:
+            s.set_persistent(False)  # graph replay vs eager launches of the same kernels
             s.set_particles(p)
             s.compute_accelerations(prec)
             s.enable_timing(timing)
