@@ -587,7 +587,7 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     // larger leaves keep 4-warp blocks that share each staged source among more threads.
     const int bs = n_bodies <= (int64_t)kWarpBlockMaxMean * a.n_leaves ? 32 : 128;
     // Targets per thread: two.  Four (two packed pairs per staged source in the mixed form,
-    // four FP64 chains per thread) measured 3-40% slower at every size and leaf capacity
+    // four FP64 chains per thread) measured 2-40% slower at every size and leaf capacity
     // tried (N = 65,536 and 2^20, leaf 16 and 64); the shape stays selectable for measurement.
     const int forced = g_p2p_tpt.load();
     const int tpt = forced ? forced : 2;
