@@ -18,9 +18,9 @@
 //     lanes of a warp split the sources (lane l takes j = l mod 32) and a butterfly of
 //     shuffles adds the 32 partial sums (every lane ends with the same bits);
 //   * kF64Exact -- the reference's operation order (direct_solver.cpp:8-23, 59-83): lane l
-//     computes the contribution of source j0 + l, and the warp adds the 32 contributions
-//     in ascending j order into one running sum per component, so each target is summed
-//     exactly as compute_direct_accelerations_for_targets sums it.  The skipped self pair
+//     computes the contribution of source j0 + l into shared memory, and lane c (c < 3)
+//     adds component c of the 32 contributions in ascending j order into one running sum,
+//     so each target is summed exactly as compute_direct_accelerations_for_targets sums it.  The skipped self pair
 //     and the s2 == 0 pair add +0.0, which leaves the running sum unchanged: it starts at
 //     +0.0 and, in round-to-nearest, a sum is -0.0 only when both addends are -0.0.
 // The grid barrier is an arrival counter and a generation word in global memory; a CTA
@@ -59,10 +59,10 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 // `gen` (thread 0 only) is the generation this CTA waits to see pass.
 __device__ bool grid_barrier(const SmallArgs& a, unsigned& gen) {
     __shared__ int s_ok;
-    __threadfence();  // every thread's position stores before the CTA's arrival
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
+        __threadfence();  // after the CTA barrier: the CTA's position stores before its arrival
         const unsigned arrived = atomicAdd(&a.bar[0], 1u);
         if (arrived == gridDim.x - 1) {
             atomicExch(&a.bar[0], 0u);  // reset before anyone can pass
@@ -97,6 +97,9 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
     __shared__ __align__(16) double sy[kSmallJT];
     __shared__ __align__(16) double sz[kSmallJT];
     __shared__ __align__(16) double sm[kSmallJT];
+    // exact form: each warp's 32 contributions (3 doubles each) per owned target
+    __shared__ double s_con_all[PREC == kF64Exact ? kSmallWarps * TPW * 96 : 1];
+    double* const s_con = s_con_all + (PREC == kF64Exact ? (threadIdx.x >> 5) * TPW * 96 : 0);
     const int lane = threadIdx.x & 31;
     const int n = a.n;
     const int total_warps = gridDim.x * kSmallWarps;
@@ -171,14 +174,16 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
                     }
                 }
             } else {
+                // lane l computes the contribution of source jb + l for each owned target into
+                // the warp's shared slots; then lane c (c < 3) adds component c of the 32
+                // contributions in ascending j, one running sum per target (fx holds it)
                 for (int jb = 0; jb < cnt; jb += 32) {
                     const int jj = jb + lane;
                     const int lim = min(32, cnt - jb);
 #pragma unroll
                     for (int k = 0; k < TPW; ++k) {
-                        if (T[k] >= n) continue;
                         double cx = 0.0, cy = 0.0, cz = 0.0;
-                        if (jj < cnt && j0 + jj != T[k]) {
+                        if (T[k] < n && jj < cnt && j0 + jj != T[k]) {
                             const double rx = dsub(sx[jj], X[k]), ry = dsub(sy[jj], Y[k]), rz = dsub(sz[jj], Z[k]);
                             const double s2 = dadd(dadd(dadd(dmul(rx, rx), dmul(ry, ry)), dmul(rz, rz)), e2);
                             if (s2 != 0.0) {
@@ -190,12 +195,19 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
                                 cz = dmul(rz, scale);
                             }
                         }
-                        for (int q = 0; q < lim; ++q) {  // ascending j, one running sum per component
-                            fx[k] = dadd(fx[k], __shfl_sync(0xffffffffu, cx, q));
-                            fy[k] = dadd(fy[k], __shfl_sync(0xffffffffu, cy, q));
-                            fz[k] = dadd(fz[k], __shfl_sync(0xffffffffu, cz, q));
+                        double* slot = s_con + (k * 32 + lane) * 3;
+                        slot[0] = cx;
+                        slot[1] = cy;
+                        slot[2] = cz;
+                    }
+                    __syncwarp();
+                    if (lane < 3) {
+                        for (int q = 0; q < lim; ++q) {
+#pragma unroll
+                            for (int k = 0; k < TPW; ++k) fx[k] = dadd(fx[k], s_con[(k * 32 + q) * 3 + lane]);
                         }
                     }
+                    __syncwarp();
                 }
             }
             __syncthreads();
@@ -213,10 +225,10 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
                 AX[k] = G * fx[k];
                 AY[k] = G * fy[k];
                 AZ[k] = G * fz[k];
-            } else {
-                AX[k] = fx[k];
-                AY[k] = fy[k];
-                AZ[k] = fz[k];
+            } else {  // lane c holds component c
+                AX[k] = __shfl_sync(0xffffffffu, fx[k], 0);
+                AY[k] = __shfl_sync(0xffffffffu, fx[k], 1);
+                AZ[k] = __shfl_sync(0xffffffffu, fx[k], 2);
             }
             if (T[k] >= n) continue;
             U[k] = dadd(U[k], dmul(AX[k], h));
@@ -265,13 +277,12 @@ cudaError_t small_steps_launch(const SmallArgs& a, int precision, bool eps0, int
     if (e != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
     if (!coop) return cudaErrorNotSupported;
-    // Targets per warp: the fewest that fit the bodies in at most half the SMs' worth of CTAs
-    // (each CTA is one arrival at every grid barrier; more targets per warp also give each
-    // lane independent chains), up to four; at most one CTA per SM either way.
+    // Targets per warp: the fewest that let one CTA per SM cover every body (measured on B200
+    // at n = 1000: one target per warp on 125 SMs 1.4x faster than two on 63, 2.1x than four).
     int tpw = g_small_tpw.load();
     if (tpw == 0) {
         tpw = 1;
-        while (tpw < 4 && (int64_t)(sms / 2) * kSmallWarps * tpw < a.n) tpw *= 2;
+        while (tpw < 4 && (int64_t)sms * kSmallWarps * tpw < a.n) tpw *= 2;
     }
     if ((int64_t)sms * kSmallWarps * tpw < a.n) return cudaErrorNotSupported;
     const int blocks = (a.n + kSmallWarps * tpw - 1) / (kSmallWarps * tpw);
