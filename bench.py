@@ -168,28 +168,37 @@ def cpu_reference_rate(p, eps, seconds: float = 10.0, threads: int | None = None
 # ---------------------------------------------------------------------------------------
 # DRAM traffic of the timed force launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)
 # ---------------------------------------------------------------------------------------
-# Measured per body on two launches of force_mixed_tp_kernel<256,6,512> at source split 8
-# with the closing kick fused (the headline variant and split; ncu flushes L2 before each
-# launch), captured at N = 262,144:
+# Measured per body on two launches of each candidate headline variant at source split 8 with
+# the closing kick fused (ncu flushes L2 before each launch), captured at N = 262,144:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:force_mixed_tp -s 1 -c 2
-#       python bench.py --quick --n 262144 --variant 0 --jsplit 8 --steps 2 --warmup 2 --no-configs
-# read 15.22 / 15.46 MB, written 9.97 / 7.94 MB per launch = 92.7 B/body on average, scaled to
-# N by the bodies per launch (the launch's traffic is per-body work: positions and masses
-# read once, accelerations written, velocities read and written).  The split's partial sums
-# (8 x 24 B/body) do not reach DRAM: the tile's last CTA consumes them from L2.
-TRAFFIC_BYTES_PER_BODY = 92.7
-TRAFFIC_CAPTURE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, force_mixed_tp_kernel<256,6,512> split 8 "
-                   "with the closing kick, 2 launches at N=262144, 92.7 B/body, scaled to N")
+#       python bench.py --quick --n 262144 --variant V --jsplit 8 --steps 2 --warmup 2 --no-configs
+#   V = 0, force_mixed_tp_kernel<256,6,512>: read 15.22 / 15.46 MB, written 9.97 / 7.94 MB
+#   V = 2, force_mixed_tp_kernel<128,6,512>: read 15.27 / 15.46 MB, written 9.76 / 7.06 MB
+# per launch: 92.7 and 90.7 B/body on average, scaled to N by the bodies per launch (the
+# launch's traffic is per-body work: positions and masses read once, accelerations written,
+# velocities read and written).  The split's partial sums (8 x 24 B/body) do not reach DRAM:
+# the tile's last CTA consumes them from L2.  Keyed by the kernel the bench ran (the autotuner
+# picks either; they are within 0.1% of each other at N = 2^20).
+TRAFFIC_BYTES_PER_BODY = {"mixed block=256 ipt=6 jt=512 f32x2-targets": 92.7,
+                          "mixed block=128 ipt=6 jt=512 f32x2-targets": 90.7}
+
+
+def traffic_capture(kernel: str):
+    return None if kernel not in TRAFFIC_BYTES_PER_BODY else (
+        f"ncu dram__bytes_read.sum + dram__bytes_write.sum of {kernel} at split 8 with the closing kick, "
+        f"2 launches at N=262144: {TRAFFIC_BYTES_PER_BODY[kernel]} B/body, scaled to N")
+
+
 # Algorithmic bytes per body of one force launch with the closing kick: x, y, z, m read
 # (32 B), a written (24 B), v read and written (48 B).
 ALGORITHMIC_BYTES_PER_BODY = 104
 
 
-def ncu_traffic(n: int):
-    if TRAFFIC_BYTES_PER_BODY is None:
+def ncu_traffic(n: int, kernel: str, jsplit: int):
+    if kernel not in TRAFFIC_BYTES_PER_BODY or jsplit != 8:
         return None
-    return TRAFFIC_BYTES_PER_BODY * n
+    return TRAFFIC_BYTES_PER_BODY[kernel] * n
 
 
 # ---------------------------------------------------------------------------------------
@@ -347,9 +356,9 @@ def run_single(gx, torch, p, args, eps, dt, prec) -> dict:
                           "MEASURED_PEAKS.json); the FP32 FMA pipe bounds this kernel, not HBM or tensor cores",
             "ops_per_interaction": FMA_PIPE_OPS_PER_INTERACTION,
             "kernel_ms_per_launch": force_avg_s * 1e3,
-            "traffic": ncu_traffic(n),
+            "traffic": ncu_traffic(n, gx.describe_variant(prec, variant), jsplit),
             "algorithmic_bytes": ALGORITHMIC_BYTES_PER_BODY * n,
-            "traffic_capture": TRAFFIC_CAPTURE}
+            "traffic_capture": traffic_capture(gx.describe_variant(prec, variant)) if jsplit == 8 else None}
     if clk.get("sm_mhz"):
         roof["frac_at_observed_clock"] = achieved / (sms * FP32_LANES_PER_SM * clk["sm_mhz"] * 1e6 / 1e12)
     if prec == gx.PRECISION_F64:

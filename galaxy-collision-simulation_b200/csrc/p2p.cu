@@ -155,12 +155,17 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
     const int tid = threadIdx.x;
     const int n_items = *a.plan_n_items;
     const bool by_slot = *a.src_ok != 0;
+    // The next item's ticket is taken while the current item runs (thread 0 reads the
+    // atomic's result only when the item is done), so its latency is not paid per item.
+    int next = 0;
+    if (tid == 0) next = atomicAdd(a.ticket, 1);
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.ticket, 1);
+        if (tid == 0) s_item = next;
         __syncthreads();
         const int item = s_item;
         __syncthreads();
         if (item >= n_items) return;
+        if (tid == 0) next = atomicAdd(a.ticket, 1);
         // leaf owning the item: one load from the table p2p_item_leaf_kernel filled; items past
         // the table (possible only with device CSR arrays that repeat bodies) search the offsets
         int leaf;

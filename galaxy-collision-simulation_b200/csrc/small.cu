@@ -55,8 +55,16 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     return v;
 }
 
+__device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Grid-wide barrier; false on every thread of the CTA when the launch has to stop.
-// `gen` (thread 0 only) is the generation this CTA waits to see pass.
+// `gen` (thread 0 only) is the generation this CTA waits to see pass.  One returning atomic
+// per CTA (the arrival); the last arrival resets the counter with a plain store and, after a
+// fence, releases the others with a non-returning release add on the generation word, so no
+// second returning round trip to L2 sits on the path.  A status set by a CTA that gave up is seen by the others at their
+// next wait (polled every 256 loads); the launch then ends within one barrier.
 __device__ bool grid_barrier(const SmallArgs& a, unsigned& gen) {
     __shared__ int s_ok;
     __syncthreads();
@@ -65,9 +73,9 @@ __device__ bool grid_barrier(const SmallArgs& a, unsigned& gen) {
         __threadfence();  // after the CTA barrier: the CTA's position stores before its arrival
         const unsigned arrived = atomicAdd(&a.bar[0], 1u);
         if (arrived == gridDim.x - 1) {
-            atomicExch(&a.bar[0], 0u);  // reset before anyone can pass
-            __threadfence();
-            atomicAdd(&a.bar[1], 1u);
+            *(volatile unsigned*)&a.bar[0] = 0u;  // nobody arrives again before the release below
+            __threadfence();  // every arrival seen through the counter, before the release
+            red_release_add_u32(&a.bar[1], 1u);
         } else {
             const unsigned long long t0 = global_ns();
             unsigned polls = 0;
@@ -82,8 +90,6 @@ __device__ bool grid_barrier(const SmallArgs& a, unsigned& gen) {
             }
         }
         if (!ok) atomicExch(a.status, 1);
-        __threadfence();
-        if (*(volatile int*)a.status) ok = 0;
         gen += 1;
         s_ok = ok;
     }
