@@ -962,6 +962,27 @@ def wl_fmm(gx, torch, args, e2e: bool = True) -> dict:
             "traffic_note": "node records, bodies and lists stay in L2: ncu DRAM reads 7.7 MB (far field) and "
                             "5.1 MB (near field) per evaluation at this size"}
 
+    # the resident session with the FMM force: chunks of 32 KDK steps replayed as CUDA graphs
+    # (no host synchronisation inside a chunk; one read of the pool-overflow word after it)
+    sess_steps = 64
+    with gx.Session(n, params) as sess:
+        sess.set_fmm(opt)
+        sess.set_particles(p)
+        sess.compute_accelerations(gx.PRECISION_F64)
+        sst = torch.cuda.Stream()
+        sess.set_stream(sst)
+        sess.step(32, dt, gx.PRECISION_F64)  # sizes the pools, captures the graph
+        sess.synchronize()
+        s0, s1 = _events(torch)
+        s0.record(sst)
+        sess.step(sess_steps, dt, gx.PRECISION_F64)
+        s1.record(sst)
+        s1.synchronize()
+        sess_ms = s0.elapsed_time(s1) / sess_steps
+    session = {"value": 1e3 / sess_ms, "unit": "steps/s", "ms_per_step": sess_ms, "steps": sess_steps,
+               "launch": "gx_session_step with the FMM force: CUDA graphs of 32 KDK steps, device pools sized by "
+                         "capacity, one read of the overflow word per chunk"}
+
     # e2e: the public API on host arrays (H2D of x, y, z, m and D2H of a inside the call)
     e2e_rate_ = None
     if e2e:
@@ -1003,8 +1024,10 @@ def wl_fmm(gx, torch, args, e2e: bool = True) -> dict:
     mixed = {"value": 1e3 / ms_mixed, "unit": "steps/s", "ms_per_step": ms_mixed,
              "rel_err_vs_f64": {"median": float(np.median(em)), "max": float(em.max()), "bodies": n}}
 
-    out = {"metric": "FMM KDK steps/s (N=65536, leaf 64, theta 0.6, p=4, FP64)", "value": 1e3 / ms,
-           "unit": "steps/s", "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+    out = {"metric": "FMM KDK steps/s (N=65536, leaf 64, theta 0.6, p=4, FP64)", "value": session["value"],
+           "session": session, "evaluation_loop": {"value": 1e3 / ms, "unit": "steps/s", "ms_per_step": ms,
+                                                   "launch": "kick-drift, gx_fmm_accel (two host reads), kick"},
+           "unit": "steps/s", "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": sess_ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "phases_ms_per_eval": ph, "stats": stats.__dict__,
            "gpu_launches": steps * (19 + stats.tree_levels + 2),

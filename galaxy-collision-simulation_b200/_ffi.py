@@ -130,6 +130,7 @@ _SIGNATURES = {
     "gx_session_synchronize": [P],
     "gx_session_set_persistent": [P, c_int],
     "gx_session_set_targets": [P, I64, I64],
+    "gx_session_set_fmm": [P, P],
     "gx_session_kick_drift": [P, D, D],
     "gx_session_force_kick": [P, D, c_int],
     "gx_session_synchronize_timeout": [P, D],
@@ -182,6 +183,8 @@ _SIGNATURES = {
     "gx_debug_stall_barrier": [I64],
     "gx_debug_p2p_targets_per_thread": [c_int],
     "gx_debug_small_targets_per_warp": [c_int],
+    "gx_debug_small_warps_per_target": [c_int],
+    "gx_debug_fmm_tight_pools": [c_int],
 }
 _RESTYPES = {"gx_last_error": c_char_p, "gx_galaxies_body_count": c_int64}
 

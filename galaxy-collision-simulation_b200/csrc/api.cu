@@ -43,6 +43,7 @@ namespace {
 thread_local std::string g_err;
 std::atomic<int> g_fail_allocs{0};
 std::atomic<int64_t> g_stall_step{-1};  // gx_debug_stall_barrier
+std::atomic<int> g_fmm_tight_pools{0};  // gx_debug_fmm_tight_pools: no headroom (tests of the regrowth)
 
 int fail(int code, const char* fmt, ...) {
     char buf[1024];
@@ -528,6 +529,18 @@ extern "C" int gx_debug_small_targets_per_warp(int tpw) {
     return GX_OK;
 }
 
+extern "C" int gx_debug_small_warps_per_target(int wpt) {
+    if (wpt != 0 && wpt != 1 && wpt != 2)
+        return fail(GX_ERR_INVALID_ARGUMENT, "gx_debug_small_warps_per_target: 0, 1 or 2");
+    small_set_warps_per_target(wpt);
+    return GX_OK;
+}
+
+extern "C" int gx_debug_fmm_tight_pools(int enable) {
+    g_fmm_tight_pools.store(enable ? 1 : 0);
+    return GX_OK;
+}
+
 extern "C" int gx_debug_stall_barrier(int64_t step) {
     g_stall_step.store(step < 0 ? -1 : step);
     return GX_OK;
@@ -774,6 +787,11 @@ extern "C" int gx_diagnostics_compute(int64_t n, const double* x, const double* 
 // ======================================================================================
 // resident session
 // ======================================================================================
+namespace {
+struct FmmWork;
+void fmm_work_release(FmmWork* w);
+}  // namespace
+
 struct gx_session {
     int device = 0;
     int64_t n = 0;
@@ -798,6 +816,15 @@ struct gx_session {
     bool persistent = true;     // small systems step in one cooperative launch (small.cu)
     void* small = nullptr;      // its scratch: barrier words, status, two position buffers
     bool small_pending = false; // a launch ran since the status word was last read
+    // FMM force (gx_session_set_fmm): the options, the capacity-mode workspace (sized by a
+    // first evaluation, regrown on overflow), a copy of the state a chunk of steps starts
+    // from, and pinned words for the chunk's overflow flag
+    bool fmm_on = false;
+    bool fmm_host_only = false;  // the tree needs the host builder: evaluations read sizes back
+    gx_fmm_options fmm_opt{0.6, 16, 32, 4};
+    FmmWork* fmm = nullptr;
+    double* backup = nullptr;
+    int* host_flag = nullptr;
 
     void clear_graphs() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -851,7 +878,12 @@ int flush_events(gx_session* s) {
 }
 
 // Force evaluation of the session (closing kick when kick_dt != 0), timed on request.
+int session_fmm_force(gx_session* s, int precision, double kick_dt);
+int session_fmm_compute(gx_session* s, int precision);
+int session_fmm_steps(gx_session* s, int64_t n_steps, double dt, int precision);
+
 int session_force(gx_session* s, int precision, double kick_dt) {
+    if (s->fmm_on) return session_fmm_force(s, precision, kick_dt);
     Choice ch;
     GX_TRY(session_choice(s, precision, &ch));
     GX_TRY(session_ensure_part(s, ch));
@@ -892,8 +924,13 @@ int session_enqueue_steps(gx_session* s, int64_t k, double dt, int precision) {
 
 int session_graph(gx_session* s, int64_t k, double dt, int precision, cudaGraphExec_t* out) {
     Choice ch;
-    GX_TRY(session_choice(s, precision, &ch));
-    GX_TRY(session_ensure_part(s, ch));
+    if (s->fmm_on) {
+        ch.variant = -2;  // the FMM force; graphs are dropped when its workspace changes
+        ch.nsplit = 0;
+    } else {
+        GX_TRY(session_choice(s, precision, &ch));
+        GX_TRY(session_ensure_part(s, ch));
+    }
     uint64_t dtb;
     std::memcpy(&dtb, &dt, sizeof(dtb));
     const auto key = std::make_tuple(k, dtb, precision, ch.variant, ch.nsplit);
@@ -929,8 +966,8 @@ int check_session(gx_session* s, const char* fn) {
 // Steps that run as one cooperative launch: small systems in FP64 or the exact form, unless
 // the caller turned it off or is timing force launches one by one.
 bool session_small_eligible(const gx_session* s, int precision) {
-    return s->persistent && !s->timing && s->n <= kSmallMaxBodies && s->t_begin == 0 && s->t_count == s->n &&
-           (precision == kF64 || precision == kF64Exact);
+    return s->persistent && !s->timing && !s->fmm_on && s->n <= kSmallMaxBodies && s->t_begin == 0 &&
+           s->t_count == s->n && (precision == kF64 || precision == kF64Exact);
 }
 
 int session_small_steps(gx_session* s, int64_t k, double dt, int precision) {
@@ -1033,6 +1070,9 @@ extern "C" int gx_session_destroy(gx_session* s) {
         cudaEventDestroy(ev.second);
     }
     s->clear_graphs();
+    fmm_work_release(s->fmm);
+    if (s->backup) cudaFree(s->backup);
+    if (s->host_flag) cudaFreeHost(s->host_flag);
     if (s->small) cudaFree(s->small);
     if (s->part) cudaFree(s->part);
     if (s->diag) cudaFree(s->diag);
@@ -1128,6 +1168,7 @@ extern "C" int gx_session_compute_accelerations(gx_session* s, int precision) {
     GX_TRY(check_session(s, "gx_session_compute_accelerations"));
     if (!valid_precision(precision)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_compute_accelerations: precision");
     DeviceGuard g(s->device);
+    if (s->fmm_on) return session_fmm_compute(s, precision);
     return session_force(s, precision, 0.0);
     GX_GUARD_END
 }
@@ -1140,6 +1181,7 @@ extern "C" int gx_session_step(gx_session* s, int64_t n_steps, double dt, int pr
     if (n_steps < 0 || !std::isfinite(dt)) return fail(GX_ERR_INVALID_ARGUMENT, "%s: need n_steps >= 0, finite dt", fn);
     if (n_steps == 0) return GX_OK;
     DeviceGuard g(s->device);
+    if (s->fmm_on) return session_fmm_steps(s, n_steps, dt, precision);
     if (session_small_eligible(s, precision)) {
         const int r = session_small_steps(s, n_steps, dt, precision);
         if (r != GX_ERR_UNSUPPORTED) return r;
@@ -1183,6 +1225,22 @@ extern "C" int gx_session_set_persistent(gx_session* s, int enable) {
     GX_TRY(check_session(s, "gx_session_set_persistent"));
     s->persistent = enable != 0;
     return GX_OK;
+}
+
+extern "C" int gx_session_set_fmm(gx_session* s, const gx_fmm_options* opt) {
+    GX_GUARD_BEGIN
+    GX_TRY(check_session(s, "gx_session_set_fmm"));
+    if (opt && !(opt->theta == opt->theta)) return fail(GX_ERR_INVALID_ARGUMENT, "gx_session_set_fmm: theta is NaN");
+    DeviceGuard g(s->device);
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    fmm_work_release(s->fmm);
+    s->fmm = nullptr;
+    s->fmm_host_only = false;
+    s->fmm_on = opt != nullptr;
+    if (opt) s->fmm_opt = *opt;
+    s->clear_graphs();
+    return GX_OK;
+    GX_GUARD_END
 }
 
 extern "C" int gx_session_set_targets(gx_session* s, int64_t begin, int64_t count) {
@@ -1429,7 +1487,7 @@ extern "C" int gx_p2p_leaves(int64_t n, const double* x, const double* y, const 
     GX_TRY(classify({x, y, z, m, leaf_offsets, leaf_particles, near_offsets, near_leaves, ax, ay, az}, &device, &dev, fn));
     DeviceGuard g(dev);
     cudaStream_t st = (cudaStream_t)stream;
-    P2PArgs a;
+    P2PArgs a{};
     a.n_leaves = n_leaves;
     a.t_begin = 0;
     a.t_end = n;
@@ -1776,7 +1834,7 @@ int fmm_plan_device(FmmPlan& P, int64_t n, const double* dx, const double* dy, c
     const size_t order_bytes = item_order_temp_bytes(fa.n_items);
     void* order_temp;
     GX_TRY(dev_array(hs, (int64_t)order_bytes, (char**)&order_temp));
-    GX_CUDA(launch_item_order(items, la.leaf_off, fa.n_items, cost, cost_alt, idx, idx_alt, order_temp, order_bytes,
+    GX_CUDA(launch_item_order(items, la.leaf_off, fa.n_items, nullptr, nullptr, cost, cost_alt, idx, idx_alt, order_temp, order_bytes,
                               sorted_items, st));
     items = sorted_items;
     GX_TRY(mark(tm, 3, st));
@@ -1905,7 +1963,7 @@ int fmm_accel(const char* fn, int64_t n, const double* x, const double* y, const
         GX_CUDA(launch_fmm_m2p(fa, mixed, st));
         GX_TRY(mark(tm.get(), 4, st));
 
-        P2PArgs pa;
+        P2PArgs pa{};
         pa.x = dx; pa.y = dy; pa.z = dz; pa.m = dm;
         pa.leaf_off = fa.leaf_off; pa.leaf_part = fa.leaf_part; pa.near_off = P->near_off; pa.near_leaf = P->near_leaf;
         pa.n_leaves = P->n_leaves;
@@ -1935,6 +1993,366 @@ int fmm_accel(const char* fn, int64_t n, const double* x, const double* y, const
             phase_ms[k] = ms;
         }
         if (tm->host_tree_ms >= 0.0) phase_ms[0] = tm->host_tree_ms;
+    }
+    return GX_OK;
+}
+
+// ---- FMM evaluation without host reads (capacity mode) ---------------------------------
+// gx_fmm_accel reads two sizes back per evaluation (node and level counts after the tree,
+// list totals after the count walk) and sizes everything after them exactly.  FmmWork holds
+// the same device arrays sized by capacities instead -- node slots and list, item and slot
+// pools from a sizing evaluation with headroom -- so that an evaluation is a fixed sequence of
+// launches with no host synchronisation (and can be captured in a CUDA graph): every kernel
+// reads its counts on the device, pool_check marks an overflow when this evaluation needs more
+// than a pool holds (or the tree needs the host builder), and everything after it is skipped;
+// the caller checks the sticky flag and redoes the work with larger pools.
+struct FmmWork {
+    int64_t n = 0;
+    gx_physics phys{};
+    gx_fmm_options opt{};
+    int32_t node_cap = 0;
+    int64_t far_cap = 0, near_cap = 0, item_cap = 0, slot_cap = 0;
+    int32_t leaves_hint = 0;
+    std::vector<void*> owned;
+    TreeBuildArgs t{};
+    void* tree_temp = nullptr;
+    size_t tree_bytes = 0;
+    FmmArgs fa{};
+    TreeListArgs la{};
+    void* list_temp = nullptr;
+    size_t list_bytes = 0;
+    M2PItem *items = nullptr, *sorted = nullptr;
+    uint32_t *cost = nullptr, *cost_alt = nullptr;
+    int32_t *idx = nullptr, *idx_alt = nullptr;
+    void* order_temp = nullptr;
+    size_t order_bytes = 0;
+    void* p2p_scratch = nullptr;
+    int* flags = nullptr;                // device: [0] per-evaluation overflow, [1] sticky (bit 1: too deep)
+    unsigned long long* need = nullptr;  // device: largest {nodes, far, near, items, slots} seen
+    ~FmmWork() {
+        for (void* p : owned) cudaFree(p);
+    }
+    template <typename T>
+    int grab(int64_t count, T** p) {
+        void* q = nullptr;
+        cudaError_t e = dev_alloc(&q, (size_t)std::max<int64_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc (FMM workspace)");
+        owned.push_back(q);
+        *p = (T*)q;
+        return GX_OK;
+    }
+};
+
+int64_t with_headroom(int64_t v) { return g_fmm_tight_pools.load() ? std::max<int64_t>(v, 1) : v + v / 2 + 4096; }
+
+// Capacities from a sizing evaluation's counts (or from the largest counts an overflowing
+// evaluation needed), with half again as much headroom; node slots never above the most a
+// tree of n bodies can have.
+int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_fmm_options opt, int64_t nodes,
+                    int64_t leaves, int64_t far, int64_t near, int64_t items, int64_t slots, cudaStream_t st) {
+    W.reset(new FmmWork());
+    FmmWork& w = *W;
+    w.n = n;
+    w.phys = phys;
+    w.opt = opt;
+    const int64_t cap = std::max<int64_t>(1, opt.leaf_capacity);
+    const int64_t node_bound = 1 + 8 * (int64_t)kKeyLevels * (n / (cap + 1) + 1);
+    w.node_cap = (int32_t)std::min<int64_t>({with_headroom(nodes), node_bound, (int64_t)0x7fff0000});
+    w.far_cap = with_headroom(far);
+    w.near_cap = with_headroom(near);
+    w.item_cap = std::min<int64_t>(with_headroom(items), 0x7fff0000);
+    w.slot_cap = with_headroom(slots);
+    w.leaves_hint = (int32_t)std::max<int64_t>(1, leaves);
+    const int32_t NC = w.node_cap;
+    TreeBuildArgs& t = w.t;
+    t.n = (int32_t)n;
+    t.softening = phys.softening;
+    t.cap = cap;
+    t.max_depth = std::max(1, opt.max_depth);
+    t.capacity = NC;
+    GX_TRY(w.grab(6 * kBboxBlocks, &t.part));
+    GX_TRY(w.grab(4, &t.root));
+    GX_TRY(w.grab(n, &t.keys));
+    GX_TRY(w.grab(n, &t.keys_alt));
+    GX_TRY(w.grab(n, &t.idx));
+    GX_TRY(w.grab(n, &t.perm));
+    GX_TRY(w.grab(kKeyLevels + 3, &t.level_off));
+    GX_TRY(w.grab(3, &t.hdr));
+    for (int32_t** q : {&t.beg, &t.end, &t.child}) GX_TRY(w.grab(NC, q));
+    for (double** q : {&t.cx, &t.cy, &t.cz, &t.hw}) GX_TRY(w.grab(NC, q));
+    w.tree_bytes = tree_build_temp_bytes(t.n, cap);
+    GX_TRY(w.grab((int64_t)w.tree_bytes, (char**)&w.tree_temp));
+    GX_TRY(w.grab(2, &w.flags));
+    GX_TRY(w.grab(5, &w.need));
+
+    FmmArgs& fa = w.fa;
+    fmm_common_args(fa, nullptr, nullptr, nullptr, nullptr, phys, opt, 0, n);
+    fa.n_nodes = NC;
+    fa.node_beg = t.beg;
+    fa.node_end = t.end;
+    fa.node_child = t.child;
+    fa.node_cx = t.cx;
+    fa.node_cy = t.cy;
+    fa.node_cz = t.cz;
+    fa.perm = t.perm;
+    fa.cnt_nodes = t.hdr;
+    GX_TRY(w.grab((int64_t)NC * kFmmRec, &fa.rec));
+    GX_TRY(w.grab((int64_t)NC * kRec32, &fa.rec32));
+
+    TreeListArgs& la = w.la;
+    la.n = t.n;
+    la.n_nodes = NC;
+    la.beg = t.beg;
+    la.end = t.end;
+    la.child = t.child;
+    la.perm = t.perm;
+    la.cx = t.cx;
+    la.cy = t.cy;
+    la.cz = t.cz;
+    la.hw = t.hw;
+    la.rec = fa.rec;
+    la.theta = std::max(1.0e-6, opt.theta);
+    la.t_begin = 0;
+    la.t_end = n;
+    la.cnt_nodes = t.hdr;
+    la.overflow = w.flags;
+    la.overflow_sticky = w.flags + 1;
+    la.need = w.need;
+    la.far_cap = w.far_cap;
+    la.near_cap = w.near_cap;
+    la.item_cap = w.item_cap;
+    la.slot_cap = w.slot_cap;
+    for (int32_t** q : {&la.start_flag, &la.start_ord, &la.keep, &la.newpos}) GX_TRY(w.grab(n + 1, q));
+    GX_TRY(w.grab((int64_t)NC + 1, &la.leaf_off));
+    GX_TRY(w.grab(n, &la.leaf_part));
+    GX_TRY(w.grab((int64_t)NC + 1, &la.leaf_node));
+    GX_TRY(w.grab((int64_t)NC + 1, &la.node_leaf));
+    for (int32_t** q : {&la.far_cnt, &la.near_cnt, &la.item_cnt, &la.slot_cnt, &la.far_off, &la.near_off,
+                        &la.item_off, &la.slot_off})
+        GX_TRY(w.grab((int64_t)NC + 1, q));
+    GX_TRY(w.grab(6, &la.totals));
+    GX_TRY(w.grab(NC, &la.wn));
+    w.list_bytes = tree_list_temp_bytes(la.n, NC);
+    GX_TRY(w.grab((int64_t)w.list_bytes, (char**)&w.list_temp));
+    GX_TRY(w.grab(w.far_cap, &la.far_node));
+    GX_TRY(w.grab(w.near_cap, &la.near_key));
+    GX_TRY(w.grab(w.near_cap, &la.near_leaf));
+    GX_TRY(w.grab((int64_t)NC, &la.long_leaf));
+    GX_TRY(w.grab(1, &la.long_count));
+    GX_TRY(w.grab(w.item_cap, &w.items));
+    la.items = w.items;
+    GX_TRY(w.grab(w.item_cap, &w.sorted));
+    GX_TRY(w.grab(w.item_cap, &w.cost));
+    GX_TRY(w.grab(w.item_cap, &w.cost_alt));
+    GX_TRY(w.grab(w.item_cap, &w.idx));
+    GX_TRY(w.grab(w.item_cap, &w.idx_alt));
+    w.order_bytes = item_order_temp_bytes((int32_t)w.item_cap);
+    GX_TRY(w.grab((int64_t)w.order_bytes, (char**)&w.order_temp));
+
+    fa.n_leaves = NC;
+    fa.cnt_leaves = la.start_ord + n;
+    fa.leaf_off = la.leaf_off;
+    fa.leaf_part = la.leaf_part;
+    fa.far_node = la.far_node;
+    fa.items = w.sorted;
+    fa.n_items = (int32_t)w.item_cap;
+    fa.cnt_items = la.totals + 2;
+    fa.overflow = w.flags;
+    GX_TRY(w.grab(w.slot_cap * 3, &fa.scratch));
+    GX_TRY(w.grab(NC, &fa.done));
+    GX_TRY(w.grab((int64_t)p2p_scratch_bytes(n, NC), (char**)&w.p2p_scratch));
+    GX_CUDA(cudaMemsetAsync(w.flags, 0, 2 * sizeof(int), st));
+    GX_CUDA(cudaMemsetAsync(w.need, 0, 5 * sizeof(unsigned long long), st));
+    return GX_OK;
+}
+
+// One FMM evaluation of the bodies (device arrays of w.n) into ax, ay, az, stream-ordered,
+// with no host synchronisation.  A pool overflow leaves ax, ay, az zeroed and sets flags[1].
+int fmm_work_enqueue(FmmWork& w, const double* x, const double* y, const double* z, const double* m,
+                     int precision, double* ax, double* ay, double* az, int dev, cudaStream_t st) {
+    const int64_t n = w.n;
+    TreeBuildArgs& t = w.t;
+    t.x = x;
+    t.y = y;
+    t.z = z;
+    GX_CUDA(cudaMemsetAsync(w.flags, 0, sizeof(int), st));
+    GX_CUDA(launch_tree_build(t, w.tree_temp, w.tree_bytes, st));
+    GX_CUDA(launch_tree_leaf_order(t, w.node_cap, w.tree_temp, w.tree_bytes, st));
+    FmmArgs& fa = w.fa;
+    fa.x = x;
+    fa.y = y;
+    fa.z = z;
+    fa.m = m;
+    GX_CUDA(launch_fmm_moments_device(fa, t.level_off, t.hdr + 1, st));
+    TreeListArgs& la = w.la;
+    GX_CUDA(launch_tree_lists_count(la, w.list_temp, w.list_bytes, st));
+    GX_CUDA(launch_pool_check(la, t.hdr, st));
+    GX_CUDA(launch_tree_lists_fill(la, w.node_cap, st));
+    GX_CUDA(launch_item_order(w.items, la.leaf_off, (int32_t)w.item_cap, la.totals + 2, w.flags, w.cost, w.cost_alt,
+                              w.idx, w.idx_alt, w.order_temp, w.order_bytes, w.sorted, st));
+    for (double* p : {ax, ay, az}) GX_CUDA(cudaMemsetAsync(p, 0, (size_t)n * sizeof(double), st));
+    fa.ax = ax;
+    fa.ay = ay;
+    fa.az = az;
+    fa.eps2f = (float)fa.eps2;
+    GX_CUDA(cudaMemsetAsync(fa.done, 0, (size_t)w.node_cap * sizeof(int), st));
+    GX_CUDA(launch_fmm_m2p(fa, precision == kMixed, st));
+    P2PArgs pa{};
+    pa.x = x; pa.y = y; pa.z = z; pa.m = m;
+    pa.leaf_off = la.leaf_off; pa.leaf_part = la.leaf_part; pa.near_off = la.near_off; pa.near_leaf = la.near_leaf;
+    pa.n_leaves = w.node_cap;
+    pa.cnt_leaves = la.start_ord + n;
+    pa.overflow = w.flags;
+    pa.leaves_hint = w.leaves_hint;
+    pa.ax = ax; pa.ay = ay; pa.az = az;
+    pa.t_begin = 0;
+    pa.t_end = n;
+    pa.G = w.phys.G;
+    pa.eps2 = w.phys.softening * w.phys.softening;
+    pa.eps2f = (float)pa.eps2;
+    GX_CUDA(launch_p2p(pa, n, precision, w.p2p_scratch, sm_count(dev), st));
+    return GX_OK;
+}
+
+void fmm_work_release(FmmWork* w) { delete w; }
+
+// Sizes the session's FMM workspace from one evaluation that reads its sizes back (the
+// accelerations of that evaluation are not kept); *device_ok is false when the tree needs
+// the host builder.
+int session_fmm_size(gx_session* s, bool* device_ok) {
+    std::unique_ptr<FmmPlan> P(new FmmPlan(s->stream));
+    bool deep = false;
+    GX_TRY(fmm_plan_device(*P, s->n, s->x, s->y, s->z, s->m, s->phys, s->fmm_opt, 0, s->n, &deep, nullptr));
+    *device_ok = !deep;
+    if (deep) return GX_OK;
+    std::unique_ptr<FmmWork> W;
+    GX_TRY(fmm_work_create(W, s->n, s->phys, s->fmm_opt, P->n_nodes, P->n_leaves, P->n_far, P->n_near,
+                           P->fa.n_items, P->n_slots, s->stream));
+    fmm_work_release(s->fmm);
+    s->fmm = W.release();
+    s->clear_graphs();
+    return GX_OK;
+}
+
+// After an overflow: pools at least as large as the largest an evaluation needed, and half
+// again larger than before.
+int session_fmm_regrow(gx_session* s) {
+    FmmWork& w = *s->fmm;
+    unsigned long long need[5];
+    GX_CUDA(cudaMemcpyAsync(need, w.need, sizeof(need), cudaMemcpyDeviceToHost, s->stream));
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    std::unique_ptr<FmmWork> W;
+    GX_TRY(fmm_work_create(W, s->n, s->phys, s->fmm_opt, std::max<int64_t>((int64_t)need[0], w.node_cap),
+                           w.leaves_hint, std::max<int64_t>((int64_t)need[1], w.far_cap),
+                           std::max<int64_t>((int64_t)need[2], w.near_cap), std::max<int64_t>((int64_t)need[3], w.item_cap),
+                           std::max<int64_t>((int64_t)need[4], w.slot_cap), s->stream));
+    fmm_work_release(s->fmm);
+    s->fmm = W.release();
+    s->clear_graphs();
+    return GX_OK;
+}
+
+// An evaluation that reads its sizes back (and builds deep trees on the host).
+int session_fmm_eval_sync(gx_session* s, int precision) {
+    return fmm_accel("gx_session_step", s->n, s->x, s->y, s->z, s->m, s->phys, s->fmm_opt, precision, 0, s->n, s->ax,
+                     s->ay, s->az, nullptr, s->stream, nullptr);
+}
+
+int session_fmm_force(gx_session* s, int precision, double kick_dt) {
+    if (!s->fmm) return fail(GX_ERR_CUDA, "session FMM force: workspace missing");
+    GX_TRY(fmm_work_enqueue(*s->fmm, s->x, s->y, s->z, s->m, precision, s->ax, s->ay, s->az, s->device, s->stream));
+    if (kick_dt != 0.0) GX_CUDA(launch_kick(s->n, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, kick_dt, s->stream));
+    return GX_OK;
+}
+
+int session_fmm_prepare(gx_session* s) {
+    if (s->t_begin != 0 || s->t_count != s->n)
+        return fail(GX_ERR_UNSUPPORTED, "session FMM: owned target ranges are not supported with the FMM force");
+    if (s->fmm || s->fmm_host_only) return GX_OK;
+    bool ok = true;
+    GX_TRY(session_fmm_size(s, &ok));
+    if (!ok) s->fmm_host_only = true;
+    return GX_OK;
+}
+
+// Reads the chunk's sticky overflow word (synchronises the stream): 0, 1 (a pool overflowed)
+// or 3 (the tree needs the host builder).
+int session_fmm_flag(gx_session* s, int* flag) {
+    if (!s->host_flag) GX_CUDA(cudaMallocHost((void**)&s->host_flag, sizeof(int)));
+    GX_CUDA(cudaMemcpyAsync(s->host_flag, s->fmm->flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    GX_CUDA(cudaStreamSynchronize(s->stream));
+    *flag = *s->host_flag;
+    return GX_OK;
+}
+
+int session_fmm_compute(gx_session* s, int precision) {
+    GX_TRY(session_fmm_prepare(s));
+    for (int attempt = 0; attempt < 3 && !s->fmm_host_only; ++attempt) {
+        GX_CUDA(cudaMemsetAsync(s->fmm->flags + 1, 0, sizeof(int), s->stream));
+        GX_TRY(session_fmm_force(s, precision, 0.0));
+        int flag = 0;
+        GX_TRY(session_fmm_flag(s, &flag));
+        if (flag == 0) return GX_OK;
+        if (flag & 2) {
+            s->fmm_host_only = true;
+            break;
+        }
+        GX_TRY(session_fmm_regrow(s));
+    }
+    return session_fmm_eval_sync(s, precision);
+}
+
+// KDK steps with the FMM force: chunks of up to 32 steps, each replayed as one CUDA graph (no
+// host synchronisation inside it) from a copy of the state taken on the device; after a chunk
+// one read of its overflow word.  An overflow restores the copy, regrows the pools and redoes
+// the chunk; a tree that needs the host builder, or a third overflow, takes the chunk one
+// evaluation at a time through the path that reads its sizes back.
+int session_fmm_steps(gx_session* s, int64_t n_steps, double dt, int precision) {
+    GX_TRY(session_fmm_prepare(s));
+    const double half = 0.5 * dt;
+    auto eager = [&](int64_t k) -> int {
+        for (int64_t i = 0; i < k; ++i) {
+            GX_TRY(session_kick_drift(s, half, dt));
+            GX_TRY(session_fmm_eval_sync(s, precision));
+            GX_CUDA(launch_kick(s->n, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, half, s->stream));
+        }
+        return GX_OK;
+    };
+    const size_t state_bytes = (size_t)9 * (size_t)s->n * sizeof(double);  // x .. az, contiguous
+    for (int64_t done = 0; done < n_steps;) {
+        const int64_t k = std::min<int64_t>(n_steps - done, 32);
+        bool ok = false;
+        for (int attempt = 0; attempt < 3 && !s->fmm_host_only; ++attempt) {
+            if (!s->backup) {
+                void* p = nullptr;
+                cudaError_t e = dev_alloc(&p, state_bytes);
+                if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc (session FMM state copy)");
+                s->backup = (double*)p;
+            }
+            GX_CUDA(cudaMemcpyAsync(s->backup, s->buf, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+            GX_CUDA(cudaMemsetAsync(s->fmm->flags + 1, 0, sizeof(int), s->stream));
+            if (s->timing || s->stream == nullptr) {
+                GX_TRY(session_enqueue_steps(s, k, dt, precision));
+            } else {
+                cudaGraphExec_t ge;
+                GX_TRY(session_graph(s, k, dt, precision, &ge));
+                GX_CUDA(cudaGraphLaunch(ge, s->stream));
+            }
+            int flag = 0;
+            GX_TRY(session_fmm_flag(s, &flag));
+            if (flag == 0) {
+                ok = true;
+                break;
+            }
+            GX_CUDA(cudaMemcpyAsync(s->buf, s->backup, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+            if (flag & 2) {
+                s->fmm_host_only = true;
+                break;
+            }
+            GX_TRY(session_fmm_regrow(s));
+        }
+        if (!ok) GX_TRY(eager(k));
+        done += k;
     }
     return GX_OK;
 }

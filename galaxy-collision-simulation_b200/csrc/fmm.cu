@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
     const int wl = threadIdx.x >> 5;
     const int w = (int)((blockIdx.x * (unsigned)kMomBlock + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (w >= a.n_nodes || a.node_child[w] >= 0) return;
+    if (w >= fmm_nodes(a) || a.node_child[w] >= 0) return;
     const int b = a.node_beg[w], e = a.node_end[w];
     double* r = a.rec + (size_t)w * kFmmRec;
     double(*sb)[32] = s_b[wl];
@@ -187,10 +187,9 @@ __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
 // contribution to every moment (lane a for moment 4 + a), and warp 0 adds the 8
 // contributions in child order, as the reference does.  A massless child adds exact zeros
 // to every sum in the reference and is skipped here (masses are >= 0).
-__global__ void __launch_bounds__(256) fmm_m2m_kernel(const FmmArgs a, int lb) {
-    __shared__ double s_child[8][kRecTrQ];
-    __shared__ double s_val[8][32];
-    const int w = lb + blockIdx.x;
+// All threads of the CTA call it for the same node w (it holds CTA barriers).
+__device__ __forceinline__ void m2m_node(const FmmArgs& a, const int w, double (*s_child)[kRecTrQ],
+                                         double (*s_val)[32]) {
     const int c0 = a.node_child[w];
     if (c0 < 0) return;
     const int tid = threadIdx.x, c = tid >> 5, lane = tid & 31;
@@ -225,21 +224,40 @@ __global__ void __launch_bounds__(256) fmm_m2m_kernel(const FmmArgs a, int lb) {
         s_val[c][lane] = value;
     }
     __syncthreads();
-    if (c != 0) return;
-    double* r = a.rec + (size_t)w * kFmmRec;
-    if (lane < 31) {
-        double total = 0.0;
-        for (int q = 0; q < 8; ++q)
-            if (s_child[q][kRecMass] > 0.0) total = dadd(total, s_val[q][lane]);
-        r[4 + lane] = total;
-    } else {
-        r[0] = cx;
-        r[1] = cy;
-        r[2] = cz;
-        r[kRecMass] = mass;
+    if (c == 0) {
+        double* r = a.rec + (size_t)w * kFmmRec;
+        if (lane < 31) {
+            double total = 0.0;
+            for (int q = 0; q < 8; ++q)
+                if (s_child[q][kRecMass] > 0.0) total = dadd(total, s_val[q][lane]);
+            r[4 + lane] = total;
+        } else {
+            r[0] = cx;
+            r[1] = cy;
+            r[2] = cz;
+            r[kRecMass] = mass;
+        }
+        __syncwarp();
+        if (lane == 0) write_traces(r);
     }
-    __syncwarp();
-    if (lane == 0) write_traces(r);
+    __syncthreads();  // the staging arrays are free for the next node
+}
+
+__global__ void __launch_bounds__(256) fmm_m2m_kernel(const FmmArgs a, int lb) {
+    __shared__ double s_child[8][kRecTrQ];
+    __shared__ double s_val[8][32];
+    m2m_node(a, lb + blockIdx.x, s_child, s_val);
+}
+
+// The same for every node of level d, with the level bounds read on the device (level_off,
+// n_levels as the topology build left them): the CTAs stride over the level's nodes.
+__global__ void __launch_bounds__(256) fmm_m2m_level_kernel(const FmmArgs a, const int32_t* level_off,
+                                                            const int32_t* n_levels, int d) {
+    __shared__ double s_child[8][kRecTrQ];
+    __shared__ double s_val[8][32];
+    if (d >= *n_levels || fmm_nodes(a) == 0) return;
+    const int lb = level_off[d], le = min(level_off[d + 1], fmm_nodes(a));
+    for (int w = lb + blockIdx.x; w < le; w += gridDim.x) m2m_node(a, w, s_child, s_val);
 }
 
 __device__ __forceinline__ double rsqrt_t(double s) { return rsqrt_f64(s); }
@@ -326,7 +344,7 @@ __device__ __forceinline__ void m2p_one(const float* __restrict__ r, double tx, 
 // The mixed-precision records (kRec32) from the FP64 ones, one thread per node.
 __global__ void __launch_bounds__(256) fmm_rec32_kernel(const FmmArgs a) {
     const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= a.n_nodes) return;
+    if (k >= fmm_nodes(a)) return;
     const double* r = a.rec + (size_t)k * kFmmRec;
     float* o = a.rec32 + (size_t)k * kRec32;
     double* oc = reinterpret_cast<double*>(o);
@@ -377,7 +395,9 @@ __global__ void __launch_bounds__(kM2PBlock) fmm_m2p_kernel(const FmmArgs a) {
     __shared__ double s_red[kM2PBlock * 3];
     __shared__ int s_last;
     const int tid = threadIdx.x;
-    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+    if (a.overflow && *a.overflow) return;
+    const int n_items = fmm_items(a);
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const M2PItem w = a.items[it];
         const int cnt = w.fe - w.fb;
         const int tb = a.leaf_off[w.leaf], nt = a.leaf_off[w.leaf + 1] - tb;
@@ -513,6 +533,21 @@ int fmm_effective_order(int expansion_order) {
     int p = std::min(4, std::max(0, expansion_order));
     if (p == 1 || p == 3) ++p;
     return p;
+}
+
+cudaError_t launch_fmm_moments_device(const FmmArgs& a, const int32_t* level_off, const int32_t* n_levels,
+                                      cudaStream_t st) {
+    constexpr int wpb = kMomBlock / 32;
+    if (a.n_nodes == 0) return cudaSuccess;
+    fmm_leaf_kernel<<<(a.n_nodes + wpb - 1) / wpb, kMomBlock, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int grid = std::min(a.n_nodes, 148 * 8);
+    for (int d = kMaxLevels - 1; d >= 0; --d) {
+        fmm_m2m_level_kernel<<<grid, 256, 0, st>>>(a, level_off, n_levels, d);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st) {

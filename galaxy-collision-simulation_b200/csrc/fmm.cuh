@@ -67,7 +67,26 @@ struct FmmArgs {
     double eps2;
     float eps2f;
     int order;  // effective expansion order: 0, 2 or 4
+    // Counts on the device, when the host did not read them back (nullable): n_nodes,
+    // n_leaves and n_items above are then capacities, and kernels use min(count, capacity).
+    // cnt_nodes points at the topology build's header {nodes, levels, flags}: with a flag
+    // set (node slots exhausted, or a tree too deep for the device build) there are no nodes.
+    // overflow (nullable) set: a pool was too small, the evaluation is skipped.
+    const int32_t* cnt_nodes;
+    const int32_t* cnt_leaves;
+    const unsigned long long* cnt_items;
+    const int* overflow;
 };
+
+__device__ __forceinline__ int fmm_nodes(const FmmArgs& a) {
+    if (!a.cnt_nodes) return a.n_nodes;
+    return a.cnt_nodes[2] ? 0 : min(a.cnt_nodes[0], a.n_nodes);
+}
+__device__ __forceinline__ int fmm_items(const FmmArgs& a) {
+    return a.cnt_items ? (int)min(*a.cnt_items, (unsigned long long)a.n_items) : a.n_items;
+}
+
+constexpr int kMaxLevels = 22;  // levels an octree of 63-bit path keys can have
 
 // Effective expansion order of multipole_acceleration (multipole.cpp:261-265).
 int fmm_effective_order(int expansion_order);
@@ -75,6 +94,9 @@ constexpr int kM2PChunk = 512;  // far nodes per work item
 
 // Stream-ordered: leaf moments, then one launch per level (deepest first), then M2P.
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st);
+// The same with the level bounds on the device (kMaxLevels launches, empty levels return).
+cudaError_t launch_fmm_moments_device(const FmmArgs& a, const int32_t* level_off, const int32_t* n_levels,
+                                      cudaStream_t st);
 // mixed: FP32 multipole arithmetic on FP64 offsets (fills a.rec32 from a.rec first); else FP64.
 cudaError_t launch_fmm_m2p(const FmmArgs& a, bool mixed, cudaStream_t st);
 

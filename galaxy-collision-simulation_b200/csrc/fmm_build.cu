@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) gather_perm_kernel(const int32_t* idx_sor
 // indices in the leaf, written to t.idx and copied back.
 __global__ void __launch_bounds__(256) leaf_sort_kernel(const TreeBuildArgs t, int n_nodes) {
     const int w = (int)((blockIdx.x * 256u + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (w >= n_nodes || t.child[w] >= 0) return;
+    if (t.hdr[2] != 0 || w >= min(n_nodes, t.hdr[0]) || t.child[w] >= 0) return;
     const int b = t.beg[w], e = t.end[w];
     if (e - b < 2) return;
     for (int i = b + lane; i < e; i += 32) {
@@ -326,10 +326,17 @@ __global__ void __launch_bounds__(256) leaf_sort_kernel(const TreeBuildArgs t, i
 
 __device__ __forceinline__ double node_mass(const double* rec, int k) { return rec[(size_t)k * kFmmRec + kRecMass]; }
 
+// Nodes of the tree: the count on the device when the host did not read it (a.n_nodes is
+// then the capacity of the node arrays).
+__device__ __forceinline__ int list_nodes(const TreeListArgs& a) {
+    if (!a.cnt_nodes) return a.n_nodes;
+    return a.cnt_nodes[2] ? 0 : min(a.cnt_nodes[0], a.n_nodes);  // header {nodes, levels, flags}
+}
+
 // Marks the first body position of every leaf with mass > 0 and the bodies it keeps.
 __global__ void __launch_bounds__(256) leaf_mark_kernel(const TreeListArgs a) {
     const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= a.n_nodes || a.child[k] >= 0 || !(node_mass(a.rec, k) > 0.0)) return;
+    if (k >= list_nodes(a) || a.child[k] >= 0 || !(node_mass(a.rec, k) > 0.0)) return;
     const int b = a.beg[k], e = a.end[k];
     a.start_flag[b] = 1;
     for (int p = b; p < e; ++p) a.keep[p] = 1;
@@ -337,7 +344,7 @@ __global__ void __launch_bounds__(256) leaf_mark_kernel(const TreeListArgs a) {
 
 __global__ void __launch_bounds__(256) leaf_emit_kernel(const TreeListArgs a) {
     const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= a.n_nodes || a.child[k] >= 0 || !(node_mass(a.rec, k) > 0.0)) return;
+    if (k >= list_nodes(a) || a.child[k] >= 0 || !(node_mass(a.rec, k) > 0.0)) return;
     const int b = a.beg[k], e = a.end[k];
     const int o = a.start_ord[b];
     a.leaf_node[o] = k;
@@ -349,7 +356,7 @@ __global__ void __launch_bounds__(256) leaf_emit_kernel(const TreeListArgs a) {
 
 __global__ void __launch_bounds__(256) walk_pack_kernel(const TreeListArgs a) {
     const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= a.n_nodes) return;
+    if (k >= list_nodes(a)) return;
     WalkNode w;
     w.cx = a.cx[k];
     w.cy = a.cy[k];
@@ -439,6 +446,7 @@ template <bool FILL>
 __global__ void __launch_bounds__(kWalkThreads, 8) walk_kernel(const TreeListArgs a) {
     constexpr int W = kWalkThreads / 32;
     __shared__ __align__(16) int s_stk[W][kWalkStack];
+    if (FILL && a.overflow && *a.overflow) return;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int l = blockIdx.x * W + wid;
     const int n_leaves = a.start_ord[a.n];
@@ -646,7 +654,7 @@ __global__ void __launch_bounds__(1024) long_sort_kernel(const TreeListArgs a) {
 
 __global__ void __launch_bounds__(256) items_kernel(const TreeListArgs a, int n_leaves) {
     const int l = blockIdx.x * 256 + threadIdx.x;
-    if (l >= n_leaves) return;
+    if (l >= min(n_leaves, a.start_ord[a.n]) || (a.overflow && *a.overflow)) return;
     const int nch = a.item_cnt[l];
     const int fb = a.far_off[l], fe = a.far_off[l + 1];
     M2PItem* items = (M2PItem*)a.items;
@@ -664,13 +672,37 @@ __global__ void __launch_bounds__(256) items_kernel(const TreeListArgs a, int n_
 }
 
 // Far-field items, largest first (cost = targets x nodes): fewer long items at the tail.
+// Sort keys: cost + 1 for the real items (n_real of them, from the device count when given),
+// 0 for the rest of the capacity, so that the real items come first in decreasing cost.
 __global__ void __launch_bounds__(256) item_cost_kernel(const M2PItem* items, const int32_t* leaf_off, int n,
+                                                        const unsigned long long* n_real, const int* overflow,
                                                         uint32_t* cost, int32_t* idx) {
     const int k = blockIdx.x * 256 + threadIdx.x;
     if (k >= n) return;
-    const M2PItem it = items[k];
-    cost[k] = (uint32_t)(leaf_off[it.leaf + 1] - leaf_off[it.leaf]) * (uint32_t)(it.fe - it.fb);
+    const int real = (overflow && *overflow) ? 0 : n_real ? (int)min(*n_real, (unsigned long long)n) : n;
+    uint32_t c = 0;
+    if (k < real) {
+        const M2PItem it = items[k];
+        c = (uint32_t)(leaf_off[it.leaf + 1] - leaf_off[it.leaf]) * (uint32_t)(it.fe - it.fb) + 1u;
+    }
+    cost[k] = c;
     idx[k] = k;
+}
+
+// Marks an overflow when a list or item pool reserved by capacity is too small for this
+// evaluation's totals, or the topology build could not complete on the device.
+__global__ void pool_check_kernel(const TreeListArgs a, const int32_t* tree_hdr) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const unsigned long long* t = a.totals;
+    if (a.need) {
+        atomicMax(&a.need[0], (unsigned long long)(tree_hdr[0] > 0 ? tree_hdr[0] : 0));
+        for (int k = 0; k < 4; ++k) atomicMax(&a.need[1 + k], t[k]);
+    }
+    if (t[0] > (unsigned long long)a.far_cap || t[1] > (unsigned long long)a.near_cap ||
+        t[2] > (unsigned long long)a.item_cap || t[3] > (unsigned long long)a.slot_cap || tree_hdr[2] != 0) {
+        *a.overflow = 1;
+        if (a.overflow_sticky) atomicOr(a.overflow_sticky, tree_hdr[2] & 1 ? 3 : 1);  // bit 1: too deep
+    }
 }
 
 __global__ void __launch_bounds__(256) item_gather_kernel(const M2PItem* items, const int32_t* idx, int n,
@@ -794,6 +826,11 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     return cudaSuccess;
 }
 
+cudaError_t launch_pool_check(const TreeListArgs& a, const int32_t* tree_hdr, cudaStream_t st) {
+    pool_check_kernel<<<1, 32, 0, st>>>(a, tree_hdr);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st) {
     if (n_leaves == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(a.long_count, 0, sizeof(int), st);
@@ -812,12 +849,13 @@ size_t item_order_temp_bytes(int32_t n_items) {
     return b;
 }
 
-cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int32_t n_items, uint32_t* cost,
+cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int32_t n_items,
+                              const unsigned long long* n_real, const int* overflow, uint32_t* cost,
                               uint32_t* cost_alt, int32_t* idx, int32_t* idx_alt, void* temp, size_t temp_bytes,
                               M2PItem* out, cudaStream_t st) {
     if (n_items == 0) return cudaSuccess;
     const int g = (n_items + 255) / 256;
-    item_cost_kernel<<<g, 256, 0, st>>>(items, leaf_off, n_items, cost, idx);
+    item_cost_kernel<<<g, 256, 0, st>>>(items, leaf_off, n_items, n_real, overflow, cost, idx);
     cub::DoubleBuffer<uint32_t> k(cost, cost_alt);
     cub::DoubleBuffer<int32_t> v(idx, idx_alt);
     cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, temp_bytes, k, v, n_items, 0, 32, st);

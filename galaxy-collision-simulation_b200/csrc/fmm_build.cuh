@@ -98,16 +98,32 @@ struct TreeListArgs {
     int32_t* far_node;
     int32_t* near_leaf;
     void* items;  // M2PItem
+    // Capacity mode (nullable cnt_nodes / overflow): n_nodes is the capacity of the node
+    // arrays and the count is read on the device (cnt_nodes = the topology build's header
+    // {nodes, levels, flags}; a flag leaves no nodes); far/near/item/slot pools were reserved
+    // by capacity, pool_check marks an overflow when a total exceeds its pool (and records the
+    // largest totals seen in need[5], with a sticky copy of the flag), and the fill pass and
+    // everything after it are skipped.
+    const int32_t* cnt_nodes;
+    int* overflow;
+    int* overflow_sticky;
+    unsigned long long* need;  // {nodes, far, near, items, slots}
+    int64_t far_cap, near_cap, item_cap, slot_cap;
 };
 size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes);
 // Leaf compaction, the count walk and the offsets (sizes become known on the host after it).
 cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
+// Capacity mode: after the count pass, the overflow check of the pools (and of the topology
+// build's header tree_hdr).
+cudaError_t launch_pool_check(const TreeListArgs& a, const int32_t* tree_hdr, cudaStream_t st);
 // The fill walk (each leaf's lists sorted into depth-first order) and the far-field work items.
 cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st);
 // The far-field items reordered by decreasing cost (targets x nodes) into out.
 struct M2PItem;
 size_t item_order_temp_bytes(int32_t n_items);
-cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int32_t n_items, uint32_t* cost,
+// n_items is the length of the arrays; n_real (nullable: all) the items on the device.
+cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int32_t n_items,
+                              const unsigned long long* n_real, const int* overflow, uint32_t* cost,
                               uint32_t* cost_alt, int32_t* idx, int32_t* idx_alt, void* temp, size_t temp_bytes,
                               M2PItem* out, cudaStream_t st);
 

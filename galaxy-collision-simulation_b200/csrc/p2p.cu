@@ -57,7 +57,8 @@ std::atomic<int> g_p2p_tpt{0};          // 0: the default shape; 2 or 4: forced 
 __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exact, int64_t item_cost) {
     const int l = (int)((blockIdx.x * 256u + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (l > a.n_leaves) return;
-    if (l == a.n_leaves) {
+    const int nl = p2p_leaves_now(a);
+    if (l >= nl) {  // past the last leaf (up to the capacity): no work, so the scans end with the totals
         if (lane == 0) {
             a.plan_cnt[l] = 0;
             a.plan_need[l] = 0;
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exa
             const int64_t c_cost = (src * (g + kStageCost) + item_cost - 1) / item_cost;
             const int64_t c_src = (src + kMinChunk - 1) / kMinChunk;
             chunks = (int)max((int64_t)1, min((int64_t)kMaxChunks, min(c_cost, c_src)));
-            if (a.leaf_off[a.n_leaves] > a.split_max_slots) chunks = 1;
+            if (a.leaf_off[nl] > a.split_max_slots) chunks = 1;
         }
     }
     a.plan_src[l] = src;
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exa
 // item offsets, which dominated items of small leaves.
 __global__ void __launch_bounds__(256) p2p_item_leaf_kernel(const P2PArgs a) {
     const int l = blockIdx.x * 256 + threadIdx.x;
-    if (l >= a.n_leaves) return;
+    if (l >= p2p_leaves_now(a)) return;
     const int b = a.plan_item_off[l], c = a.plan_cnt[l];
     for (int k = 0; k < c && b + k < a.plan_item_cap; ++k) a.plan_item_leaf[b + k] = l;
 }
@@ -110,7 +111,8 @@ __global__ void __launch_bounds__(256) p2p_item_leaf_kernel(const P2PArgs a) {
 // leaf slot k, when the slots fit the buffer (cap of them; a CSR that lists a body in
 // several leaves can have more, and the leaf kernel then reads through leaf_part).
 __global__ void __launch_bounds__(256) p2p_gather_kernel(const P2PArgs a, int64_t cap) {
-    const int64_t np = a.leaf_off[a.n_leaves];
+    const int nl = p2p_leaves_now(a);
+    const int64_t np = nl > 0 ? a.leaf_off[nl] : 0;
     const bool ok = np <= cap;
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.src_ok = ok ? 1 : 0;
     if (!ok) return;
@@ -120,9 +122,26 @@ __global__ void __launch_bounds__(256) p2p_gather_kernel(const P2PArgs a, int64_
     }
 }
 
-// Resident threads per SM the launch bounds ask for: 640 (20 warps, 96 registers) with two
-// targets per thread; with four, 512 in the mixed form (128 registers) and 384 in FP64 (168
-// registers: four FP64 chains per thread in place of warps).
+// Asynchronous global -> shared copies (cp.async): the staging of the next pass of sources is
+// in flight while the current pass is computed, without holding the data in registers.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Resident threads per SM the launch bounds ask for: 640 (20 warps) with two targets per
+// thread; with four, 512 in the mixed form and 384 in FP64 (four FP64 chains per thread in
+// place of warps).
 constexpr int p2p_threads_per_sm(int mode, int tpt) { return tpt == 2 ? 640 : mode == kMixed ? 512 : 384; }
 
 // BS threads per block (a multiple of 32), 4 x BS sources staged per pass, TPT targets per
@@ -132,40 +151,45 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
     constexpr int kP2PBlock = BS;
     constexpr int kP2PJT = 4 * BS;  // sources staged per shared-memory pass
     static_assert(TPT == 2 || TPT == 4, "two or four targets per thread");
-    // FP64 forms: x, y, z, m as four arrays of kP2PJT doubles.  Mixed form: the same bytes
-    // as float4 (x, x, y, y)[kP2PJT] then (z, z, m, m)[kP2PJT] -- every source duplicated so
-    // that one 16-byte load gives a packed pair per coordinate (two targets per f32x2 op).
-    __shared__ __align__(16) double sbuf[4 * kP2PJT];
-    double* const sxd = sbuf;
-    double* const syd = sbuf + kP2PJT;
-    double* const szd = sbuf + 2 * kP2PJT;
-    double* const smd = sbuf + 3 * kP2PJT;
-    float4* const sA = reinterpret_cast<float4*>(sbuf);
-    float4* const sB = sA + kP2PJT;
-    __shared__ int sidx[kP2PJT];
+    // Sources of a pass arrive as (x, y), (z, m) double pairs by cp.async.  FP64 forms read
+    // them there, from two buffers: pass k + 1 is copied into one while pass k is read from
+    // the other.  The mixed form copies into one raw buffer and each thread converts its own
+    // slots into FP32 offsets, stored by source PAIR -- (x0, x1, y0, y1), (z0, z1, m0, m1) -- in
+    // two packed buffers: one 16-byte load gives every coordinate of two sources as packed
+    // pairs, so each target (held duplicated) takes two interactions per f32x2 instruction.
+    // A thread stages kStageU consecutive slots; the raw buffers hold slot c of thread
+    // t = c / kStageU, u = c mod kStageU at raw_at(c) = u x block + (t + 2u) mod block: the
+    // lanes of a warp copy to (and convert from) consecutive 16-byte words, and the runs of
+    // consecutive slots that the FP64 forms read together spread over the 8 groups of 4
+    // banks (11 consecutive slots: at most 2 in a group, as in a linear layout).
+    constexpr int kRawBufs = MODE == kMixed ? 1 : 2;
+    constexpr int kPairs = kP2PJT / 2;
+    constexpr int kStageU = kP2PJT / kP2PBlock;  // slots a thread stages per pass
+    __shared__ __align__(16) double2 sraw[kRawBufs][2][kP2PJT];
+    __shared__ __align__(16) float4 spk[MODE == kMixed ? 2 : 1][MODE == kMixed ? 2 * kPairs : 1];
+    // source body indices: raw order (FP64 forms: one per raw buffer; mixed: the third), and
+    // in the mixed form pair order (the first two, one per packed buffer)
+    __shared__ __align__(8) int sidx[MODE == kMixed ? 3 : 2][kP2PJT];
     __shared__ int s_beg[kNearBatch];
     __shared__ int s_pre[kNearBatch + 1];
-    __shared__ double s_red[3 * TPT][kP2PBlock];
     __shared__ int s_item, s_last;
+    // row partial sums of the fast forms, in the raw buffer (free once a sweep has ended)
+    static_assert(sizeof(sraw) >= 3 * TPT * kP2PBlock * sizeof(double), "row sums fit the raw buffer");
+    double* const s_red = reinterpret_cast<double*>(&sraw[0][0][0]);
+    auto raw_at = [](int c) { return (c % kStageU) * kP2PBlock + (c / kStageU + 2 * (c % kStageU)) % kP2PBlock; };
 
     // body indices of the staged sources are needed only to skip the target itself where a
     // zero distance does not already give a zero term
     constexpr bool kNeedIdx = MODE == kF64Exact || EPS0;
-    constexpr int kStageU = kP2PJT / kP2PBlock;  // slots a thread stages per pass
     const int tid = threadIdx.x;
     const int n_items = *a.plan_n_items;
     const bool by_slot = *a.src_ok != 0;
-    // The next item's ticket is taken while the current item runs (thread 0 reads the
-    // atomic's result only when the item is done), so its latency is not paid per item.
-    int next = 0;
-    if (tid == 0) next = atomicAdd(a.ticket, 1);
     for (;;) {
-        if (tid == 0) s_item = next;
+        if (tid == 0) s_item = atomicAdd(a.ticket, 1);
         __syncthreads();
         const int item = s_item;
         __syncthreads();
         if (item >= n_items) return;
-        if (tid == 0) next = atomicAdd(a.ticket, 1);
         // leaf owning the item: one load from the table p2p_item_leaf_kernel filled; items past
         // the table (possible only with device CSR arrays that repeat bodies) search the offsets
         int leaf;
@@ -198,23 +222,77 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
         const int first = a.leaf_part[tb];
         const double ox = a.x[first], oy = a.y[first], oz = a.z[first];
 
-        auto stage = [&](int c, const double4 q, int j) {
-            if (kNeedIdx) sidx[c] = j;
-            if (MODE == kMixed) {
-                const float fx = __double2float_rn(q.x - ox), fy = __double2float_rn(q.y - oy);
-                const float fz = __double2float_rn(q.z - oz), fm = __double2float_rn(q.w);
-                sA[c] = make_float4(fx, fx, fy, fy);
-                sB[c] = make_float4(fz, fz, fm, fm);
-            } else {
-                sxd[c] = q.x;
-                syd[c] = q.y;
-                szd[c] = q.z;
-                smd[c] = q.w;
+        // cp.async of this thread's slots of a pass: kStageU consecutive slots from
+        // c0 + kStageU * tid of the current near batch (s_pre / s_beg) into raw buffer rb and
+        // index buffer ib.  One binary search finds the near leaf of the first slot; the
+        // others are in the same leaf or a few leaves further.
+        auto issue = [&](int c0, int take, int rb, int ib, int cnt) {
+            const int cb = tid * kStageU;
+            if (cb < take) {
+                int l2 = 0, h2 = cnt;  // s_pre[l2] <= c0 + cb < s_pre[h2]
+                while (h2 - l2 > 1) {
+                    const int mid = (l2 + h2) >> 1;
+                    if (s_pre[mid] <= c0 + cb) l2 = mid;
+                    else h2 = mid;
+                }
+#pragma unroll
+                for (int u = 0; u < kStageU; ++u) {
+                    const int c = cb + u;
+                    if (c >= take) break;
+                    const int sl = c0 + c;
+                    while (s_pre[l2 + 1] <= sl) ++l2;  // sl < s_pre[cnt]: ends by l2 = cnt - 1
+                    const int pos = s_beg[l2] + (sl - s_pre[l2]);
+                    const int r = raw_at(c);
+                    double* dxy = reinterpret_cast<double*>(&sraw[rb][0][r]);
+                    double* dzm = reinterpret_cast<double*>(&sraw[rb][1][r]);
+                    if (by_slot) {
+                        const double* g = reinterpret_cast<const double*>(a.src + pos);
+                        cp_async16(dxy, g);
+                        cp_async16(dzm, g + 2);
+                        if (kNeedIdx) cp_async4(&sidx[ib][r], a.leaf_part + pos);
+                    } else {
+                        const int j = a.leaf_part[pos];
+                        cp_async8(dxy, a.x + j);
+                        cp_async8(dxy + 1, a.y + j);
+                        cp_async8(dzm, a.z + j);
+                        cp_async8(dzm + 1, a.m + j);
+                        if (kNeedIdx) sidx[ib][r] = j;
+                    }
+                }
+            }
+            cp_async_commit();
+        };
+        // Mixed form: this thread's slots of the pass, raw -> FP32 offsets in packed buffer pb,
+        // one 16-byte store per pair and array; an odd count is padded with a massless source
+        // far away (its term is exactly zero).
+        auto convert = [&](int take, int pb) {
+            static_assert(kStageU % 2 == 0, "a thread converts whole pairs");
+#pragma unroll
+            for (int k = 0; k < kStageU / 2; ++k) {
+                const int c = tid * kStageU + 2 * k;
+                if (c >= take) break;
+                const double2 a0 = sraw[0][0][raw_at(c)], b0 = sraw[0][1][raw_at(c)];
+                double2 a1 = make_double2(ox + 1e18, oy), b1 = make_double2(oz, 0.0);
+                if (c + 1 < take) {
+                    a1 = sraw[0][0][raw_at(c + 1)];
+                    b1 = sraw[0][1][raw_at(c + 1)];
+                }
+                if (kNeedIdx) {
+                    sidx[pb][c] = sidx[2][raw_at(c)];
+                    sidx[pb][c + 1] = c + 1 < take ? sidx[2][raw_at(c + 1)] : -1;
+                }
+                const float x0 = __double2float_rn(a0.x - ox), x1 = __double2float_rn(a1.x - ox);
+                const float y0 = __double2float_rn(a0.y - oy), y1 = __double2float_rn(a1.y - oy);
+                const float z0 = __double2float_rn(b0.x - oz), z1 = __double2float_rn(b1.x - oz);
+                spk[pb][c >> 1] = make_float4(x0, x1, y0, y1);
+                spk[pb][kPairs + (c >> 1)] = make_float4(z0, z1, __double2float_rn(b0.y), __double2float_rn(b1.y));
             }
         };
-        // Every source slot [c_lo, c_hi) of this item staged kP2PJT at a time, compute(take)
-        // after each: the near list is walked in batches, a warp scan of the near leaves'
-        // sizes lets every thread gather its own slots by index.
+        // Every source slot [c_lo, c_hi) of this item, kP2PJT per pass, compute(take, buf)
+        // on each: the near list is walked in batches, a warp scan of the near leaves' sizes
+        // lets every thread find its own slots.  One barrier per pass: after it the pass's
+        // buffer is complete and every thread has finished the previous pass, whose buffer
+        // then takes the copies of the next.
         auto sweep = [&](auto&& compute) {
             int64_t base = 0;  // slots before the current near batch
             for (int qb = nb; qb < ne && base < c_hi; qb += kNearBatch) {
@@ -245,48 +323,19 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                 // this batch covers slots [base, base + total) of the sequence; keep [c_lo, c_hi)
                 const int b_lo = (int)max((int64_t)0, c_lo - base);
                 const int b_hi = (int)min((int64_t)total, c_hi - base);
-                for (int c0 = b_lo; c0 < b_hi; c0 += kP2PJT) {
+                int buf = 0;
+                if (b_lo < b_hi) issue(b_lo, min(kP2PJT, b_hi - b_lo), 0, MODE == kMixed ? 2 : 0, cnt);
+                for (int c0 = b_lo; c0 < b_hi; c0 += kP2PJT, buf ^= 1) {
                     const int take = min(kP2PJT, b_hi - c0);
-                    // a thread's kStageU slots: positions first, then all loads, then the
-                    // stores, so that the loads of the slots are in flight together
-                    int pos[kStageU];
-#pragma unroll
-                    for (int u = 0; u < kStageU; ++u) {
-                        const int sl = c0 + tid + u * kP2PBlock;
-                        pos[u] = -1;
-                        if (tid + u * kP2PBlock < take) {
-                            int l2 = 0, h2 = cnt;  // s_pre[l2] <= sl < s_pre[h2]
-                            while (h2 - l2 > 1) {
-                                const int mid = (l2 + h2) >> 1;
-                                if (s_pre[mid] <= sl) l2 = mid;
-                                else h2 = mid;
-                            }
-                            pos[u] = s_beg[l2] + (sl - s_pre[l2]);
-                        }
-                    }
-                    double4 q[kStageU];
-                    int jx[kStageU];
-#pragma unroll
-                    for (int u = 0; u < kStageU; ++u) {
-                        if (pos[u] < 0) continue;
-                        if (by_slot) {
-                            q[u] = a.src[pos[u]];
-                            jx[u] = kNeedIdx ? a.leaf_part[pos[u]] : 0;
-                        } else {
-                            const int j = a.leaf_part[pos[u]];
-                            q[u] = make_double4(a.x[j], a.y[j], a.z[j], a.m[j]);
-                            jx[u] = j;
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < kStageU; ++u)
-                        if (pos[u] >= 0) stage(tid + u * kP2PBlock, q[u], jx[u]);
+                    cp_async_wait_all();
+                    if (MODE == kMixed) convert(take, buf);
                     __syncthreads();
-                    compute(take);
-                    __syncthreads();
+                    const int c1 = c0 + kP2PJT;
+                    if (c1 < b_hi) issue(c1, min(kP2PJT, b_hi - c1), kRawBufs == 2 ? buf ^ 1 : 0, MODE == kMixed ? 2 : buf ^ 1, cnt);
+                    compute(take, buf);
                 }
                 base += total;
-                __syncthreads();  // s_beg / s_pre are rewritten by the next batch
+                __syncthreads();  // s_beg / s_pre and the buffers are rewritten by the next batch
             }
         };
 
@@ -304,10 +353,14 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                     fy = a.ay[i];
                     fz = a.az[i];
                 }
-                sweep([&](int cnt) {
+                sweep([&](int cnt, int buf) {
+                    const int* I = sidx[buf];
                     for (int jj = 0; jj < cnt; ++jj) {
-                        if (sidx[jj] == i) continue;
-                        const double rx = dsub(sxd[jj], xi), ry = dsub(syd[jj], yi), rz = dsub(szd[jj], zi);
+                        const int r = raw_at(jj);
+                        if (I[r] == i) continue;
+                        const double2 xy = sraw[buf][0][r], zm = sraw[buf][1][r];
+                        const double4 q = make_double4(xy.x, xy.y, zm.x, zm.y);
+                        const double rx = dsub(q.x, xi), ry = dsub(q.y, yi), rz = dsub(q.z, zi);
                         const double s2 = dadd(dadd(dadd(dmul(rx, rx), dmul(ry, ry)), dmul(rz, rz)), a.eps2);
                         if (s2 == 0.0) {
                             fx = dadd(fx, 0.0);
@@ -317,7 +370,7 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                         }
                         const double inv = __ddiv_rn(1.0, __dsqrt_rn(s2));
                         const double inv3 = dmul(dmul(inv, inv), inv);
-                        const double scale = dmul(dmul(a.G, smd[jj]), inv3);
+                        const double scale = dmul(dmul(a.G, q.w), inv3);
                         fx = dadd(fx, dmul(rx, scale));
                         fy = dadd(fy, dmul(ry, scale));
                         fz = dadd(fz, dmul(rz, scale));
@@ -356,18 +409,21 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
 #pragma unroll
                 for (int k = 0; k < 3 * TPT; ++k) f[k] = 0.0;
                 if constexpr (MODE == kF64) {
-                    sweep([&](int cnt) {
+                    sweep([&](int cnt, int buf) {
                         if (!act) return;
+                        const int* I = sidx[buf];
 #pragma unroll 2
                         for (int jj = lane; jj < cnt; jj += L) {
-                            const double qx = sxd[jj], qy = syd[jj], qz = szd[jj], qm = smd[jj];
+                            const int r = raw_at(jj);
+                            const double2 xy = sraw[buf][0][r], zm = sraw[buf][1][r];
+                            const double4 q = make_double4(xy.x, xy.y, zm.x, zm.y);
 #pragma unroll
                             for (int h = 0; h < TPT; ++h) {
-                                const double dx = qx - xt[h], dy = qy - yt[h], dz = qz - zt[h];
-                                const double r = fma(dz, dz, fma(dy, dy, fma(dx, dx, a.eps2)));
-                                double y = rsqrt_f64(r);
-                                if (EPS0) y = (r == 0.0 || sidx[jj] == ti[h]) ? 0.0 : y;
-                                const double w = qm * (y * y * y);
+                                const double dx = q.x - xt[h], dy = q.y - yt[h], dz = q.z - zt[h];
+                                const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, a.eps2)));
+                                double y = rsqrt_f64(r2);
+                                if (EPS0) y = (r2 == 0.0 || I[r] == ti[h]) ? 0.0 : y;
+                                const double w = q.w * (y * y * y);
                                 f[3 * h] = fma(dx, w, f[3 * h]);
                                 f[3 * h + 1] = fma(dy, w, f[3 * h + 1]);
                                 f[3 * h + 2] = fma(dz, w, f[3 * h + 2]);
@@ -375,33 +431,41 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                         }
                     });
                 } else {
-                    constexpr int NP = TPT / 2;  // packed target pairs
-                    f2 XI[NP], YI[NP], ZI[NP];
+                    // every target duplicated into both halves of its packed registers
+                    f2 XI[TPT], YI[TPT], ZI[TPT];
 #pragma unroll
-                    for (int q = 0; q < NP; ++q) {
-                        XI[q] = pk2(__double2float_rn(xt[2 * q] - ox), __double2float_rn(xt[2 * q + 1] - ox));
-                        YI[q] = pk2(__double2float_rn(yt[2 * q] - oy), __double2float_rn(yt[2 * q + 1] - oy));
-                        ZI[q] = pk2(__double2float_rn(zt[2 * q] - oz), __double2float_rn(zt[2 * q + 1] - oz));
+                    for (int h = 0; h < TPT; ++h) {
+                        const float fx = __double2float_rn(xt[h] - ox), fy = __double2float_rn(yt[h] - oy);
+                        const float fz = __double2float_rn(zt[h] - oz);
+                        XI[h] = pk2(fx, fx);
+                        YI[h] = pk2(fy, fy);
+                        ZI[h] = pk2(fz, fz);
                     }
                     const f2 E2 = pk2(a.eps2f, a.eps2f);
                     CompF c[3 * TPT];
 #pragma unroll
                     for (int k = 0; k < 3 * TPT; ++k) c[k].init();
-                    sweep([&](int cnt) {
+                    sweep([&](int cnt, int buf) {
                         if (!act) return;
-                        f2 PX[NP], PY[NP], PZ[NP];
+                        const float4* PA = &spk[buf][0];
+                        const float4* PB = &spk[buf][kPairs];
+                        const int2* I2 = reinterpret_cast<const int2*>(sidx[buf]);
+                        f2 PX[TPT], PY[TPT], PZ[TPT];
 #pragma unroll
-                        for (int q = 0; q < NP; ++q) PX[q] = PY[q] = PZ[q] = pk2(0.f, 0.f);
+                        for (int h = 0; h < TPT; ++h) PX[h] = PY[h] = PZ[h] = pk2(0.f, 0.f);
+                        const int np = (cnt + 1) >> 1;
 #pragma unroll 2
-                        for (int jj = lane; jj < cnt; jj += L) {
+                        for (int pp = lane; pp < np; pp += L) {
                             f2 X, Y, Z, M;
-                            lds_v2b64(reinterpret_cast<const float*>(&sA[jj]), X, Y);
-                            lds_v2b64(reinterpret_cast<const float*>(&sB[jj]), Z, M);
+                            lds_v2b64(reinterpret_cast<const float*>(&PA[pp]), X, Y);
+                            lds_v2b64(reinterpret_cast<const float*>(&PB[pp]), Z, M);
+                            int2 jj2 = make_int2(-1, -1);
+                            if (EPS0) jj2 = I2[pp];
 #pragma unroll
-                            for (int q = 0; q < NP; ++q) {
-                                const f2 dX = sub2(X, XI[q]);
-                                const f2 dY = sub2(Y, YI[q]);
-                                const f2 dZ = sub2(Z, ZI[q]);
+                            for (int h = 0; h < TPT; ++h) {
+                                const f2 dX = sub2(X, XI[h]);
+                                const f2 dY = sub2(Y, YI[h]);
+                                const f2 dZ = sub2(Z, ZI[h]);
                                 f2 R = fma2(dX, dX, E2);
                                 R = fma2(dY, dY, R);
                                 R = fma2(dZ, dZ, R);
@@ -409,30 +473,27 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                                 upk2(R, r0, r1);
                                 float i0 = rsqrt_f32(r0), i1 = rsqrt_f32(r1);
                                 if (EPS0) {
-                                    i0 = (r0 == 0.f || sidx[jj] == ti[2 * q]) ? 0.f : i0;
-                                    i1 = (r1 == 0.f || sidx[jj] == ti[2 * q + 1]) ? 0.f : i1;
+                                    i0 = (r0 == 0.f || jj2.x == ti[h]) ? 0.f : i0;
+                                    i1 = (r1 == 0.f || jj2.y == ti[h]) ? 0.f : i1;
                                 }
                                 const f2 I = pk2(i0, i1);
                                 f2 T = mul2(I, I);
                                 T = mul2(T, I);
                                 const f2 W = mul2(M, T);
-                                PX[q] = fma2(dX, W, PX[q]);
-                                PY[q] = fma2(dY, W, PY[q]);
-                                PZ[q] = fma2(dZ, W, PZ[q]);
+                                PX[h] = fma2(dX, W, PX[h]);
+                                PY[h] = fma2(dY, W, PY[h]);
+                                PZ[h] = fma2(dZ, W, PZ[h]);
                             }
                         }
 #pragma unroll
-                        for (int q = 0; q < NP; ++q) {
+                        for (int h = 0; h < TPT; ++h) {  // the pass's two halves, then the compensated sum
                             float p0, p1;
-                            upk2(PX[q], p0, p1);
-                            c[6 * q].add(p0);
-                            c[6 * q + 3].add(p1);
-                            upk2(PY[q], p0, p1);
-                            c[6 * q + 1].add(p0);
-                            c[6 * q + 4].add(p1);
-                            upk2(PZ[q], p0, p1);
-                            c[6 * q + 2].add(p0);
-                            c[6 * q + 5].add(p1);
+                            upk2(PX[h], p0, p1);
+                            c[3 * h].add(p0 + p1);
+                            upk2(PY[h], p0, p1);
+                            c[3 * h + 1].add(p0 + p1);
+                            upk2(PZ[h], p0, p1);
+                            c[3 * h + 2].add(p0 + p1);
                         }
                     });
 #pragma unroll
@@ -440,7 +501,7 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                 }
                 if (act)
 #pragma unroll
-                    for (int k = 0; k < 3 * TPT; ++k) s_red[k][tid] = f[k];
+                    for (int k = 0; k < 3 * TPT; ++k) s_red[k * kP2PBlock + tid] = f[k];
                 __syncthreads();
                 if (act && lane == 0) {
                     double S[3 * TPT];
@@ -448,7 +509,7 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                     for (int k = 0; k < 3 * TPT; ++k) S[k] = 0.0;
                     for (int q = 0; q < L; ++q)
 #pragma unroll
-                        for (int k = 0; k < 3 * TPT; ++k) S[k] += s_red[k][tid + q];
+                        for (int k = 0; k < 3 * TPT; ++k) S[k] += s_red[k * kP2PBlock + tid + q];
 #pragma unroll
                     for (int h = 0; h < TPT; ++h) {
                         if (!has[h]) continue;
@@ -590,7 +651,8 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     // Block size: with few bodies per leaf a leaf's item is small, and one-warp blocks (20
     // independent warps per SM, no block-wide barriers) hide the latency of its gathers;
     // larger leaves keep 4-warp blocks that share each staged source among more threads.
-    const int bs = n_bodies <= (int64_t)kWarpBlockMaxMean * a.n_leaves ? 32 : 128;
+    const int leaves_est = a.leaves_hint > 0 ? a.leaves_hint : a.n_leaves;
+    const int bs = n_bodies <= (int64_t)kWarpBlockMaxMean * leaves_est ? 32 : 128;
     // Targets per thread: two.  Four (two packed pairs per staged source in the mixed form,
     // four FP64 chains per thread) measured 2-40% slower at every size and leaf capacity
     // tried (N = 65,536 and 2^20, leaf 16 and 64); the shape stays selectable for measurement.

@@ -42,7 +42,18 @@ struct P2PArgs {
     int* src_ok;
     double* scratch;
     int64_t split_max_slots;  // leaves are split only if their slots number at most this
+    // Capacity mode (nullable): the leaf count on the device (n_leaves is then the capacity
+    // of the leaf arrays), an overflow flag that turns the launch into a no-op, and the
+    // expected leaf count for the choice of block size.
+    const int32_t* cnt_leaves;
+    const int* overflow;
+    int32_t leaves_hint;
 };
+
+__device__ __forceinline__ int p2p_leaves_now(const P2PArgs& a) {
+    if (a.overflow && *a.overflow) return 0;
+    return a.cnt_leaves ? min(*a.cnt_leaves, a.n_leaves) : a.n_leaves;
+}
 
 // Targets per thread of the fast forms: 2 or 4 forces that many, 0 restores the choice by
 // mean leaf size (for measurements).

@@ -42,6 +42,7 @@ constexpr int kSmallWarps = kSmallThreads / 32;
 constexpr int kSmallJT = 512;  // sources staged per shared-memory pass
 constexpr size_t kSmallHeader = 256;  // barrier words + status, then the position buffers
 std::atomic<int> g_small_tpw{0};      // 0: chosen from n; 1, 2 or 4: forced (measurement)
+std::atomic<int> g_small_wpt{0};      // 0: chosen; 1 or 2 warps per target: forced (measurement)
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -97,8 +98,14 @@ __device__ bool grid_barrier(const SmallArgs& a, unsigned& gen) {
     return s_ok != 0;
 }
 
-template <int PREC, int TPW, bool EPS0>
-__global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const SmallArgs a) {
+// WPT warps per target slot (FP64 form): the slot's sources are split over its warps and the
+// warps' sums are added in warp order through shared memory, so each warp has half (a
+// quarter) of the dependent pair terms to run per step.  256 x WPT threads per CTA.
+template <int PREC, int TPW, bool EPS0, int WPT>
+__global__ void __launch_bounds__(kSmallThreads * WPT, 1) small_steps_kernel(const SmallArgs a) {
+    constexpr int kBlock = kSmallThreads * WPT;
+    static_assert(PREC == kF64 || WPT == 1, "the exact form sums each target in one warp");
+    __shared__ double s_part[WPT > 1 ? kSmallWarps * WPT * TPW * 3 : 1];
     __shared__ __align__(16) double sx[kSmallJT];
     __shared__ __align__(16) double sy[kSmallJT];
     __shared__ __align__(16) double sz[kSmallJT];
@@ -108,8 +115,9 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
     double* const s_con = s_con_all + (PREC == kF64Exact ? (threadIdx.x >> 5) * TPW * 96 : 0);
     const int lane = threadIdx.x & 31;
     const int n = a.n;
-    const int total_warps = gridDim.x * kSmallWarps;
-    const int w = blockIdx.x * kSmallWarps + (threadIdx.x >> 5);
+    const int total_warps = gridDim.x * kSmallWarps;  // target slots of the grid
+    const int slot = (threadIdx.x >> 5) / WPT, part = (threadIdx.x >> 5) % WPT;
+    const int w = blockIdx.x * kSmallWarps + slot;
     const double h = 0.5 * a.dt, dt = a.dt, G = a.G, e2 = a.eps2;
 
     int T[TPW];
@@ -139,7 +147,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
             X[k] = dadd(X[k], dmul(U[k], dt));
             Y[k] = dadd(Y[k], dmul(V[k], dt));
             Z[k] = dadd(Z[k], dmul(W[k], dt));
-            if (lane == 0) {
+            if (lane == 0 && part == 0) {
                 px[T[k]] = X[k];
                 py[T[k]] = Y[k];
                 pz[T[k]] = Z[k];
@@ -153,7 +161,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
         for (int k = 0; k < TPW; ++k) fx[k] = fy[k] = fz[k] = 0.0;
         for (int j0 = 0; j0 < n; j0 += kSmallJT) {
             const int cnt = min(kSmallJT, n - j0);
-            for (int jj = threadIdx.x; jj < cnt; jj += kSmallThreads) {
+            for (int jj = threadIdx.x; jj < cnt; jj += kBlock) {
                 sx[jj] = __ldcg(px + j0 + jj);
                 sy[jj] = __ldcg(py + j0 + jj);
                 sz[jj] = __ldcg(pz + j0 + jj);
@@ -162,7 +170,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
             __syncthreads();
             if constexpr (PREC == kF64) {
 #pragma unroll 4
-                for (int jj = lane; jj < cnt; jj += 32) {
+                for (int jj = part * 32 + lane; jj < cnt; jj += 32 * WPT) {
                     const double qx = sx[jj], qy = sy[jj], qz = sz[jj], qm = sm[jj];
 #pragma unroll
                     for (int k = 0; k < TPW; ++k) {
@@ -219,30 +227,65 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
             __syncthreads();
         }
         // results and the closing kick (dt/2)
+        if constexpr (PREC == kF64) {
 #pragma unroll
-        for (int k = 0; k < TPW; ++k) {
-            if constexpr (PREC == kF64) {
+            for (int k = 0; k < TPW; ++k) {
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {
                     fx[k] += __shfl_xor_sync(0xffffffffu, fx[k], o);
                     fy[k] += __shfl_xor_sync(0xffffffffu, fy[k], o);
                     fz[k] += __shfl_xor_sync(0xffffffffu, fz[k], o);
                 }
+                if constexpr (WPT > 1) {
+                    double* mine = s_part + ((slot * WPT + part) * TPW + k) * 3;
+                    if (lane == 0) {
+                        mine[0] = fx[k];
+                        mine[1] = fy[k];
+                        mine[2] = fz[k];
+                    }
+                }
+            }
+            if constexpr (WPT > 1) {  // the slot's warps' sums, added in warp order by each of them
+                __syncthreads();
+#pragma unroll
+                for (int k = 0; k < TPW; ++k) {
+                    const double* p0 = s_part + ((slot * WPT) * TPW + k) * 3;
+                    double sx = p0[0], sy = p0[1], sz = p0[2];
+#pragma unroll
+                    for (int q = 1; q < WPT; ++q) {
+                        const double* pq = p0 + q * TPW * 3;
+                        sx += pq[0];
+                        sy += pq[1];
+                        sz += pq[2];
+                    }
+                    fx[k] = sx;
+                    fy[k] = sy;
+                    fz[k] = sz;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < TPW; ++k) {
                 AX[k] = G * fx[k];
                 AY[k] = G * fy[k];
                 AZ[k] = G * fz[k];
-            } else {  // lane c holds component c
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < TPW; ++k) {  // lane c holds component c
                 AX[k] = __shfl_sync(0xffffffffu, fx[k], 0);
                 AY[k] = __shfl_sync(0xffffffffu, fx[k], 1);
                 AZ[k] = __shfl_sync(0xffffffffu, fx[k], 2);
             }
+        }
+#pragma unroll
+        for (int k = 0; k < TPW; ++k) {
             if (T[k] >= n) continue;
             U[k] = dadd(U[k], dmul(AX[k], h));
             V[k] = dadd(V[k], dmul(AY[k], h));
             W[k] = dadd(W[k], dmul(AZ[k], h));
         }
     }
-    if (lane == 0) {
+    if (lane == 0 && part == 0) {
 #pragma unroll
         for (int k = 0; k < TPW; ++k) {
             const int t = T[k];
@@ -254,18 +297,19 @@ __global__ void __launch_bounds__(kSmallThreads, 1) small_steps_kernel(const Sma
     }
 }
 
-template <int PREC, bool EPS0>
+template <int PREC, bool EPS0, int WPT>
 const void* pick(int tpw) {
     switch (tpw) {
-        case 1: return (const void*)&small_steps_kernel<PREC, 1, EPS0>;
-        case 2: return (const void*)&small_steps_kernel<PREC, 2, EPS0>;
-        default: return (const void*)&small_steps_kernel<PREC, 4, EPS0>;
+        case 1: return (const void*)&small_steps_kernel<PREC, 1, EPS0, WPT>;
+        case 2: return (const void*)&small_steps_kernel<PREC, 2, EPS0, WPT>;
+        default: return (const void*)&small_steps_kernel<PREC, 4, EPS0, WPT>;
     }
 }
 
 }  // namespace
 
 void small_set_targets_per_warp(int tpw) { g_small_tpw.store(tpw == 1 || tpw == 2 || tpw == 4 ? tpw : 0); }
+void small_set_warps_per_target(int wpt) { g_small_wpt.store(wpt == 1 || wpt == 2 ? wpt : 0); }
 
 size_t small_scratch_bytes(int n) { return kSmallHeader + (size_t)6 * (size_t)n * sizeof(double); }
 
@@ -283,24 +327,39 @@ cudaError_t small_steps_launch(const SmallArgs& a, int precision, bool eps0, int
     if (e != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
     if (!coop) return cudaErrorNotSupported;
-    // Targets per warp: the fewest that let one CTA per SM cover every body (measured on B200
-    // at n = 1000: one target per warp on 125 SMs 1.4x faster than two on 63, 2.1x than four).
-    int tpw = g_small_tpw.load();
-    if (tpw == 0) {
-        tpw = 1;
-        while (tpw < 4 && (int64_t)sms * kSmallWarps * tpw < a.n) tpw *= 2;
+    // Shape: targets per warp (tpw) and, in the FP64 form, warps per target (wpt), the first
+    // of (1, 2), (1, 1), (2, 2), (2, 1), (4, 2), (4, 1) whose grid is co-resident.  Measured on
+    // B200 (steps/s of the FP64 form): n = 1000: 155k at (1, 2), 128k at (1, 1), 111k at
+    // (2, 2), 90k at (2, 1); n = 4096: 26.4k at (2, 1) and (2, 2), 18.8k at (4, 1).  Forced
+    // shapes (measurement knobs) skip the others.
+    const int f_tpw = g_small_tpw.load(), f_wpt = g_small_wpt.load();
+    const void* fn = nullptr;
+    int blocks = 0, threads = 0;
+    for (int tpw : {1, 2, 4}) {
+        if (f_tpw && tpw != f_tpw) continue;
+        for (int wpt : {2, 1}) {
+            if (precision == kF64Exact ? wpt != 1 : (f_wpt && wpt != f_wpt)) continue;  // exact: one warp
+            const void* g;
+            if (precision == kF64Exact) g = pick<kF64Exact, true, 1>(tpw);
+            else if (wpt == 2) g = eps0 ? pick<kF64, true, 2>(tpw) : pick<kF64, false, 2>(tpw);
+            else g = eps0 ? pick<kF64, true, 1>(tpw) : pick<kF64, false, 1>(tpw);
+            const int b = (a.n + kSmallWarps * tpw - 1) / (kSmallWarps * tpw);
+            int occ = 0;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, g, kSmallThreads * wpt, 0)) != cudaSuccess)
+                return e;
+            if ((int64_t)occ * sms < b) continue;
+            fn = g;
+            blocks = b;
+            threads = kSmallThreads * wpt;
+            break;
+        }
+        if (fn) break;
     }
-    if ((int64_t)sms * kSmallWarps * tpw < a.n) return cudaErrorNotSupported;
-    const int blocks = (a.n + kSmallWarps * tpw - 1) / (kSmallWarps * tpw);
-    const void* fn = precision == kF64Exact ? pick<kF64Exact, true>(tpw)
-                                            : (eps0 ? pick<kF64, true>(tpw) : pick<kF64, false>(tpw));
-    int occ = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kSmallThreads, 0)) != cudaSuccess) return e;
-    if ((int64_t)occ * sms < blocks) return cudaErrorNotSupported;
+    if (!fn) return cudaErrorNotSupported;
     if ((e = cudaMemsetAsync(a.bar, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) return e;
     SmallArgs args = a;
     void* params[] = {(void*)&args};
-    return cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(kSmallThreads), params, 0, st);
+    return cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(threads), params, 0, st);
 }
 
 }  // namespace gx

@@ -24,6 +24,8 @@ struct SmallArgs {
 
 // Targets per warp: 1, 2 or 4 forces that many, 0 restores the choice from n (measurements).
 void small_set_targets_per_warp(int tpw);
+// Warps per target of the FP64 form: 1 or 2 forces that many, 0 restores the choice (measurements).
+void small_set_warps_per_target(int wpt);
 // Device bytes of the scratch a launch needs (position buffers, barrier, status); the barrier
 // and status words sit at the start and must be zero before each launch.
 size_t small_scratch_bytes(int n);

@@ -86,6 +86,15 @@ class Session:
         """Small FP64 / exact-form systems step in one cooperative launch (default True)."""
         _ffi.call("gx_session_set_persistent", self._h, 1 if enable else 0)
 
+    def set_fmm(self, options=None) -> None:
+        """The force of later steps: the reference FMM with ``options`` (an FmmOptions), or the
+        direct sum again with None.  FMM steps run in graph-replayed chunks of up to 32."""
+        if options is None:
+            _ffi.call("gx_session_set_fmm", self._h, None)
+        else:
+            self._fmm_opt = options.ffi()
+            _ffi.call("gx_session_set_fmm", self._h, ctypes.addressof(self._fmm_opt))
+
     def set_targets(self, begin: int, count: int) -> None:
         """Owned bodies [begin, begin + count): the only ones kicked, drifted and given forces."""
         _ffi.call("gx_session_set_targets", self._h, int(begin), int(count))

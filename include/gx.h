@@ -159,6 +159,21 @@ int gx_session_step(gx_session* s, int64_t n_steps, double dt, int precision);
 /* Whether small systems use the single-launch step loop (default 1); 0 replays graphs of
  * separate kick-drift and force launches instead.  No reference counterpart. */
 int gx_session_set_persistent(gx_session* s, int enable);
+/* The session's force: the reference FMM with `opt` (the options and semantics of
+ * gx_fmm_accel, declared below), or the direct sum again with opt == NULL (the default).
+ * With the FMM, gx_session_step runs chunks of up to 32 KDK steps, each replayed as one CUDA
+ * graph with no host synchronisation inside: the octree, lists, moments, far and near field
+ * of every step run in device pools sized by a first evaluation with headroom.  After each
+ * chunk the session reads one overflow word; when a pool was too small it restores the
+ * chunk's starting state (copied on the device), regrows the pools and redoes the chunk, and
+ * a tree that needs the host builder (more than leaf_capacity nearly coincident bodies) is
+ * stepped one evaluation at a time through gx_fmm_accel's path.  Results equal gx_fmm_accel
+ * between kick-drift and kick launches step by step (bit for bit in the exact form).  Owned
+ * target ranges (gx_session_set_targets) are not supported with the FMM.  No reference
+ * counterpart: the reference's FMM step loop is cpp/core/main.cpp:172-184 with
+ * compute_fmm_accelerations (cpp/fmm/fmm_solver.cpp:315-322). */
+struct gx_fmm_options;
+int gx_session_set_fmm(gx_session* s, const struct gx_fmm_options* opt);
 /* The bodies this session owns: [begin, begin + count) (default: all n).  Steps, the two
  * half steps below and compute_accelerations kick, drift and evaluate forces for the owned
  * bodies only, with all n bodies as sources -- the ownership range of the reference's MPI
@@ -431,6 +446,13 @@ int gx_debug_p2p_targets_per_thread(int tpt);
  * picks it from n.  For measurements; results agree within the forms' tolerances (the exact
  * form stays bit-identical) either way. */
 int gx_debug_small_targets_per_warp(int tpw);
+/* Warps per target of the FP64 single-launch step loop: 1 or 2 forces that shape, 0 (default)
+ * picks it.  For measurements; results agree within the FP64 tolerance either way. */
+int gx_debug_small_warps_per_target(int wpt);
+/* Sessions that set up their FMM pools after this call size them with no headroom (1) or
+ * with the default half again plus a margin (0), so that tests can make a pool overflow and
+ * check that the step is redone with regrown pools. */
+int gx_debug_fmm_tight_pools(int enable);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

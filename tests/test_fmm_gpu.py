@@ -373,3 +373,91 @@ def test_sharded_fmm_ranges_and_steps():
         for k, v in enumerate(("vx", "vy", "vz")):
             setattr(q, v, getattr(q, v) + a[k] * 0.001)
     assert np.abs(X.cpu().numpy() - np.stack([q.x, q.y, q.z])).max() <= 1e-13
+
+
+def _fmm_loop_stateless(p, params, opt, prec, steps, dt):
+    """Reference loop for the session's FMM steps: kick-drift, gx_fmm_accel (the evaluation that
+    reads its sizes back), kick -- the reference's leapfrog_step with the FMM force."""
+    import torch
+    d = {k: torch.from_numpy(getattr(p, k).copy()).cuda() for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    A = [torch.zeros(len(p), dtype=torch.float64, device="cuda") for _ in range(3)]
+    ptrs = lambda *ts: [t.data_ptr() for t in ts]
+    gx.fmm.fmm_accelerations(d["x"], d["y"], d["z"], d["m"], *A, params, opt, prec)
+    for _ in range(steps):
+        gx._ffi.call("gx_kick_drift", len(p), *ptrs(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], *A),
+                     0.5 * dt, dt, None)
+        gx.fmm.fmm_accelerations(d["x"], d["y"], d["z"], d["m"], *A, params, opt, prec)
+        gx._ffi.call("gx_kick", len(p), *ptrs(d["vx"], d["vy"], d["vz"], *A), 0.5 * dt, None)
+    torch.cuda.synchronize()
+    out = {k: d[k].cpu().numpy() for k in ("x", "y", "z", "vx", "vy", "vz")}
+    out.update(ax=A[0].cpu().numpy(), ay=A[1].cpu().numpy(), az=A[2].cpu().numpy())
+    return out
+
+
+@pytest.mark.parametrize("tight", [False, True])
+@pytest.mark.parametrize("prec", [gx.PRECISION_F64_EXACT, gx.PRECISION_F64, gx.PRECISION_MIXED])
+def test_session_fmm_steps_match_the_evaluation_loop(prec, tight):
+    """gx_session_step with the FMM force (chunks of up to 32 steps replayed as graphs, pools
+    sized on the device by capacity) equals the loop of gx_fmm_accel evaluations between
+    kick-drift and kick launches: bit for bit in the exact form, within 1e-12 in FP64 and 1e-5 in
+    the mixed form; with tight pools (no headroom) chunks overflow and are redone with regrown
+    pools, with the same results."""
+    n, dt, steps = 6000, 0.002, 40
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 515, 0.02)
+    params, opt = gx.PhysicsParams(1.0, 0.02), gx.FmmOptions(0.6, 32, 32, 4)
+    want = _fmm_loop_stateless(p, params, opt, prec, steps, dt)
+    gx._ffi.call("gx_debug_fmm_tight_pools", 1 if tight else 0)
+    try:
+        with gx.Session(n, params) as s:
+            s.set_fmm(opt)
+            s.set_particles(p)
+            s.compute_accelerations(prec)
+            s.step(steps, dt, prec)
+            got = s.get_state()
+    finally:
+        gx._ffi.call("gx_debug_fmm_tight_pools", 0)
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az"):
+        if prec == gx.PRECISION_F64_EXACT:
+            assert np.array_equal(got[k], want[k]), k
+        else:
+            scale = np.abs(want[k]).max()
+            tol = 1e-12 if prec == gx.PRECISION_F64 else 1e-5
+            assert np.max(np.abs(got[k] - want[k])) <= tol * scale, (k, np.max(np.abs(got[k] - want[k])) / scale)
+
+
+def test_session_fmm_deep_tree_falls_back():
+    """More than leaf_capacity coincident bodies need a split below the device key's depth: the
+    session steps such a system through the evaluation path that builds the tree on the host,
+    with the loop's results."""
+    n, dt, steps = 1500, 0.002, 5
+    p = gx.ics.two_disk_encounter(750, 750, 77, 0.02)
+    p.x[:40] = p.x[0]
+    p.y[:40] = p.y[0]
+    p.z[:40] = p.z[0]
+    params, opt = gx.PhysicsParams(1.0, 0.02), gx.FmmOptions(0.6, 8, 32, 4)
+    want = _fmm_loop_stateless(p, params, opt, gx.PRECISION_F64_EXACT, steps, dt)
+    with gx.Session(n, params) as s:
+        s.set_fmm(opt)
+        s.set_particles(p)
+        s.compute_accelerations(gx.PRECISION_F64_EXACT)
+        s.step(steps, dt, gx.PRECISION_F64_EXACT)
+        got = s.get_state()
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.array_equal(got[k], want[k]), k
+
+
+def test_session_fmm_then_direct_again():
+    n = 2000
+    p = gx.ics.two_disk_encounter(1000, 1000, 9, 0.02)
+    params = gx.PhysicsParams(1.0, 0.02)
+    with gx.Session(n, params) as s:
+        s.set_particles(p)
+        s.set_fmm(gx.FmmOptions(0.6, 16, 32, 4))
+        s.compute_accelerations(gx.PRECISION_F64)
+        a_fmm = s.get_state()["ax"]
+        s.set_fmm(None)
+        s.compute_accelerations(gx.PRECISION_F64)
+        a_dir = s.get_state()["ax"]
+    want = oracle.direct_targets(p.x, p.y, p.z, p.m, 1.0, 0.02)[:, 0]
+    assert np.max(np.abs(a_dir - want)) <= 1e-12 * np.abs(want).max()
+    assert np.median(np.abs(a_fmm - want) / np.abs(want).max()) <= 1e-3
