@@ -8,8 +8,10 @@
 // (near-list order, then leaf order).  Leaf costs are very uneven (in the N = 65,536
 // two-disk tree the heaviest leaf has 13x the mean number of sources), so a leaf is cut into
 // target groups x source chunks (at most kMaxChunks chunks of at least kMinChunk sources),
-// items of bounded cost.  A plan computed on the device (p2p_count_kernel, then CUB scans)
-// numbers the items; a persistent grid takes them from a ticket counter.  Items of an
+// items of bounded cost.  A plan computed on the device (p2p_count_kernel, a CUB sort of the
+// leaves by item cost, scans) numbers the items, the leaves with the costliest items first;
+// a persistent grid takes them from a ticket counter, so that the last items handed out are
+// the cheapest and the blocks finish together.  Items of an
 // unsplit leaf add their sums to the accelerations directly (target groups are disjoint).
 // A leaf split into chunks writes per-chunk partial sums to scratch; the block that finishes
 // the leaf's last item (a per-leaf counter, after a memory fence) adds the partials in chunk
@@ -30,6 +32,7 @@
 #include <algorithm>
 #include <atomic>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "gx_device.cuh"
@@ -62,6 +65,8 @@ __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exa
         if (lane == 0) {
             a.plan_cnt[l] = 0;
             a.plan_need[l] = 0;
+            a.plan_key[l] = 0;
+            a.plan_ord[l] = l;
         }
         return;
     }
@@ -94,6 +99,27 @@ __global__ void __launch_bounds__(256) p2p_count_kernel(const P2PArgs a, int exa
     a.plan_groups[l] = groups;
     a.plan_cnt[l] = chunks * groups;
     a.plan_need[l] = chunks > 1 ? (int64_t)chunks * nt : 0;
+    // Sort key: the cost of one item, cs sources x (g targets + the staging cost), on a
+    // log scale with four steps per octave (7 bits; 0: no items).
+    uint32_t key = 0;
+    if (chunks > 0) {
+        const int64_t g = (nt + groups - 1) / groups, cs = (src + chunks - 1) / chunks;
+        const uint32_t cost = (uint32_t)min((int64_t)0x7fffffffLL, max((int64_t)4, cs * (g + kStageCost)));
+        const int msb = 31 - __clz(cost);
+        key = (uint32_t)(msb * 4 + ((cost >> (msb - 2)) & 3));
+    }
+    a.plan_key[l] = key;
+    a.plan_ord[l] = l;
+}
+
+// The item counts in decreasing-cost order, and back: each leaf's first item number.
+__global__ void __launch_bounds__(256) p2p_cnt_sorted_kernel(const P2PArgs a, const int* ord, int nl) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k < nl) a.plan_cnt_sorted[k] = a.plan_cnt[ord[k]];
+}
+__global__ void __launch_bounds__(256) p2p_off_scatter_kernel(const P2PArgs a, const int* ord, int nl) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k < nl) a.plan_item_off[ord[k]] = a.plan_off_sorted[k];
 }
 
 // The leaf of every item: item plan_item_off[l] + k belongs to leaf l (k < plan_cnt[l]).  One
@@ -196,13 +222,13 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
         if (item < a.plan_item_cap) {
             leaf = a.plan_item_leaf[item];
         } else {
-            int lo = 0, hi = a.n_leaves;  // largest l with plan_item_off[l] <= item
+            int lo = 0, hi = a.n_leaves;  // largest k with plan_off_sorted[k] <= item
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
-                if (a.plan_item_off[mid] <= item) lo = mid;
+                if (a.plan_off_sorted[mid] <= item) lo = mid;
                 else hi = mid;
             }
-            leaf = lo;
+            leaf = a.plan_ord[lo];
         }
         const int chunks = a.plan_chunks[leaf], groups = a.plan_groups[leaf];
         const int local = item - a.plan_item_off[leaf];
@@ -293,32 +319,37 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
         // lets every thread find its own slots.  One barrier per pass: after it the pass's
         // buffer is complete and every thread has finished the previous pass, whose buffer
         // then takes the copies of the next.
+        // Near leaves qb .. qb + cnt - 1 of the list: s_beg[q] = first slot of leaf q, s_pre[q] =
+        // sources before it in the batch (a warp scan of the sizes).  Ends with a barrier.
+        auto load_batch = [&](int qb, int cnt) {
+            for (int q = tid; q < cnt; q += kP2PBlock) {
+                const int s = a.near_leaf[qb + q];
+                const int b = a.leaf_off[s];
+                s_beg[q] = b;
+                s_pre[q + 1] = a.leaf_off[s + 1] - b;
+            }
+            if (tid == 0) s_pre[0] = 0;
+            __syncthreads();
+            if (tid < 32) {  // inclusive scan of the lengths s_pre[1..cnt] by warp 0
+                int carry = 0;
+                for (int k0 = 1; k0 <= cnt; k0 += 32) {
+                    const int k = k0 + tid;
+                    int v = k <= cnt ? s_pre[k] : 0;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int u = __shfl_up_sync(0xffffffffu, v, o);
+                        if (tid >= o) v += u;
+                    }
+                    if (k <= cnt) s_pre[k] = v + carry;
+                    carry += __shfl_sync(0xffffffffu, v, 31);
+                }
+            }
+            __syncthreads();
+        };
         auto sweep = [&](auto&& compute) {
             int64_t base = 0;  // slots before the current near batch
             for (int qb = nb; qb < ne && base < c_hi; qb += kNearBatch) {
                 const int cnt = min(kNearBatch, ne - qb);
-                for (int q = tid; q < cnt; q += kP2PBlock) {
-                    const int s = a.near_leaf[qb + q];
-                    const int b = a.leaf_off[s];
-                    s_beg[q] = b;
-                    s_pre[q + 1] = a.leaf_off[s + 1] - b;
-                }
-                if (tid == 0) s_pre[0] = 0;
-                __syncthreads();
-                if (tid < 32) {  // inclusive scan of the lengths s_pre[1..cnt] by warp 0
-                    int carry = 0;
-                    for (int k0 = 1; k0 <= cnt; k0 += 32) {
-                        const int k = k0 + tid;
-                        int v = k <= cnt ? s_pre[k] : 0;
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int u = __shfl_up_sync(0xffffffffu, v, o);
-                            if (tid >= o) v += u;
-                        }
-                        if (k <= cnt) s_pre[k] = v + carry;
-                        carry += __shfl_sync(0xffffffffu, v, 31);
-                    }
-                }
-                __syncthreads();
+                load_batch(qb, cnt);
                 const int total = s_pre[cnt];
                 // this batch covers slots [base, base + total) of the sequence; keep [c_lo, c_hi)
                 const int b_lo = (int)max((int64_t)0, c_lo - base);
@@ -412,22 +443,28 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                     sweep([&](int cnt, int buf) {
                         if (!act) return;
                         const int* I = sidx[buf];
-#pragma unroll 2
-                        for (int jj = lane; jj < cnt; jj += L) {
-                            const int r = raw_at(jj);
+                        auto source = [&](const int r) {
                             const double2 xy = sraw[buf][0][r], zm = sraw[buf][1][r];
-                            const double4 q = make_double4(xy.x, xy.y, zm.x, zm.y);
 #pragma unroll
                             for (int h = 0; h < TPT; ++h) {
-                                const double dx = q.x - xt[h], dy = q.y - yt[h], dz = q.z - zt[h];
+                                const double dx = xy.x - xt[h], dy = xy.y - yt[h], dz = zm.x - zt[h];
                                 const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, a.eps2)));
                                 double y = rsqrt_f64(r2);
                                 if (EPS0) y = (r2 == 0.0 || I[r] == ti[h]) ? 0.0 : y;
-                                const double w = q.w * (y * y * y);
+                                const double w = zm.y * (y * y * y);
                                 f[3 * h] = fma(dx, w, f[3 * h]);
                                 f[3 * h + 1] = fma(dy, w, f[3 * h + 1]);
                                 f[3 * h + 2] = fma(dz, w, f[3 * h + 2]);
                             }
+                        };
+                        // the order of the sources does not matter here: a full pass is read
+                        // in buffer order, a partial one through raw_at
+                        if (cnt == kP2PJT) {
+#pragma unroll 2
+                            for (int r = lane; r < kP2PJT; r += L) source(r);
+                        } else {
+#pragma unroll 2
+                            for (int jj = lane; jj < cnt; jj += L) source(raw_at(jj));
                         }
                     });
                 } else {
@@ -594,10 +631,12 @@ size_t item_leaf_bytes(int64_t n, int32_t n_leaves) {
 }
 
 size_t plan_scan_temp_bytes(int32_t n_leaves) {
-    size_t b1 = 0, b2 = 0;
+    size_t b1 = 0, b2 = 0, b3 = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b1, (const int*)nullptr, (int*)nullptr, n_leaves + 1);
     cub::DeviceScan::ExclusiveSum(nullptr, b2, (const int64_t*)nullptr, (int64_t*)nullptr, n_leaves + 1);
-    return (std::max(b1, b2) + 255) & ~(size_t)255;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, b3, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (const int*)nullptr, (int*)nullptr, n_leaves + 1);
+    return (std::max({b1, b2, b3}) + 255) & ~(size_t)255;
 }
 
 }  // namespace
@@ -606,12 +645,13 @@ void p2p_set_targets_per_thread(int tpt) { g_p2p_tpt.store(tpt == 2 || tpt == 4 
 
 size_t p2p_scratch_bytes(int64_t n, int32_t n_leaves) {
     // plan arrays (src, need and scratch offsets int64; chunks, groups, counts, item offsets,
-    // done counters int), the item -> leaf table, the scan's temporary storage, src_ok +
-    // ticket, the partial sums (at most kMaxChunks per leaf slot, leaf slots <= n when leaves
-    // are split), and the slot-ordered sources (32 bytes per body); 256 bytes of alignment
-    // per piece.
+    // done counters int; item-cost keys and leaf order, each with the sort's second buffer,
+    // counts and offsets in that order), the item -> leaf table, the scan's and sort's
+    // temporary storage, src_ok + ticket, the partial sums (at most kMaxChunks per leaf slot,
+    // leaf slots <= n when leaves are split), and the slot-ordered sources (32 bytes per
+    // body); 256 bytes of alignment per piece.
     const size_t nl = (size_t)n_leaves + 1;
-    return nl * (3 * 8 + 5 * 4) + item_leaf_bytes(n, n_leaves) + plan_scan_temp_bytes(n_leaves) + 5 * 256 +
+    return nl * (3 * 8 + 11 * 4) + item_leaf_bytes(n, n_leaves) + plan_scan_temp_bytes(n_leaves) + 6 * 256 +
            (size_t)kMaxChunks * 3 * sizeof(double) * (size_t)n + (size_t)n * sizeof(double4);
 }
 
@@ -635,6 +675,12 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     a.plan_item_off = (int*)carve(nl * 4);
     a.plan_done = (int*)carve(nl * 4);
     a.plan_n_items = a.plan_item_off + a.n_leaves;
+    a.plan_key = (uint32_t*)carve(nl * 4);
+    uint32_t* key_sorted = (uint32_t*)carve(nl * 4);
+    a.plan_ord = (int*)carve(nl * 4);
+    int* ord_sorted = (int*)carve(nl * 4);
+    a.plan_cnt_sorted = (int*)carve(nl * 4);
+    a.plan_off_sorted = (int*)carve(nl * 4);
     align();
     a.plan_item_leaf = (int*)carve(item_leaf_bytes(n_bodies, a.n_leaves));
     a.plan_item_cap = (int)std::min<size_t>(item_leaf_bytes(n_bodies, a.n_leaves) / sizeof(int), 0x7fffffff);
@@ -665,9 +711,35 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     p2p_gather_kernel<<<sms * 8, 256, 0, st>>>(a, n_bodies);
     p2p_count_kernel<<<(a.n_leaves + 8) / 8, 256, 0, st>>>(a, precision == kF64Exact ? 1 : 0, item_cost);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, a.plan_cnt, a.plan_item_off, (int)nl, st)) != cudaSuccess)
-        return e;
-    if ((e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
+    // With few items per block, the leaves by decreasing item cost and the items numbered in
+    // that order: without it the last items handed out can be the largest, and at
+    // N = 65,536 leaf 64 (3011 leaves, 740 blocks) the SMs sat idle for 18% of the P2P kernel.
+    // With many items per block the tail is small and the sort (four launches) is skipped,
+    // except in the exact form, whose leaves are never split (N = 2^20 leaf 16: 17 ms sorted,
+    // 28 ms in leaf order).
+    size_t tb = temp_bytes;
+    if (precision == kF64Exact || leaves_est <= 16 * 4 * sms) {
+        if ((e = cub::DeviceRadixSort::SortPairsDescending(temp, tb, a.plan_key, key_sorted, a.plan_ord,
+                                                           ord_sorted, (int)nl, 0, 7, st)) != cudaSuccess)
+            return e;
+        const unsigned gl = (unsigned)((nl + 255) / 256);
+        p2p_cnt_sorted_kernel<<<gl, 256, 0, st>>>(a, ord_sorted, (int)nl);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        tb = temp_bytes;
+        if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.plan_cnt_sorted, a.plan_off_sorted, (int)nl, st)) !=
+            cudaSuccess)
+            return e;
+        p2p_off_scatter_kernel<<<gl, 256, 0, st>>>(a, ord_sorted, (int)nl);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        a.plan_ord = ord_sorted;  // the leaf kernel's fallback search walks the sorted order
+    } else {
+        // leaf order: plan_ord is the identity the count kernel wrote
+        if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.plan_cnt, a.plan_item_off, (int)nl, st)) != cudaSuccess)
+            return e;
+        a.plan_off_sorted = a.plan_item_off;
+    }
+    tb = temp_bytes;
+    if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
         return e;
     p2p_item_leaf_kernel<<<(a.n_leaves + 255) / 256, 256, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

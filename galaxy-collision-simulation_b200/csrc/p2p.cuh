@@ -35,6 +35,10 @@ struct P2PArgs {
     int* plan_n_items;      // = plan_item_off + n_leaves
     int* plan_item_leaf;    // leaf of each item (the first plan_item_cap items)
     int plan_item_cap;
+    uint32_t* plan_key;     // cost of one item of each leaf (0: no items), n_leaves + 1
+    int* plan_ord;          // leaves by decreasing item cost, n_leaves + 1
+    int* plan_cnt_sorted;   // plan_cnt in that order
+    int* plan_off_sorted;   // its exclusive scan: item offsets in that order
     int* ticket;
     // (x, y, z, m) of leaf_part[k] at slot k, gathered once per launch when the leaf slots
     // fit the buffer (src_ok); sources are then read by slot, without the leaf_part hop
