@@ -2028,8 +2028,21 @@ struct FmmWork {
     size_t order_bytes = 0;
     void* p2p_scratch = nullptr;
     int* flags = nullptr;                // device: [0] per-evaluation overflow, [1] sticky (bit 1: too deep)
+    int* m2m_ready = nullptr;            // device: per-node flags and a ticket of the one-launch M2M
+    int* m2m_ticket = nullptr;
+    // The far and near fields run side by side (FP64 and mixed forms): the far field on aux,
+    // the near field into near[0..3n) on the caller's stream, then one add.
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    double* near = nullptr;
     unsigned long long* need = nullptr;  // device: largest {nodes, far, near, items, slots} seen
     ~FmmWork() {
+        if (aux) {
+            cudaStreamSynchronize(aux);
+            cudaStreamDestroy(aux);
+        }
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
         for (void* p : owned) cudaFree(p);
     }
     template <typename T>
@@ -2084,6 +2097,12 @@ int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_
     GX_TRY(w.grab((int64_t)w.tree_bytes, (char**)&w.tree_temp));
     GX_TRY(w.grab(2, &w.flags));
     GX_TRY(w.grab(5, &w.need));
+    GX_TRY(w.grab(NC, &w.m2m_ready));
+    GX_TRY(w.grab(1, &w.m2m_ticket));
+    GX_TRY(w.grab(3 * n, &w.near));
+    GX_CUDA(cudaStreamCreateWithFlags(&w.aux, cudaStreamNonBlocking));
+    GX_CUDA(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming));
+    GX_CUDA(cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming));
 
     FmmArgs& fa = w.fa;
     fmm_common_args(fa, nullptr, nullptr, nullptr, nullptr, phys, opt, 0, n);
@@ -2183,20 +2202,36 @@ int fmm_work_enqueue(FmmWork& w, const double* x, const double* y, const double*
     fa.y = y;
     fa.z = z;
     fa.m = m;
-    GX_CUDA(launch_fmm_moments_device(fa, t.level_off, t.hdr + 1, st));
+    GX_CUDA(launch_fmm_moments_tree(fa, w.m2m_ticket, w.m2m_ready, w.flags, sm_count(dev), st));
     TreeListArgs& la = w.la;
     GX_CUDA(launch_tree_lists_count(la, w.list_temp, w.list_bytes, st));
     GX_CUDA(launch_pool_check(la, t.hdr, st));
     GX_CUDA(launch_tree_lists_fill(la, w.node_cap, st));
     GX_CUDA(launch_item_order(w.items, la.leaf_off, (int32_t)w.item_cap, la.totals + 2, w.flags, w.cost, w.cost_alt,
                               w.idx, w.idx_alt, w.order_temp, w.order_bytes, w.sorted, st));
-    for (double* p : {ax, ay, az}) GX_CUDA(cudaMemsetAsync(p, 0, (size_t)n * sizeof(double), st));
+    // The exact form's near field continues the far field's sums in the reference's order, so
+    // it runs after it; the other forms run the two side by side.
+    const bool side = precision != kF64Exact;
+    cudaStream_t fst = st;
+    if (side) {
+        GX_CUDA(cudaEventRecord(w.fork, st));
+        GX_CUDA(cudaStreamWaitEvent(w.aux, w.fork, 0));
+        fst = w.aux;
+    }
+    for (double* p : {ax, ay, az}) GX_CUDA(cudaMemsetAsync(p, 0, (size_t)n * sizeof(double), fst));
     fa.ax = ax;
     fa.ay = ay;
     fa.az = az;
     fa.eps2f = (float)fa.eps2;
-    GX_CUDA(cudaMemsetAsync(fa.done, 0, (size_t)w.node_cap * sizeof(int), st));
-    GX_CUDA(launch_fmm_m2p(fa, precision == kMixed, st));
+    GX_CUDA(cudaMemsetAsync(fa.done, 0, (size_t)w.node_cap * sizeof(int), fst));
+    GX_CUDA(launch_fmm_m2p(fa, precision == kMixed, fst));
+    if (side) {
+        GX_CUDA(cudaEventRecord(w.join, w.aux));
+        GX_CUDA(cudaMemsetAsync(w.near, 0, (size_t)(3 * n) * sizeof(double), st));
+    }
+    double* nx = side ? w.near : ax;
+    double* ny = side ? w.near + n : ay;
+    double* nz = side ? w.near + 2 * n : az;
     P2PArgs pa{};
     pa.x = x; pa.y = y; pa.z = z; pa.m = m;
     pa.leaf_off = la.leaf_off; pa.leaf_part = la.leaf_part; pa.near_off = la.near_off; pa.near_leaf = la.near_leaf;
@@ -2204,13 +2239,17 @@ int fmm_work_enqueue(FmmWork& w, const double* x, const double* y, const double*
     pa.cnt_leaves = la.start_ord + n;
     pa.overflow = w.flags;
     pa.leaves_hint = w.leaves_hint;
-    pa.ax = ax; pa.ay = ay; pa.az = az;
+    pa.ax = nx; pa.ay = ny; pa.az = nz;
     pa.t_begin = 0;
     pa.t_end = n;
     pa.G = w.phys.G;
     pa.eps2 = w.phys.softening * w.phys.softening;
     pa.eps2f = (float)pa.eps2;
     GX_CUDA(launch_p2p(pa, n, precision, w.p2p_scratch, sm_count(dev), st));
+    if (side) {
+        GX_CUDA(cudaStreamWaitEvent(st, w.join, 0));
+        GX_CUDA(launch_fmm_add_near(n, ax, ay, az, nx, ny, nz, sm_count(dev), st));
+    }
     return GX_OK;
 }
 

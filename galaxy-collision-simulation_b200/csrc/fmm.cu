@@ -193,7 +193,8 @@ __device__ __forceinline__ void m2m_node(const FmmArgs& a, const int w, double (
     const int c0 = a.node_child[w];
     if (c0 < 0) return;
     const int tid = threadIdx.x, c = tid >> 5, lane = tid & 31;
-    for (int k = tid; k < 8 * kRecTrQ; k += 256) s_child[k / kRecTrQ][k % kRecTrQ] = a.rec[(size_t)(c0 + k / kRecTrQ) * kFmmRec + k % kRecTrQ];
+    for (int k = tid; k < 8 * kRecTrQ; k += 256)
+        s_child[k / kRecTrQ][k % kRecTrQ] = __ldcg(&a.rec[(size_t)(c0 + k / kRecTrQ) * kFmmRec + k % kRecTrQ]);
     __syncthreads();
     double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
     for (int q = 0; q < 8; ++q) {
@@ -249,15 +250,55 @@ __global__ void __launch_bounds__(256) fmm_m2m_kernel(const FmmArgs a, int lb) {
     m2m_node(a, lb + blockIdx.x, s_child, s_val);
 }
 
-// The same for every node of level d, with the level bounds read on the device (level_off,
-// n_levels as the topology build left them): the CTAs stride over the level's nodes.
-__global__ void __launch_bounds__(256) fmm_m2m_level_kernel(const FmmArgs a, const int32_t* level_off,
-                                                            const int32_t* n_levels, int d) {
+// Every internal node in one launch, without a barrier per level.  Blocks take the nodes
+// from a ticket counter in decreasing index order; levels are numbered top down, so a node
+// comes after all its children.  A block waits (thread c for child c) until the flag of each
+// internal child is set, computes the node as above and sets its own flag.  A block only
+// waits for nodes whose tickets were taken before its own, by blocks already running, so the
+// wait always ends; it is bounded all the same (timeout_ns of the global timer), and a wait
+// that gives up sets bit 0 of err[0] and err[1] (the evaluation is then redone).  Child
+// records are read through L2 (__ldcg), since another SM wrote them in this launch.
+__device__ __forceinline__ unsigned long long m2m_clock() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void __launch_bounds__(256) fmm_m2m_tree_kernel(const FmmArgs a, int* ticket, int* ready, int* err,
+                                                           unsigned long long timeout_ns) {
     __shared__ double s_child[8][kRecTrQ];
     __shared__ double s_val[8][32];
-    if (d >= *n_levels || fmm_nodes(a) == 0) return;
-    const int lb = level_off[d], le = min(level_off[d + 1], fmm_nodes(a));
-    for (int w = lb + blockIdx.x; w < le; w += gridDim.x) m2m_node(a, w, s_child, s_val);
+    __shared__ int s_t;
+    const int nn = fmm_nodes(a);
+    for (;;) {
+        if (threadIdx.x == 0) s_t = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int t = s_t;
+        __syncthreads();
+        if (t >= nn) return;
+        const int w = nn - 1 - t;
+        const int c0 = a.node_child[w];
+        if (c0 < 0) continue;  // a leaf: fmm_leaf_kernel wrote it
+        if (threadIdx.x < 8 && a.node_child[c0 + threadIdx.x] >= 0) {
+            const int* f = ready + c0 + threadIdx.x;
+            const unsigned long long t0 = m2m_clock();
+            int v = 0;
+            for (unsigned it = 0;; ++it) {
+                asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+                if (v) break;
+                if ((it & 255) == 255 && m2m_clock() - t0 > timeout_ns) {
+                    atomicOr(err, 1);
+                    atomicOr(err + 1, 1);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        m2m_node(a, w, s_child, s_val);  // ends with a block barrier
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(ready + w), "r"(1) : "memory");
+    }
 }
 
 __device__ __forceinline__ double rsqrt_t(double s) { return rsqrt_f64(s); }
@@ -535,19 +576,36 @@ int fmm_effective_order(int expansion_order) {
     return p;
 }
 
-cudaError_t launch_fmm_moments_device(const FmmArgs& a, const int32_t* level_off, const int32_t* n_levels,
-                                      cudaStream_t st) {
+cudaError_t launch_fmm_moments_tree(const FmmArgs& a, int* ticket, int* ready, int* err, int sms, cudaStream_t st) {
     constexpr int wpb = kMomBlock / 32;
     if (a.n_nodes == 0) return cudaSuccess;
-    fmm_leaf_kernel<<<(a.n_nodes + wpb - 1) / wpb, kMomBlock, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(ready, 0, (size_t)a.n_nodes * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    const int grid = std::min(a.n_nodes, 148 * 8);
-    for (int d = kMaxLevels - 1; d >= 0; --d) {
-        fmm_m2m_level_kernel<<<grid, 256, 0, st>>>(a, level_off, n_levels, d);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    fmm_leaf_kernel<<<(a.n_nodes + wpb - 1) / wpb, kMomBlock, 0, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int grid = std::min(a.n_nodes, sms * 8);
+    fmm_m2m_tree_kernel<<<grid, 256, 0, st>>>(a, ticket, ready, err, 1000000000ull);
+    return cudaGetLastError();
+}
+
+// ax += nx, ay += ny, az += nz: the near field, computed into its own arrays while the far
+// field ran, added to it (one rounding, as when the near kernel adds to the far field).
+__global__ void __launch_bounds__(256) fmm_add_near_kernel(int64_t n, double* ax, double* ay, double* az,
+                                                           const double* nx, const double* ny, const double* nz) {
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        ax[i] = ax[i] + nx[i];
+        ay[i] = ay[i] + ny[i];
+        az[i] = az[i] + nz[i];
     }
-    return cudaSuccess;
+}
+
+cudaError_t launch_fmm_add_near(int64_t n, double* ax, double* ay, double* az, const double* nx, const double* ny,
+                                const double* nz, int sms, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8);
+    fmm_add_near_kernel<<<(unsigned)blocks, 256, 0, st>>>(n, ax, ay, az, nx, ny, nz);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st) {

@@ -94,9 +94,13 @@ constexpr int kM2PChunk = 512;  // far nodes per work item
 
 // Stream-ordered: leaf moments, then one launch per level (deepest first), then M2P.
 cudaError_t launch_fmm_moments(const FmmArgs& a, const int32_t* level_off_host, int n_levels, cudaStream_t st);
-// The same with the level bounds on the device (kMaxLevels launches, empty levels return).
-cudaError_t launch_fmm_moments_device(const FmmArgs& a, const int32_t* level_off, const int32_t* n_levels,
-                                      cudaStream_t st);
+// The same with every internal node in one launch (blocks wait on their children's flags):
+// ticket (1 int) and ready (n_nodes ints) are scratch; a wait that times out sets bit 0 of
+// err[0] and err[1].
+cudaError_t launch_fmm_moments_tree(const FmmArgs& a, int* ticket, int* ready, int* err, int sms, cudaStream_t st);
+// ax += nx etc. for i < n (the near field added to the far field).
+cudaError_t launch_fmm_add_near(int64_t n, double* ax, double* ay, double* az, const double* nx, const double* ny,
+                                const double* nz, int sms, cudaStream_t st);
 // mixed: FP32 multipole arithmetic on FP64 offsets (fills a.rec32 from a.rec first); else FP64.
 cudaError_t launch_fmm_m2p(const FmmArgs& a, bool mixed, cudaStream_t st);
 

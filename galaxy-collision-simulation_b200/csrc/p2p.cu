@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
 #pragma unroll
                         for (int h = 0; h < TPT; ++h) PX[h] = PY[h] = PZ[h] = pk2(0.f, 0.f);
                         const int np = (cnt + 1) >> 1;
-#pragma unroll 2
+#pragma unroll 4
                         for (int pp = lane; pp < np; pp += L) {
                             f2 X, Y, Z, M;
                             lds_v2b64(reinterpret_cast<const float*>(&PA[pp]), X, Y);
