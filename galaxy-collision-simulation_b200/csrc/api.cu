@@ -2035,7 +2035,8 @@ struct FmmWork {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     double* near = nullptr;
-    unsigned long long* need = nullptr;  // device: largest {nodes, far, near, items, slots} seen
+    unsigned long long* need = nullptr;  // device: largest {nodes, far, near, items, slots, tree levels} seen
+    int key_levels = 0;                  // levels of the path keys the tree sort orders
     ~FmmWork() {
         if (aux) {
             cudaStreamSynchronize(aux);
@@ -2061,10 +2062,15 @@ int64_t with_headroom(int64_t v) { return g_fmm_tight_pools.load() ? std::max<in
 // Capacities from a sizing evaluation's counts (or from the largest counts an overflowing
 // evaluation needed), with half again as much headroom; node slots never above the most a
 // tree of n bodies can have.
+// The tree sort orders key_levels levels of the path keys: two more than the sizing tree had,
+// so a tree two levels deeper still builds; a deeper one sets the overflow flag and the
+// chunk is redone with all levels.
 int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_fmm_options opt, int64_t nodes,
-                    int64_t leaves, int64_t far, int64_t near, int64_t items, int64_t slots, cudaStream_t st) {
+                    int64_t leaves, int64_t far, int64_t near, int64_t items, int64_t slots, int key_levels,
+                    cudaStream_t st) {
     W.reset(new FmmWork());
     FmmWork& w = *W;
+    w.key_levels = std::max(1, std::min(key_levels, (int)kKeyLevels));
     w.n = n;
     w.phys = phys;
     w.opt = opt;
@@ -2083,6 +2089,7 @@ int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_
     t.cap = cap;
     t.max_depth = std::max(1, opt.max_depth);
     t.capacity = NC;
+    t.key_levels = w.key_levels;
     GX_TRY(w.grab(6 * kBboxBlocks, &t.part));
     GX_TRY(w.grab(4, &t.root));
     GX_TRY(w.grab(n, &t.keys));
@@ -2096,7 +2103,7 @@ int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_
     w.tree_bytes = tree_build_temp_bytes(t.n, cap);
     GX_TRY(w.grab((int64_t)w.tree_bytes, (char**)&w.tree_temp));
     GX_TRY(w.grab(2, &w.flags));
-    GX_TRY(w.grab(5, &w.need));
+    GX_TRY(w.grab(6, &w.need));
     GX_TRY(w.grab(NC, &w.m2m_ready));
     GX_TRY(w.grab(1, &w.m2m_ticket));
     GX_TRY(w.grab(3 * n, &w.near));
@@ -2181,7 +2188,7 @@ int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_
     GX_TRY(w.grab(NC, &fa.done));
     GX_TRY(w.grab((int64_t)p2p_scratch_bytes(n, NC), (char**)&w.p2p_scratch));
     GX_CUDA(cudaMemsetAsync(w.flags, 0, 2 * sizeof(int), st));
-    GX_CUDA(cudaMemsetAsync(w.need, 0, 5 * sizeof(unsigned long long), st));
+    GX_CUDA(cudaMemsetAsync(w.need, 0, 6 * sizeof(unsigned long long), st));
     return GX_OK;
 }
 
@@ -2266,7 +2273,8 @@ int session_fmm_size(gx_session* s, bool* device_ok) {
     if (deep) return GX_OK;
     std::unique_ptr<FmmWork> W;
     GX_TRY(fmm_work_create(W, s->n, s->phys, s->fmm_opt, P->n_nodes, P->n_leaves, P->n_far, P->n_near,
-                           P->fa.n_items, P->n_slots, s->stream));
+                           P->fa.n_items, P->n_slots,
+                           g_fmm_tight_pools.load() ? 1 : (int)P->level_off.size() - 1 + 2, s->stream));
     fmm_work_release(s->fmm);
     s->fmm = W.release();
     s->clear_graphs();
@@ -2277,14 +2285,15 @@ int session_fmm_size(gx_session* s, bool* device_ok) {
 // again larger than before.
 int session_fmm_regrow(gx_session* s) {
     FmmWork& w = *s->fmm;
-    unsigned long long need[5];
+    unsigned long long need[6];
     GX_CUDA(cudaMemcpyAsync(need, w.need, sizeof(need), cudaMemcpyDeviceToHost, s->stream));
     GX_CUDA(cudaStreamSynchronize(s->stream));
     std::unique_ptr<FmmWork> W;
     GX_TRY(fmm_work_create(W, s->n, s->phys, s->fmm_opt, std::max<int64_t>((int64_t)need[0], w.node_cap),
                            w.leaves_hint, std::max<int64_t>((int64_t)need[1], w.far_cap),
                            std::max<int64_t>((int64_t)need[2], w.near_cap), std::max<int64_t>((int64_t)need[3], w.item_cap),
-                           std::max<int64_t>((int64_t)need[4], w.slot_cap), s->stream));
+                           std::max<int64_t>((int64_t)need[4], w.slot_cap),
+                           std::max(w.key_levels, (int)std::min<unsigned long long>(need[5], kKeyLevels) + 2), s->stream));
     fmm_work_release(s->fmm);
     s->fmm = W.release();
     s->clear_graphs();

@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
     double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
     for (int k0 = b; k0 < e; k0 += 32) {
         const int cnt = stage(k0);
+#pragma unroll 4
         for (int q = 0; q < cnt; ++q) {
             const double mi = sb[3][q];
             mass = dadd(mass, mi);
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(kMomBlock) fmm_leaf_kernel(const FmmArgs a) {
     double v = 0.0;
     for (int k0 = b; k0 < e; k0 += 32) {
         const int cnt = stage(k0);
+#pragma unroll 4
         for (int q = 0; q < cnt; ++q) {
             const Pow4 px(dsub(sb[0][q], cx)), py(dsub(sb[1][q], cy)), pz(dsub(sb[2][q], cz));
             const double mono = dmul(dmul(px(ex), py(ey)), pz(ez));
@@ -213,14 +215,21 @@ __device__ __forceinline__ void m2m_node(const FmmArgs& a, const int w, double (
     const double cm = cr[kRecMass];
     if (lane < 31 && cm > 0.0) {
         const Pow4 px(dsub(cr[0], cx)), py(dsub(cr[1], cy)), pz(dsub(cr[2], cz));
+        // The terms are independent until the sum: the loop runs to the table's bound with the
+        // lane's own count as a predicate, so the loads and products of later terms overlap the
+        // additions, which stay in the reference's order.
         const int nt = kTab.nterm[lane];
         double value = 0.0;
-        for (int q = 0; q < nt; ++q) {
-            const double sf = dmul(dmul(dmul(kTab.bin[lane][q], px(kTab.dx[lane][q])), py(kTab.dy[lane][q])),
-                                   pz(kTab.dz[lane][q]));
-            if (sf == 0.0) continue;
-            const int kb = kTab.kb[lane][q];
-            value = dadd(value, dmul(sf, kb == 0 ? cm : cr[kb]));
+#pragma unroll
+        for (int q = 0; q < kMaxShiftTerms; ++q) {
+            if (q < nt) {
+                const double sf = dmul(dmul(dmul(kTab.bin[lane][q], px(kTab.dx[lane][q])), py(kTab.dy[lane][q])),
+                                       pz(kTab.dz[lane][q]));
+                if (sf != 0.0) {
+                    const int kb = kTab.kb[lane][q];
+                    value = dadd(value, dmul(sf, kb == 0 ? cm : cr[kb]));
+                }
+            }
         }
         s_val[c][lane] = value;
     }

@@ -26,6 +26,8 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <thrust/iterator/zip_iterator.h>
+#include <thrust/tuple.h>
 
 #include <algorithm>
 #include <cfloat>
@@ -159,7 +161,9 @@ __device__ __forceinline__ int lower_octant(const uint64_t* keys, int b, int e, 
 // A node's centre is the reference's recurrence (subdivide, fmm_solver.cpp:111-131) walked
 // from the root along its prefix -- the same operations in the same order as building level
 // by level, so the same bits.  A prefix of depth kKeyLevels that would still split needs a
-// deeper key: hdr[2] bit 0 hands the tree to the host builder.
+// deeper key: hdr[2] bit 0 hands the tree to the host builder.  When the sort ordered only
+// the first key_levels levels, a prefix of that depth that would split sets hdr[2] bit 2
+// instead (the build stops there; the caller redoes it with all levels).
 
 __device__ __forceinline__ uint64_t key_prefix(uint64_t key, int L) {
     const int sh = 3 * (kKeyLevels - L);
@@ -199,6 +203,7 @@ __global__ void __launch_bounds__(256) split_flags_kernel(const TreeBuildArgs t,
     if (i == 0) flags[(size_t)kKeyLevels * t.n] = 0;
     if (i >= t.n) return;
     const int lmax = min(t.max_depth, kKeyLevels + 1);
+    const int sorted = t.key_levels > 0 ? t.key_levels : kKeyLevels;  // levels the sort ordered
     const uint64_t key = keys[i];
     const bool big = (int64_t)i + t.cap < (int64_t)t.n;
     const uint64_t far = big ? keys[i + t.cap] : 0;
@@ -206,6 +211,7 @@ __global__ void __launch_bounds__(256) split_flags_kernel(const TreeBuildArgs t,
         bool split = false;
         if (L < lmax && big && prefix_first(keys, i, L) && key_prefix(far, L) == key_prefix(key, L)) {
             if (L == kKeyLevels) atomicOr(&t.hdr[2], 1);
+            else if (L >= sorted) atomicOr(&t.hdr[2], 4);  // the children need deeper sorted keys
             else split = true;
         }
         if (L < kKeyLevels) flags[(size_t)L * t.n + i] = split ? 1 : 0;
@@ -672,8 +678,10 @@ __global__ void __launch_bounds__(256) items_kernel(const TreeListArgs a, int n_
 }
 
 // Far-field items, largest first (cost = targets x nodes): fewer long items at the tail.
-// Sort keys: cost + 1 for the real items (n_real of them, from the device count when given),
-// 0 for the rest of the capacity, so that the real items come first in decreasing cost.
+// Sort keys: the cost of the real items (n_real of them, from the device count when given) on
+// a log scale with four steps per octave (1..127, 7 bits: one radix pass), 0 for the rest of
+// the capacity, so that the real items come first, largest first.  The order only balances
+// the blocks' work: a leaf's partial sums are added in chunk order whatever it is.
 __global__ void __launch_bounds__(256) item_cost_kernel(const M2PItem* items, const int32_t* leaf_off, int n,
                                                         const unsigned long long* n_real, const int* overflow,
                                                         uint32_t* cost, int32_t* idx) {
@@ -683,7 +691,10 @@ __global__ void __launch_bounds__(256) item_cost_kernel(const M2PItem* items, co
     uint32_t c = 0;
     if (k < real) {
         const M2PItem it = items[k];
-        c = (uint32_t)(leaf_off[it.leaf + 1] - leaf_off[it.leaf]) * (uint32_t)(it.fe - it.fb) + 1u;
+        const uint32_t v = min((uint32_t)(leaf_off[it.leaf + 1] - leaf_off[it.leaf]) * (uint32_t)(it.fe - it.fb) + 1u,
+                               0x7fffffffu);
+        const int msb = 31 - __clz(v);
+        c = v < 4u ? v : (uint32_t)(msb * 4 + ((v >> (msb - 2)) & 3));
     }
     cost[k] = c;
     idx[k] = k;
@@ -697,6 +708,8 @@ __global__ void pool_check_kernel(const TreeListArgs a, const int32_t* tree_hdr)
     if (a.need) {
         atomicMax(&a.need[0], (unsigned long long)(tree_hdr[0] > 0 ? tree_hdr[0] : 0));
         for (int k = 0; k < 4; ++k) atomicMax(&a.need[1 + k], t[k]);
+        // levels of the tree; a tree cut short by too few sorted key levels asks for all
+        atomicMax(&a.need[5], (unsigned long long)(tree_hdr[2] & 4 ? kKeyLevels : max(tree_hdr[1], 0)));
     }
     if (t[0] > (unsigned long long)a.far_cap || t[1] > (unsigned long long)a.near_cap ||
         t[2] > (unsigned long long)a.item_cap || t[3] > (unsigned long long)a.slot_cap || tree_hdr[2] != 0) {
@@ -714,6 +727,31 @@ __global__ void __launch_bounds__(256) item_gather_kernel(const M2PItem* items, 
 size_t scan_bytes(int count) {
     size_t b = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b, (const int32_t*)nullptr, (int32_t*)nullptr, count);
+    return b;
+}
+
+// The four per-leaf counts of the list pass (far, near, work items, partial-sum slots)
+// scanned together: one exclusive scan of 4-tuples, element-wise sums.
+using Count4 = thrust::tuple<int32_t, int32_t, int32_t, int32_t>;
+struct Sum4 {
+    __host__ __device__ Count4 operator()(const Count4& a, const Count4& b) const {
+        return Count4(thrust::get<0>(a) + thrust::get<0>(b), thrust::get<1>(a) + thrust::get<1>(b),
+                      thrust::get<2>(a) + thrust::get<2>(b), thrust::get<3>(a) + thrust::get<3>(b));
+    }
+};
+
+cudaError_t scan4(void* temp, size_t& bytes, const int32_t* const cnt[4], int32_t* const off[4], int count,
+                  cudaStream_t st) {
+    auto in = thrust::make_zip_iterator(thrust::make_tuple(cnt[0], cnt[1], cnt[2], cnt[3]));
+    auto out = thrust::make_zip_iterator(thrust::make_tuple(off[0], off[1], off[2], off[3]));
+    return cub::DeviceScan::ExclusiveScan(temp, bytes, in, out, Sum4{}, Count4(0, 0, 0, 0), count, st);
+}
+
+size_t scan4_bytes(int count) {
+    size_t b = 0;
+    const int32_t* cnt[4] = {nullptr, nullptr, nullptr, nullptr};
+    int32_t* off[4] = {nullptr, nullptr, nullptr, nullptr};
+    scan4(nullptr, b, cnt, off, count, nullptr);
     return b;
 }
 
@@ -760,7 +798,9 @@ cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_by
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cub::DoubleBuffer<uint64_t> k(t.keys, t.keys_alt);
     cub::DoubleBuffer<int32_t> v(t.idx, t.perm);
-    if ((e = cub::DeviceRadixSort::SortPairs(work, work_bytes, k, v, t.n, 0, 3 * kKeyLevels, st)) != cudaSuccess)
+    const int sorted = t.key_levels > 0 ? std::min(t.key_levels, kKeyLevels) : kKeyLevels;
+    if ((e = cub::DeviceRadixSort::SortPairs(work, work_bytes, k, v, t.n, 3 * (kKeyLevels - sorted), 3 * kKeyLevels,
+                                             st)) != cudaSuccess)
         return e;
     if (v.Current() != t.perm) gather_perm_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(v.Current(), t.perm, t.n);
     split_flags_kernel<<<(t.n + 255) / 256, 256, 0, st>>>(t, k.Current(), flags);
@@ -783,7 +823,7 @@ cudaError_t launch_tree_leaf_order(const TreeBuildArgs& t, int32_t n_nodes, void
 }
 
 size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes) {
-    return std::max(scan_bytes(n + 1), scan_bytes(n_nodes + 1));
+    return std::max({scan_bytes(n + 1), scan_bytes(n_nodes + 1), scan4_bytes(n_nodes + 1)});
 }
 
 // Both walk kernels prefer the largest shared-memory carveout (8 blocks of 28.5 KiB).
@@ -817,13 +857,10 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     if ((e = walk_carveout()) != cudaSuccess) return e;
     walk_kernel<false><<<(a.n_nodes + kWalkThreads / 32 - 1) / (kWalkThreads / 32), kWalkThreads, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const int32_t* cnt[4] = {a.far_cnt, a.near_cnt, a.item_cnt, a.slot_cnt};
-    int32_t* off[4] = {a.far_off, a.near_off, a.item_off, a.slot_off};
-    for (int k = 0; k < 4; ++k) {
-        tb = temp_bytes;
-        if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, cnt[k], off[k], a.n_nodes + 1, st)) != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    const int32_t* const cnt[4] = {a.far_cnt, a.near_cnt, a.item_cnt, a.slot_cnt};
+    int32_t* const off[4] = {a.far_off, a.near_off, a.item_off, a.slot_off};
+    tb = temp_bytes;
+    return scan4(temp, tb, cnt, off, a.n_nodes + 1, st);
 }
 
 cudaError_t launch_pool_check(const TreeListArgs& a, const int32_t* tree_hdr, cudaStream_t st) {
@@ -858,7 +895,7 @@ cudaError_t launch_item_order(const M2PItem* items, const int32_t* leaf_off, int
     item_cost_kernel<<<g, 256, 0, st>>>(items, leaf_off, n_items, n_real, overflow, cost, idx);
     cub::DoubleBuffer<uint32_t> k(cost, cost_alt);
     cub::DoubleBuffer<int32_t> v(idx, idx_alt);
-    cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, temp_bytes, k, v, n_items, 0, 32, st);
+    cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, temp_bytes, k, v, n_items, 0, 7, st);
     if (e != cudaSuccess) return e;
     item_gather_kernel<<<g, 256, 0, st>>>(items, v.Current(), n_items, out);
     return cudaGetLastError();

@@ -37,6 +37,10 @@ struct TreeBuildArgs {
     double* hw;
     int32_t* level_off;  // kKeyLevels + 3
     int32_t* hdr;        // 3
+    // Levels of the key that the sort orders (0: all kKeyLevels).  Fewer levels take fewer
+    // radix passes; a tree that would split a node at that depth sets hdr[2] bit 2 instead
+    // (the caller rebuilds with more levels).
+    int key_levels;
 };
 size_t tree_build_temp_bytes(int32_t n, int64_t cap);
 cudaError_t launch_tree_build(const TreeBuildArgs& t, void* temp, size_t temp_bytes, cudaStream_t st);

@@ -451,7 +451,8 @@ int gx_debug_small_targets_per_warp(int tpw);
 int gx_debug_small_warps_per_target(int wpt);
 /* Sessions that set up their FMM pools after this call size them with no headroom (1) or
  * with the default half again plus a margin (0), so that tests can make a pool overflow and
- * check that the step is redone with regrown pools. */
+ * check that the step is redone with regrown pools.  With 1 the tree sort also starts with
+ * one level of the path keys, so the first tree deeper than that is redone with all levels. */
 int gx_debug_fmm_tight_pools(int enable);
 
 #if defined(__GNUC__)
