@@ -225,7 +225,8 @@ def main():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the N=1000, N=65536 and ensemble configurations of the default line")
     ap.add_argument("--workload", default="mixed-n1048576",
-                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "fmm-evals", "snapshots-n1048576",
+                    choices=["mixed-n1048576", "ensemble", "fmm-n65536", "fmm-session-n65536", "fmm-evals",
+                             "snapshots-n1048576",
                              "ics-ensemble512", "p2p", "p2p-n65536", "direct-n65536", "direct-n1000", "fit-n16384"],
                     help="headline (default) or one of the other configurations")
     args = ap.parse_args()
@@ -890,6 +891,35 @@ FP64_OPS_PER_M2P_PAIR = 171
 FP64_OPS_PER_P2P_PAIR = 17
 
 
+def wl_fmm_session(gx, torch, args) -> dict:
+    """The FMM KDK step of the N = 65,536 workload (leaf 64, theta 0.6, order 4, FP64) in a
+    resident session only: gx_session_set_fmm, --warmup calls of min(--steps, 32) steps (the
+    first sizes the pools and captures the chunk's graph), then --steps steps timed on the
+    session's stream.  Small enough to run under a profiler."""
+    n, cap, theta, eps, dt = 65536, 64, 0.6, 0.02, 0.002
+    p = gx.ics.two_disk_encounter(n // 2, n // 2, 20260502, eps)
+    params, opt = gx.PhysicsParams(1.0, eps), gx.FmmOptions(theta, cap, 32, 4)
+    st = torch.cuda.Stream()
+    with gx.Session(n, params) as s:
+        s.set_stream(st)
+        s.set_fmm(opt)
+        s.set_particles(p)
+        s.compute_accelerations(gx.PRECISION_F64)
+        for _ in range(max(1, args.warmup)):
+            s.step(min(args.steps, 32), dt, gx.PRECISION_F64)
+        s.synchronize()
+        a, e = _events(torch)
+        a.record(st)
+        s.step(args.steps, dt, gx.PRECISION_F64)
+        e.record(st)
+        e.synchronize()
+        ms = a.elapsed_time(e) / args.steps
+    return {"metric": "FMM KDK steps/s (N=65536, leaf 64, theta 0.6, p=4, FP64, resident session)",
+            "value": 1e3 / ms, "unit": "steps/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "fmm-session-n65536", "leaf_capacity": cap, "theta": theta, "order": 4}}
+
+
 def wl_fmm(gx, torch, args, e2e: bool = True) -> dict:
     """The reference FMM solver on the N = 65,536 two-disk workload (leaf_capacity 64,
     theta 0.6, expansion order 4, softening 0.02, dt 0.002): one KDK step = kick-drift,
@@ -1220,6 +1250,7 @@ def wl_ics(gx, torch, args) -> dict:
 OTHER_WORKLOADS = {
     "ensemble": wl_ensemble,
     "fmm-n65536": wl_fmm,
+    "fmm-session-n65536": wl_fmm_session,
     "fmm-evals": wl_fmm_evals,
     "snapshots-n1048576": wl_snapshots,
     "ics-ensemble512": wl_ics,

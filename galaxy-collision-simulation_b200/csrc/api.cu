@@ -2030,10 +2030,10 @@ struct FmmWork {
     int* flags = nullptr;                // device: [0] per-evaluation overflow, [1] sticky (bit 1: too deep)
     int* m2m_ready = nullptr;            // device: per-node flags and a ticket of the one-launch M2M
     int* m2m_ticket = nullptr;
-    // The far and near fields run side by side (FP64 and mixed forms): the far field on aux,
-    // the near field into near[0..3n) on the caller's stream, then one add.
+    // Second stream of the evaluation (moments, far field) and the events that fork and join
+    // it; the near field of the FP64 and mixed forms goes to near[0..3n) and is added after.
     cudaStream_t aux = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t fork0 = nullptr, fork = nullptr, join = nullptr;
     double* near = nullptr;
     unsigned long long* need = nullptr;  // device: largest {nodes, far, near, items, slots, tree levels} seen
     int key_levels = 0;                  // levels of the path keys the tree sort orders
@@ -2042,6 +2042,7 @@ struct FmmWork {
             cudaStreamSynchronize(aux);
             cudaStreamDestroy(aux);
         }
+        if (fork0) cudaEventDestroy(fork0);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         for (void* p : owned) cudaFree(p);
@@ -2108,6 +2109,7 @@ int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_
     GX_TRY(w.grab(1, &w.m2m_ticket));
     GX_TRY(w.grab(3 * n, &w.near));
     GX_CUDA(cudaStreamCreateWithFlags(&w.aux, cudaStreamNonBlocking));
+    GX_CUDA(cudaEventCreateWithFlags(&w.fork0, cudaEventDisableTiming));
     GX_CUDA(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming));
     GX_CUDA(cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming));
 
@@ -2146,6 +2148,7 @@ int fmm_work_create(std::unique_ptr<FmmWork>& W, int64_t n, gx_physics phys, gx_
     la.need = w.need;
     la.far_cap = w.far_cap;
     la.near_cap = w.near_cap;
+    GX_TRY(w.grab(n + 1, &la.mprefix));
     la.item_cap = w.item_cap;
     la.slot_cap = w.slot_cap;
     for (int32_t** q : {&la.start_flag, &la.start_ord, &la.keep, &la.newpos}) GX_TRY(w.grab(n + 1, q));
@@ -2209,33 +2212,35 @@ int fmm_work_enqueue(FmmWork& w, const double* x, const double* y, const double*
     fa.y = y;
     fa.z = z;
     fa.m = m;
-    GX_CUDA(launch_fmm_moments_tree(fa, w.m2m_ticket, w.m2m_ready, w.flags, sm_count(dev), st));
+    // Two streams after the tree: the moments and then the far field on aux; the lists (which
+    // need only whether a node has mass, from counts of massive bodies) and the near field on
+    // the caller's stream.  The far field waits for the lists.  The exact form's near field
+    // continues the far field's sums in the reference's order, so it waits for the far field;
+    // the other forms write the near field apart and add it once both are done.
+    const bool side = precision != kF64Exact;
+    GX_CUDA(cudaEventRecord(w.fork0, st));
+    GX_CUDA(cudaStreamWaitEvent(w.aux, w.fork0, 0));
+    GX_CUDA(launch_fmm_moments_tree(fa, w.m2m_ticket, w.m2m_ready, w.flags, sm_count(dev), w.aux));
     TreeListArgs& la = w.la;
+    la.m = m;
+    GX_CUDA(launch_tree_massive(la, w.list_temp, w.list_bytes, st));
     GX_CUDA(launch_tree_lists_count(la, w.list_temp, w.list_bytes, st));
     GX_CUDA(launch_pool_check(la, t.hdr, st));
     GX_CUDA(launch_tree_lists_fill(la, w.node_cap, st));
     GX_CUDA(launch_item_order(w.items, la.leaf_off, (int32_t)w.item_cap, la.totals + 2, w.flags, w.cost, w.cost_alt,
                               w.idx, w.idx_alt, w.order_temp, w.order_bytes, w.sorted, st));
-    // The exact form's near field continues the far field's sums in the reference's order, so
-    // it runs after it; the other forms run the two side by side.
-    const bool side = precision != kF64Exact;
-    cudaStream_t fst = st;
-    if (side) {
-        GX_CUDA(cudaEventRecord(w.fork, st));
-        GX_CUDA(cudaStreamWaitEvent(w.aux, w.fork, 0));
-        fst = w.aux;
-    }
-    for (double* p : {ax, ay, az}) GX_CUDA(cudaMemsetAsync(p, 0, (size_t)n * sizeof(double), fst));
+    GX_CUDA(cudaEventRecord(w.fork, st));
+    GX_CUDA(cudaStreamWaitEvent(w.aux, w.fork, 0));
+    for (double* p : {ax, ay, az}) GX_CUDA(cudaMemsetAsync(p, 0, (size_t)n * sizeof(double), w.aux));
     fa.ax = ax;
     fa.ay = ay;
     fa.az = az;
     fa.eps2f = (float)fa.eps2;
-    GX_CUDA(cudaMemsetAsync(fa.done, 0, (size_t)w.node_cap * sizeof(int), fst));
-    GX_CUDA(launch_fmm_m2p(fa, precision == kMixed, fst));
-    if (side) {
-        GX_CUDA(cudaEventRecord(w.join, w.aux));
-        GX_CUDA(cudaMemsetAsync(w.near, 0, (size_t)(3 * n) * sizeof(double), st));
-    }
+    GX_CUDA(cudaMemsetAsync(fa.done, 0, (size_t)w.node_cap * sizeof(int), w.aux));
+    GX_CUDA(launch_fmm_m2p(fa, precision == kMixed, w.aux));
+    GX_CUDA(cudaEventRecord(w.join, w.aux));
+    if (side) GX_CUDA(cudaMemsetAsync(w.near, 0, (size_t)(3 * n) * sizeof(double), st));
+    else GX_CUDA(cudaStreamWaitEvent(st, w.join, 0));
     double* nx = side ? w.near : ax;
     double* ny = side ? w.near + n : ay;
     double* nz = side ? w.near + 2 * n : az;

@@ -339,10 +339,33 @@ __device__ __forceinline__ int list_nodes(const TreeListArgs& a) {
     return a.cnt_nodes[2] ? 0 : min(a.cnt_nodes[0], a.n_nodes);  // header {nodes, levels, flags}
 }
 
+// Node k has mass > 0: from the massive-body counts when given, else from its record.
+__device__ __forceinline__ bool node_massive(const TreeListArgs& a, int k) {
+    if (a.mprefix) return a.mprefix[a.end[k]] > a.mprefix[a.beg[k]];
+    return node_mass(a.rec, k) > 0.0;
+}
+
+// mflag[k] = body at tree position k has mass > 0 (k < n), mflag[n] = 0; a mass < 0 or NaN
+// (whose node sums the counts cannot stand for) raises the overflow words.
+__global__ void __launch_bounds__(256) massive_flags_kernel(const TreeListArgs a, int32_t* mflag) {
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    if (k > a.n) return;
+    if (k == a.n) {
+        mflag[k] = 0;
+        return;
+    }
+    const double mk = a.m[a.perm[k]];
+    mflag[k] = mk > 0.0 ? 1 : 0;
+    if (!(mk >= 0.0)) {
+        if (a.overflow) *a.overflow = 1;
+        if (a.overflow_sticky) atomicOr(a.overflow_sticky, 3);
+    }
+}
+
 // Marks the first body position of every leaf with mass > 0 and the bodies it keeps.
 __global__ void __launch_bounds__(256) leaf_mark_kernel(const TreeListArgs a) {
     const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= list_nodes(a) || a.child[k] >= 0 || !(node_mass(a.rec, k) > 0.0)) return;
+    if (k >= list_nodes(a) || a.child[k] >= 0 || !node_massive(a, k)) return;
     const int b = a.beg[k], e = a.end[k];
     a.start_flag[b] = 1;
     for (int p = b; p < e; ++p) a.keep[p] = 1;
@@ -350,7 +373,7 @@ __global__ void __launch_bounds__(256) leaf_mark_kernel(const TreeListArgs a) {
 
 __global__ void __launch_bounds__(256) leaf_emit_kernel(const TreeListArgs a) {
     const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= list_nodes(a) || a.child[k] >= 0 || !(node_mass(a.rec, k) > 0.0)) return;
+    if (k >= list_nodes(a) || a.child[k] >= 0 || !node_massive(a, k)) return;
     const int b = a.beg[k], e = a.end[k];
     const int o = a.start_ord[b];
     a.leaf_node[o] = k;
@@ -368,13 +391,13 @@ __global__ void __launch_bounds__(256) walk_pack_kernel(const TreeListArgs a) {
     w.cy = a.cy[k];
     w.cz = a.cz[k];
     w.hw = a.hw[k];
-    w.mass = node_mass(a.rec, k);
+    w.mass = node_massive(a, k) ? 1.0 : 0.0;  // the walk only asks whether it is > 0
     w.child = a.child[k];
     w.beg = a.beg[k];
     w.end = a.end[k];
     w.mask = 0;
     if (w.child >= 0)
-        for (int c = 0; c < 8; ++c) w.mask |= (node_mass(a.rec, w.child + c) > 0.0 ? 1 : 0) << c;
+        for (int c = 0; c < 8; ++c) w.mask |= (node_massive(a, w.child + c) ? 1 : 0) << c;
     a.wn[k] = w;
 }
 
@@ -861,6 +884,15 @@ cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t te
     int32_t* const off[4] = {a.far_off, a.near_off, a.item_off, a.slot_off};
     tb = temp_bytes;
     return scan4(temp, tb, cnt, off, a.n_nodes + 1, st);
+}
+
+cudaError_t launch_tree_massive(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st) {
+    // the flags go to start_flag (free until the list pass clears it), the counts to mprefix
+    massive_flags_kernel<<<(a.n + 256) / 256, 256, 0, st>>>(a, a.start_flag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t tb = temp_bytes;
+    return cub::DeviceScan::ExclusiveSum(temp, tb, a.start_flag, a.mprefix, a.n + 1, st);
 }
 
 cudaError_t launch_pool_check(const TreeListArgs& a, const int32_t* tree_hdr, cudaStream_t st) {

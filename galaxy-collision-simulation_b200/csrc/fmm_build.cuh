@@ -72,6 +72,12 @@ struct TreeListArgs {
     const double* cz;
     const double* hw;
     const double* rec;  // node records (mass at slot 3)
+    // Optional (capacity mode): the bodies' masses and, filled by launch_tree_massive, the
+    // number of bodies with mass > 0 before each tree position (n + 1).  With all masses
+    // finite and >= 0 a node's mass is > 0 exactly when its range holds such a body, so the
+    // lists then need no node records and can be built while the moments are computed.
+    const double* m;
+    int32_t* mprefix;
     WalkNode* wn;       // n_nodes, filled before the walk
     double theta;
     int64_t t_begin, t_end;
@@ -119,6 +125,10 @@ size_t tree_list_temp_bytes(int32_t n, int32_t n_nodes);
 cudaError_t launch_tree_lists_count(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
 // Capacity mode: after the count pass, the overflow check of the pools (and of the topology
 // build's header tree_hdr).
+// mprefix from the masses (a.m, a.perm); a mass < 0 or NaN marks an overflow with bit 1 of
+// the sticky word (the caller then evaluates through the host-read path).  temp: scan scratch
+// for n + 1 ints.
+cudaError_t launch_tree_massive(const TreeListArgs& a, void* temp, size_t temp_bytes, cudaStream_t st);
 cudaError_t launch_pool_check(const TreeListArgs& a, const int32_t* tree_hdr, cudaStream_t st);
 // The fill walk (each leaf's lists sorted into depth-first order) and the far-field work items.
 cudaError_t launch_tree_lists_fill(const TreeListArgs& a, int32_t n_leaves, cudaStream_t st);
