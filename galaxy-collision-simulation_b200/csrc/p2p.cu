@@ -479,9 +479,6 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                         ZI[h] = pk2(fz, fz);
                     }
                     const f2 E2 = pk2(a.eps2f, a.eps2f);
-                    CompF c[3 * TPT];
-#pragma unroll
-                    for (int k = 0; k < 3 * TPT; ++k) c[k].init();
                     sweep([&](int cnt, int buf) {
                         if (!act) return;
                         const float4* PA = &spk[buf][0];
@@ -523,18 +520,16 @@ __global__ void __launch_bounds__(BS, p2p_threads_per_sm(MODE, TPT) / BS) p2p_ke
                             }
                         }
 #pragma unroll
-                        for (int h = 0; h < TPT; ++h) {  // the pass's two halves, then the compensated sum
+                        for (int h = 0; h < TPT; ++h) {  // the pass's two halves, added into FP64 sums
                             float p0, p1;
                             upk2(PX[h], p0, p1);
-                            c[3 * h].add(p0 + p1);
+                            f[3 * h] += (double)(p0 + p1);
                             upk2(PY[h], p0, p1);
-                            c[3 * h + 1].add(p0 + p1);
+                            f[3 * h + 1] += (double)(p0 + p1);
                             upk2(PZ[h], p0, p1);
-                            c[3 * h + 2].add(p0 + p1);
+                            f[3 * h + 2] += (double)(p0 + p1);
                         }
                     });
-#pragma unroll
-                    for (int k = 0; k < 3 * TPT; ++k) f[k] = c[k].value();
                 }
                 if (act)
 #pragma unroll
