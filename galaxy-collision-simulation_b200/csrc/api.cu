@@ -1450,10 +1450,13 @@ extern "C" int gx_session_autotune(gx_session* s, int precision, double* best_ms
             bms = r.first;
             best = r.second;
         }
-    cudaMemcpyAsync(s->ax, save, (size_t)s->n * 3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
-    cudaStreamSynchronize(s->stream);
+    // the caller's accelerations back, whatever the timing runs did to them
+    cudaError_t restore = cudaMemcpyAsync(s->ax, save, (size_t)s->n * 3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                          s->stream);
+    if (restore == cudaSuccess) restore = cudaStreamSynchronize(s->stream);
     cudaFree(save);
     if (status != GX_OK) return status;
+    if (restore != cudaSuccess) return fail_cuda(restore, "cudaMemcpyAsync (autotune: restoring the accelerations)");
     if (best.variant < 0) return fail(GX_ERR_UNSUPPORTED, "%s: no candidate variant", fn);
     s->cfg[precision] = best;
     {
@@ -3076,10 +3079,10 @@ extern "C" int gx_batch_autotune(gx_batch* b, int precision, double* best_ms) {
             cudaEventRecord(e0, b->stream);
             status = batch_force(b, precision, 0.0);
             cudaEventRecord(e1, b->stream);
-            cudaEventSynchronize(e1);
-            float ms;
-            cudaEventElapsedTime(&ms, e0, e1);
-            t = std::min(t, (double)ms);
+            float ms = 0.f;
+            const cudaError_t te = cudaEventSynchronize(e1);
+            if (te == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) t = std::min(t, (double)ms);
+            else if (status == GX_OK) status = fail_cuda(te != cudaSuccess ? te : cudaGetLastError(), "batch autotune timing");
         }
         if (status == GX_OK && t < bms) {
             bms = t;
