@@ -8,8 +8,9 @@
 // (near-list order, then leaf order).  Leaf costs are very uneven (in the N = 65,536
 // two-disk tree the heaviest leaf has 13x the mean number of sources), so a leaf is cut into
 // target groups x source chunks (at most kMaxChunks chunks of at least kMinChunk sources),
-// items of bounded cost.  A plan computed on the device (p2p_count_kernel, a CUB sort of the
-// leaves by item cost, scans) numbers the items, the leaves with the costliest items first;
+// items of bounded cost.  A plan computed on the device (p2p_count_kernel, then one block's
+// counting sort of the leaves by item cost and its scans, or a CUB sort and scans for large
+// leaf tables) numbers the items, the leaves with the costliest items first;
 // a persistent grid takes them from a ticket counter, so that the last items handed out are
 // the cheapest and the blocks finish together.  Items of an
 // unsplit leaf add their sums to the accelerations directly (target groups are disjoint).
@@ -120,6 +121,90 @@ __global__ void __launch_bounds__(256) p2p_cnt_sorted_kernel(const P2PArgs a, co
 __global__ void __launch_bounds__(256) p2p_off_scatter_kernel(const P2PArgs a, const int* ord, int nl) {
     const int k = blockIdx.x * 256 + threadIdx.x;
     if (k < nl) a.plan_item_off[ord[k]] = a.plan_off_sorted[k];
+}
+
+// The whole plan order in one block when the leaf table is small (at most kSmallPlan entries):
+// leaves by decreasing item-cost key (a counting sort on the 7-bit keys; leaves with equal keys
+// land in no fixed order, which changes only the order in which items are handed out, never a
+// sum), the item counts in that order, their exclusive scan (plan_off_sorted and each leaf's
+// first item), and the exclusive scan of the partial-sum needs in leaf order.  It replaces a
+// radix sort, two scans and two scatter kernels -- about nine launches -- with one.
+constexpr int kSmallPlan = 16384;
+constexpr int kSmallPlanThreads = 1024;
+
+// Exclusive scan of v over the block (kSmallPlanThreads threads); *carry holds the running
+// total of the earlier chunks and is advanced.  Ends with a barrier.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T* carry) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    T x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        T z = s_warp[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const T y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        s_warp[lane] = z;
+    }
+    __syncthreads();
+    const T incl = x + (w > 0 ? s_warp[w - 1] : T(0)) + *carry;
+    __syncthreads();
+    if (t == kSmallPlanThreads - 1) *carry = incl;
+    __syncthreads();
+    return incl - v;
+}
+
+__global__ void __launch_bounds__(kSmallPlanThreads) p2p_small_plan_kernel(const P2PArgs a, int* ord_sorted, int nl) {
+    __shared__ int s_bin[128];
+    __shared__ int s_wi[32];
+    __shared__ long long s_wl[32];
+    __shared__ int s_ci;
+    __shared__ long long s_cl;
+    const int t = threadIdx.x;
+    if (t < 128) s_bin[t] = 0;
+    if (t == 0) {
+        s_ci = 0;
+        s_cl = 0;
+    }
+    __syncthreads();
+    for (int k = t; k < nl; k += kSmallPlanThreads) atomicAdd(&s_bin[a.plan_key[k] & 127], 1);
+    __syncthreads();
+    if (t == 0) {  // bin starts, largest key first
+        int run = 0;
+        for (int b = 127; b >= 0; --b) {
+            const int c = s_bin[b];
+            s_bin[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int k = t; k < nl; k += kSmallPlanThreads) {  // plan_ord is the identity here
+        const int pos = atomicAdd(&s_bin[a.plan_key[k] & 127], 1);
+        ord_sorted[pos] = k;
+        a.plan_cnt_sorted[pos] = a.plan_cnt[k];
+    }
+    __syncthreads();
+    for (int c0 = 0; c0 < nl; c0 += kSmallPlanThreads) {
+        const int k = c0 + t;
+        const int v = k < nl ? a.plan_cnt_sorted[k] : 0;
+        const int ex = block_exclusive_scan<int>(v, s_wi, &s_ci);
+        if (k < nl) {
+            a.plan_off_sorted[k] = ex;
+            a.plan_item_off[ord_sorted[k]] = ex;
+        }
+    }
+    for (int c0 = 0; c0 < nl; c0 += kSmallPlanThreads) {
+        const int k = c0 + t;
+        const long long v = k < nl ? (long long)a.plan_need[k] : 0;
+        const long long ex = block_exclusive_scan<long long>(v, s_wl, &s_cl);
+        if (k < nl) a.plan_scratch[k] = (int64_t)ex;
+    }
 }
 
 // The leaf of every item: item plan_item_off[l] + k belongs to leaf l (k < plan_cnt[l]).  One
@@ -713,7 +798,12 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
     // except in the exact form, whose leaves are never split (N = 2^20 leaf 16: 17 ms sorted,
     // 28 ms in leaf order).
     size_t tb = temp_bytes;
-    if (precision == kF64Exact || leaves_est <= 16 * 4 * sms) {
+    const bool sorted = precision == kF64Exact || leaves_est <= 16 * 4 * sms;
+    if (sorted && nl <= (size_t)kSmallPlan) {
+        p2p_small_plan_kernel<<<1, kSmallPlanThreads, 0, st>>>(a, ord_sorted, (int)nl);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        a.plan_ord = ord_sorted;
+    } else if (sorted) {
         if ((e = cub::DeviceRadixSort::SortPairsDescending(temp, tb, a.plan_key, key_sorted, a.plan_ord,
                                                            ord_sorted, (int)nl, 0, 7, st)) != cudaSuccess)
             return e;
@@ -733,9 +823,11 @@ cudaError_t launch_p2p(P2PArgs a, int64_t n_bodies, int precision, void* scratch
             return e;
         a.plan_off_sorted = a.plan_item_off;
     }
-    tb = temp_bytes;
-    if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
-        return e;
+    if (!(sorted && nl <= (size_t)kSmallPlan)) {  // the small plan kernel scanned the needs already
+        tb = temp_bytes;
+        if ((e = cub::DeviceScan::ExclusiveSum(temp, tb, a.plan_need, a.plan_scratch, (int)nl, st)) != cudaSuccess)
+            return e;
+    }
     p2p_item_leaf_kernel<<<(a.n_leaves + 255) / 256, 256, 0, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (precision == kF64Exact) return launch_bs<kF64Exact, false>(a, bs, 2, sms, st);
